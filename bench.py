@@ -1,0 +1,405 @@
+"""Benchmark: pair interactions/s and steps/s of the WCSPH step on the 1M-fluid
+dam break (dx = 0.005: 1,024,000 fluid + 571,308 wall particles), on one B200
+per rank.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload dam1m|dam16k|periodic8m] [--precision fp32|tiled|half2]
+
+One JSON line on rank 0.  A "step" is one full device-resident timestep
+(binning + Morton sort, density pass when due, EoS, hydro pass, gravity, KDK,
+CFL dt) of the whole workload.  `value` counts the hydro pass's true
+in-support pairs (0 < r^2 < (2h)^2) per second over the timed steps.
+`e2e` is the same metric through the FDPS drop-in C ABI
+(wcsph_hydro_dispatch / wcsph_hydro_retrieve) from host walk records, copies
+included.  `--impl reference` times the reference's own CPU functor
+(STD::CalcHydroForce, built by oracle/) on the same walks, on all host cores.
+Multi-GPU: independent replicas (the dam break is not sharded), weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "pair interactions/s and steps/s (1M dam-break) vs plain FP32; p50/p99 ensemble latency"
+UNIT = "pair interactions/s"
+BYTES_PER_PAIR = {"fp32": 36, "tiled": 36, "half2": 18}  # hydro j-record per evaluated true pair
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="dam1m", choices=["dam1m", "dam16k", "periodic8m"])
+    ap.add_argument("--precision", default="best", choices=["best", "fp32", "tiled", "half2"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def make_case(workload):
+    from weaklycompressiblesph_b200 import cases
+    if workload == "dam1m":
+        return cases.dam_break(dx=0.005)
+    if workload == "dam16k":
+        return cases.dam_break(dx=0.02)
+    return cases.periodic_lattice(n_side=200, dx=0.01, seed=12345)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[4 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def cuda_events_ms(stream_handle, fn):
+    import torch
+    s = torch.cuda.ExternalStream(stream_handle)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    fn()
+    e1.record(s)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def precision_code(name):
+    from weaklycompressiblesph_b200 import _native as N
+    return {"fp32": N.PREC_FP32, "tiled": N.PREC_TILED, "half2": N.PREC_HALF2}[name]
+
+
+def best_precision():
+    from weaklycompressiblesph_b200.sim import BEST_PRECISION
+    return BEST_PRECISION
+
+
+def run_device(case, prec_name, steps, warmup, device, clocks=False):
+    """Timed device-resident steps; returns dict of measurements."""
+    from weaklycompressiblesph_b200.sim import Solver
+    res = {}
+    with Solver(case.n + 1024, precision=precision_code(prec_name), device=device, max_instances=4) as s:
+        k = s.add(case)
+        s.step(warmup)
+        s.synchronize()
+        pairs = s.last_pairs()
+        sampler = ClockSampler(device) if clocks else None
+        if sampler:
+            sampler.__enter__()
+        ms = cuda_events_ms(s.stream(), lambda: s.step(steps))
+        if sampler:
+            sampler.__exit__()
+            res["clocks"] = sampler.summary()
+        pairs_end = s.last_pairs()
+        res["ms_per_step"] = ms / steps
+        res["pairs_per_step"] = 0.5 * (pairs + pairs_end)
+        res["kernels_per_step"] = s.kernels_per_step()
+        # per-phase kernel times (eager launches, CUDA events on the solver stream)
+        prof_steps = max(3, min(20, steps // 5))
+        ph = s.profile_steps(prof_steps)
+        res["phase_ms"] = (ph / prof_steps).tolist()
+        res["status"] = s.status(k)
+    return res
+
+
+def run_e2e(case, steps, warmup, device):
+    """FDPS drop-in over host walk records: dispatch + retrieve per pass."""
+    import ctypes as C
+    from weaklycompressiblesph_b200 import fdps
+    from weaklycompressiblesph_b200 import _native as N
+    pres, snds = case.eos()
+    w = fdps.build_walks(case.pos, 2.0 * case.h, group_size=128)
+    epi, epj = fdps.walk_records(w, case.pos, case.vel, case.dens, pres, snds, case.h, case.mass, case.phys.nu,
+                                 type_=case.type)
+    out = np.zeros(len(epi), fdps.RESULT_HYDRO)
+    N.call("wcsph_init", device)
+    fdps.configure(fdps.pair_params("reference_cpu", alpha=case.phys.alpha, beta=case.phys.beta,
+                                    c_cfl=case.phys.c_cfl, vsig_mode=case.phys.vsig_mode))
+    limit = 16384  # N_WALK_LIMIT, kernel.cuh:4
+    batches = []
+    for w0 in range(0, w.n_walk, limit):
+        w1 = min(w.n_walk, w0 + limit)
+        pi = (C.c_void_p * (w1 - w0))(*[epi[w.i_off[k]:].ctypes.data for k in range(w0, w1)])
+        pj = (C.c_void_p * (w1 - w0))(*[epj[w.j_off[k]:].ctypes.data for k in range(w0, w1)])
+        po = (C.c_void_p * (w1 - w0))(*[out[w.i_off[k]:].ctypes.data for k in range(w0, w1)])
+        ni = np.ascontiguousarray(np.diff(w.i_off[w0:w1 + 1]), np.int32)
+        nj = np.ascontiguousarray(np.diff(w.j_off[w0:w1 + 1]), np.int32)
+        batches.append((pi, pj, po, ni, nj, w1 - w0))
+    L = N.lib()
+
+    def one_pass():
+        for pi, pj, po, ni, nj, nw in batches:
+            N.check("dispatch", L.wcsph_hydro_dispatch(0, nw, pi, N.ptr(ni, C.c_int32), pj, N.ptr(nj, C.c_int32)))
+            N.check("retrieve", L.wcsph_hydro_retrieve(0, nw, N.ptr(ni, C.c_int32), po))
+
+    for _ in range(warmup):
+        one_pass()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one_pass()
+    dt = (time.perf_counter() - t0) / steps
+    h2d = len(epi) * 48 + len(epj) * 48 + 8 * (w.n_walk + len(batches))
+    d2h = len(epi) * 20
+    return dict(s_per_pass=dt, h2d=h2d, d2h=d2h, n_walk=w.n_walk, evaluated=w.n_evaluated, walks=w, epi=epi,
+                epj=epj)
+
+
+def cpu_reference(case, walks, epi, epj, seconds, pairs_total):
+    """The reference's CalcHydroForce (oracle/_ref) on a bounded sample of the
+    same walks, all host threads.  Returns (pairs/s, sample description, cores)."""
+    import oracle
+    if not oracle.ref_available():
+        raise RuntimeError("oracle/_ref/libwcsph_ref.so missing")
+    cores = os.cpu_count() or 1
+    cfg = oracle.config_from_case(case)
+    cnt, tot = oracle.neighbors(oracle.pos4(case.pos.astype(np.float32)), cfg)
+    # probe: time one small sample to size the bounded run
+    n_walk = walks.n_walk
+    stride = max(1, n_walk // 64)
+    sel = np.arange(0, n_walk, stride)
+
+    def sample(sel):
+        i_off = np.zeros(len(sel) + 1, np.int64)
+        j_off = np.zeros(len(sel) + 1, np.int64)
+        i_off[1:] = np.cumsum(walks.i_off[sel + 1] - walks.i_off[sel])
+        j_off[1:] = np.cumsum(walks.j_off[sel + 1] - walks.j_off[sel])
+        ei = np.concatenate([epi[walks.i_off[k]:walks.i_off[k + 1]] for k in sel])
+        ej = np.concatenate([epj[walks.j_off[k]:walks.j_off[k + 1]] for k in sel])
+        pairs = int(sum(cnt[walks.i_idx[walks.i_off[k]:walks.i_off[k + 1]]].sum() for k in sel))
+        return i_off, ei, j_off, ej, pairs
+
+    i_off, ei, j_off, ej, pairs = sample(sel)
+    t0 = time.perf_counter()
+    oracle.ref_hydro_walks(i_off, ei, j_off, ej, nthreads=cores)
+    t1 = time.perf_counter() - t0
+    reps = max(1, int(seconds / max(t1, 1e-3)))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        oracle.ref_hydro_walks(i_off, ei, j_off, ej, nthreads=cores)
+    el = (time.perf_counter() - t0) / reps
+    desc = (f"{len(sel)} of {n_walk} FDPS-style walks (every {stride}th, <=128 i each), {pairs} true pairs, "
+            f"{reps} repetitions, STD::CalcHydroForce -O3 -ffast-math OpenMP")
+    return pairs / el, desc, cores
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args)
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        return main_reference(args)
+    import torch
+    torch.cuda.set_device(local)
+    from weaklycompressiblesph_b200 import build as B
+    B.build()
+    prec = args.precision if args.precision != "best" else best_precision()
+    case = make_case(args.workload)
+    barrier(pg)
+    dev = run_device(case, prec, args.steps, args.warmup, local, clocks=(rank == 0))
+    ms = max_over_ranks(pg, dev["ms_per_step"])
+    pairs_all = sum_over_ranks(pg, dev["pairs_per_step"])
+    value = pairs_all / (ms * 1e-3)
+    steps_per_s = 1e3 / ms
+    plain = None
+    if prec != "fp32":
+        p = run_device(case, "fp32", max(10, args.steps // 4), args.warmup, local)
+        plain = {"value": p["pairs_per_step"] / (p["ms_per_step"] * 1e-3), "steps_per_s": 1e3 / p["ms_per_step"],
+                 "ms_per_step": p["ms_per_step"]}
+    peak, peak_kind = load_peaks()
+    hydro_ms = dev["phase_ms"][2]
+    bpp = BYTES_PER_PAIR[prec]
+    achieved = dev["pairs_per_step"] * bpp / (hydro_ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "hydro_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            t = json.load(f)
+        if t.get("workload") == args.workload and t.get("precision") == prec:
+            traffic = t.get("bytes_per_launch")
+    e2e = None
+    cpu = None
+    if rank == 0 and not args.no_e2e and args.workload != "periodic8m":
+        e = run_e2e(case, max(1, min(3, args.steps // 50)), 1, local)
+        e2e = {"value": dev["pairs_per_step"] / e["s_per_pass"], "unit": UNIT, "h2d_bytes_per_step": e["h2d"],
+               "d2h_bytes_per_step": e["d2h"], "path": "wcsph_hydro_dispatch/retrieve, FDPS walks of <=128 i",
+               "walks": e["n_walk"], "pair_evaluations_per_pass": e["evaluated"]}
+        if not args.no_cpu:
+            v, desc, cores = cpu_reference(case, e["walks"], e["epi"], e["epj"], args.cpu_seconds,
+                                           dev["pairs_per_step"])
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc}
+    if rank != 0:
+        barrier(pg)
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if prec != "half2" else "f16x2-pair/f32-accumulate",
+        "data": "synthetic (seeded lattice IC, no dataset)",
+        "config": {"workload": {"dam1m": "3-D dam break dx=0.005 (1,024,000 fluid + 571,308 wall particles)",
+                                "dam16k": "3-D dam break dx=0.02 (16,000 fluid + 38,508 wall particles)",
+                                "periodic8m": "periodic jittered lattice 200^3 dx=0.01"}[args.workload],
+                   "n_particles": case.n, "precision": prec, "h_over_dx": case.phys.h_over_dx,
+                   "density_mode": case.phys.density_mode, "parallelism": f"replicas x{world}",
+                   "l2": "working set > L2 (126 MB): particle state and records "
+                         f"{case.n * 200 / 1e6:.0f} MB, no flush needed"},
+        "steps_per_s": steps_per_s * 1.0,
+        "pairs_per_step": dev["pairs_per_step"],
+        "plain_fp32": plain,
+        "phase_ms": {"bin_sort_permute": dev["phase_ms"][0], "density": dev["phase_ms"][1],
+                     "hydro": dev["phase_ms"][2], "total": dev["phase_ms"][3]},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "kernel": "hydro pass",
+                     "model": f"{bpp} B per true pair (j-record) / hydro kernel time", "peak_kind": peak_kind},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": dev["kernels_per_step"] * args.steps,
+        "clocks": dev.get("clocks"),
+        "sim_time_s": dev["status"]["time"],
+    }
+    print(json.dumps(line))
+    sys.stdout.flush()
+    barrier(pg)
+    return 0
+
+
+def main_reference(args):
+    """The reference arm: STD::CalcHydroForce (oracle/_ref) over the walks of the
+    same workload on all host cores; each step a bounded sample of walks."""
+    import oracle
+    case = make_case(args.workload)
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libwcsph_ref.so was not built"}))
+        return 0
+    from weaklycompressiblesph_b200 import fdps
+    pres, snds = case.eos()
+    w = fdps.build_walks(case.pos, 2.0 * case.h, group_size=128)
+    epi, epj = fdps.walk_records(w, case.pos, case.vel, case.dens, pres, snds, case.h, case.mass, case.phys.nu,
+                                 type_=case.type)
+    per_step = max(1.0, min(10.0, 120.0 / max(1, args.steps + args.warmup)))
+    vals = []
+    for k in range(args.warmup + args.steps):
+        v, desc, cores = cpu_reference(case, w, epi, epj, per_step, None)
+        if k >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice IC, no dataset)",
+            "config": {"workload": args.workload, "n_particles": case.n},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,238 @@
+/* wcsph — B200-native weakly-compressible SPH hydro force path, C ABI.
+ *
+ * Two surfaces:
+ *
+ *  1. The FDPS multiwalk plugin pair.  The reference hands
+ *       GPU_WC::HydrDispatchKernel / GPU_WC::HydrRetrieveKernel
+ *     (src/prototype.h:7-10, src/kernel.cu:289-409) to
+ *       calcForceAllAndWriteBackMultiWalk(dispatch, retrieve, tag_max, ...)
+ *     (src/main.cpp:71,112,118).  wcsph_hydro_dispatch / wcsph_hydro_retrieve
+ *     take exactly those arguments, with the EPI/EPJ/RESULT records described
+ *     by a byte-offset layout instead of the reference's C++ types, so that the
+ *     library does not depend on the reference's headers.  include/wcsph_fdps.hpp
+ *     defines the GPU_WC:: functions with the reference's signatures on top.
+ *
+ *  2. A device-resident solver (wcsph_sim_*): particle state stays in HBM;
+ *     each step runs cell binning + Morton sort, the density pass, the Tait EoS,
+ *     the hydro pass, gravity, the KDK update and the CFL dt reduction on the
+ *     device (src/main.cpp:89-133 loop order).  One solver object holds any
+ *     number of independent simulation instances that step together
+ *     (ensembles and the serving loop).
+ *
+ * Error convention: every int-returning entry point returns 0 (WCSPH_OK) on
+ * success and a non-zero wcsph_status otherwise; wcsph_last_error() then holds
+ * a message for the calling thread.  (The reference returns 0 always and
+ * asserts on overflow, src/kernel.cu:316,367,380,408.)
+ *
+ * Threading: the plugin state is process-global like the reference's
+ * (src/kernel.cu:239-240); call it from one host thread.  Solver objects are
+ * independent and may be used from different threads.
+ */
+#ifndef WCSPH_H
+#define WCSPH_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WCSPH_ABI_VERSION 1
+
+typedef enum {
+  WCSPH_OK = 0,
+  WCSPH_E_INVALID = 1,  /* bad argument or configuration */
+  WCSPH_E_CUDA = 2,     /* a CUDA runtime call failed */
+  WCSPH_E_CAPACITY = 3, /* a size limit was exceeded (particles, walks, cells, neighbours) */
+  WCSPH_E_STATE = 4,    /* call out of order (e.g. retrieve without dispatch) */
+  WCSPH_E_NOMEM = 5,    /* device or pinned-host allocation failed */
+  WCSPH_E_NODEVICE = 6  /* no CUDA device / the library was not built for it */
+} wcsph_status;
+
+int wcsph_abi_version(void);
+const char* wcsph_last_error(void);
+
+/* Select the CUDA device the plugin uses (replaces the cudaSetDevice(rank) /
+ * stdin prompt of src/kernel.cu:291-299).  Optional: the first dispatch uses
+ * the current device when wcsph_init was not called. */
+int wcsph_init(int32_t device);
+/* Release the plugin's device and pinned buffers (the reference never frees them). */
+int wcsph_finalize(void);
+
+/* ------------------------------------------------------------------------- */
+/* 1. FDPS multiwalk plugin                                                    */
+/* ------------------------------------------------------------------------- */
+
+/* Byte offsets of the FP64 fields inside the caller's plugin records.  Vector
+ * fields are three consecutive doubles.  wcsph_fdps_default_layout() fills in
+ * STD::EPI::Hydro / STD::EPJ::Hydro / STD::RESULT::Hydro of src/class.h:61-263
+ * on x86-64 (96 / 112 / 40 bytes). */
+typedef struct wcsph_fdps_layout {
+  int32_t epi_size, epi_pos, epi_vel, epi_smth, epi_dens, epi_pres, epi_snds, epi_visc;
+  int32_t epj_size, epj_pos, epj_vel, epj_dens, epj_mass, epj_smth, epj_pres, epj_snds, epj_visc;
+  int32_t res_size, res_acc, res_dt, res_div_v;
+  /* Shepard filter records (EPI::Filter, EPJ::Filter, RESULT::Filter, class.h:75-81,194-208,246-262) */
+  int32_t fepi_size, fepi_pos, fepi_smth;
+  int32_t fepj_size, fepj_pos, fepj_dens, fepj_mass;
+  int32_t fres_size, fres_dens;
+} wcsph_fdps_layout;
+
+/* Which pair-sum variant the plugin computes. */
+typedef enum {
+  WCSPH_VSIG_REF_CPU = 0, /* v_sig = max(v_sig,  mu) as src/force.h:47 (always 0)       */
+  WCSPH_VSIG_SIGNAL = 1   /* v_sig = max(v_sig, -mu) as src/kernel.cu:263               */
+} wcsph_vsig_mode;
+typedef enum {
+  WCSPH_GRAD_HBAR = 0, /* gradW(dr, (h_i+h_j)/2)             src/force.h:49   */
+  WCSPH_GRAD_SYM = 1   /* (gradW(dr,h_i) + gradW(dr,h_j))/2  src/kernel.cu:265 */
+} wcsph_grad_mode;
+
+typedef struct wcsph_pair_params {
+  double alpha; /* artificial-viscosity alpha */
+  double beta;  /* coefficient of the mu^2 term (kernel.cu:262 has 2*alpha) */
+  double c_cfl; /* CFL number of the per-particle dt (param.h:5) */
+  double eps;   /* 0.01 in r^2 + eps h_i h_j (force.h:45) */
+  int32_t vsig_mode, grad_mode;
+} wcsph_pair_params;
+
+void wcsph_fdps_default_layout(wcsph_fdps_layout* out);
+/* force.h:31-60 semantics: alpha 0.01, beta 0, C_CFL 0.3, v_sig = max(mu), gradW(hbar). */
+void wcsph_pair_params_reference_cpu(wcsph_pair_params* out);
+/* kernel.cu:241-280 semantics: alpha 0.01, beta 0.02, C_CFL 0.3, v_sig = max(-mu), symmetrised gradW. */
+void wcsph_pair_params_reference_gpu(wcsph_pair_params* out);
+/* Set the record layout and pair variant used by later dispatches (defaults:
+ * wcsph_fdps_default_layout, wcsph_pair_params_reference_gpu). */
+int wcsph_fdps_configure(const wcsph_fdps_layout* layout, const wcsph_pair_params* params);
+
+/* Number of independent tags (buffer sets).  FDPS's tag_max argument
+ * (main.cpp:71 passes 1) must not exceed it. */
+#define WCSPH_FDPS_MAX_TAGS 4
+
+/* Replaces GPU_WC::HydrDispatchKernel (src/prototype.h:9, src/kernel.cu:289-381).
+ * epi[w] points at n_epi[w] EPI records and epj[w] at n_epj[w] EPJ records of
+ * walk w.  The records are staged and the pair sum is enqueued; the call
+ * returns without waiting for the GPU.  Every i of a walk is summed against
+ * every j of the same walk (the FDPS j-list is a superset; pairs outside the
+ * kernel support contribute zero, except to v_sig in WCSPH_VSIG_SIGNAL mode,
+ * which src/kernel.cu:263 takes over the whole list). */
+int wcsph_hydro_dispatch(int32_t tag, int32_t n_walk, const void* const* epi, const int32_t* n_epi,
+                         const void* const* epj, const int32_t* n_epj);
+/* Replaces GPU_WC::HydrRetrieveKernel (src/prototype.h:10, src/kernel.cu:383-409).
+ * Blocks until the walks of the last dispatch with this tag are done and
+ * writes acc, dt and div_v of n_i[w] RESULT records at force[w]. */
+int wcsph_hydro_retrieve(int32_t tag, int32_t n_walk, const int32_t* n_i, void* const* force);
+
+/* Shepard density filter in the same dispatch/retrieve shape (the reference
+ * runs STD::ApplyFilter, src/force.h:10-30, on the CPU through
+ * calcForceAllAndWriteBack; its Gather j-lists contain i itself). */
+int wcsph_filter_dispatch(int32_t tag, int32_t n_walk, const void* const* epi, const int32_t* n_epi,
+                          const void* const* epj, const int32_t* n_epj);
+int wcsph_filter_retrieve(int32_t tag, int32_t n_walk, const int32_t* n_i, void* const* result);
+
+/* ------------------------------------------------------------------------- */
+/* 2. Device-resident solver                                                   */
+/* ------------------------------------------------------------------------- */
+
+typedef enum {
+  WCSPH_PREC_FP32 = 0,  /* plain FP32 pair arithmetic, one thread per i-particle          */
+  WCSPH_PREC_TILED = 1, /* FP32, shared-memory j-tiles, ballot-compacted pair queues      */
+  WCSPH_PREC_HALF2 = 2  /* tiled; pair geometry and kernel gradient in packed half2,
+                           FP32 accumulation, FP32 positions and velocities              */
+} wcsph_precision;
+
+typedef enum {
+  WCSPH_DENSITY_CONTINUITY = 0, /* d rho/dt = -rho div v only (class.h:151)                */
+  WCSPH_DENSITY_SUMMATION = 1,  /* rho_i = sum_j m W_ij (incl. self) every step            */
+  WCSPH_DENSITY_SHEPARD = 2     /* continuity + Shepard filter every shepard_interval steps
+                                   (force.h:10-30, main.cpp:105, param.h:12)              */
+} wcsph_density_mode;
+
+typedef enum { WCSPH_HYDRO = 0, WCSPH_FREEZE = 1 } wcsph_particle_type; /* class.h:33-36 */
+
+/* One simulation instance.  h and mass are uniform within an instance (as the
+ * reference assumes when it hoists them, src/kernel.cu:303-304). */
+typedef struct wcsph_instance_desc {
+  int32_t n;                   /* particles */
+  int32_t density_mode;        /* wcsph_density_mode */
+  int32_t shepard_interval;    /* steps between Shepard filters (reference: 30) */
+  int32_t periodic;            /* 1: periodic box [lo, hi) on all three axes */
+  double h, mass, nu;          /* smoothing length, particle mass, kinematic viscosity */
+  double rho0, gamma, c0;      /* Tait EoS (EoS.h:75-90) */
+  double g;                    /* gravity along -z, added to every particle (Dam2.h:104-108) */
+  double rho_floor;            /* density floor applied after each step (Dam2.h:111) */
+  wcsph_pair_params pair;      /* alpha, beta, C_CFL, eps, v_sig variant (grad_mode is moot: h uniform) */
+  float lo[3], hi[3];          /* cell-grid bounds (the periodic box when periodic) */
+  float kill_lo[3], kill_hi[3];/* HYDRO particles leaving this box are removed (Dam2.h:117-122);
+                                  ignored when kill_lo >= kill_hi on an axis */
+  double t_end;                /* physical end time; 0 = run until removed */
+} wcsph_instance_desc;
+
+typedef struct wcsph_sim_options {
+  int32_t device;              /* CUDA device ordinal */
+  int32_t precision;           /* wcsph_precision */
+  int64_t max_particles;       /* capacity over all instances */
+  int64_t max_cells;           /* capacity of the cell table over all instances */
+  int32_t max_instances;
+  int32_t use_graph;           /* capture each step in a CUDA graph (1) or launch eagerly (0) */
+} wcsph_sim_options;
+
+typedef struct wcsph_sim wcsph_sim;
+
+int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out);
+int wcsph_sim_destroy(wcsph_sim* sim);
+/* Bytes of device memory the solver allocates for these options (admission
+ * control uses it). */
+int64_t wcsph_sim_device_bytes(const wcsph_sim_options* opt);
+
+/* Add an instance from host arrays (pos3/vel3: 3 floats per particle, dens:
+ * 1 float, type: wcsph_particle_type).  Runs the instance's initial force pass
+ * (main.cpp:69-78) before returning.  *slot receives the instance handle. */
+int wcsph_sim_add_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, const float* pos3, const float* vel3,
+                           const float* dens, const int32_t* type, int32_t* slot);
+/* Remove an instance; its particles and cells are reclaimed at the next step. */
+int wcsph_sim_remove_instance(wcsph_sim* sim, int32_t slot);
+
+/* Advance every active instance by nsteps steps (each by its own CFL dt).
+ * Instances whose time reached t_end stop advancing. */
+int wcsph_sim_step(wcsph_sim* sim, int32_t nsteps);
+int wcsph_sim_synchronize(wcsph_sim* sim);
+
+/* Instance status: physical time, steps taken, live particle count, finished flag. */
+int wcsph_sim_instance_status(wcsph_sim* sim, int32_t slot, double* time, int64_t* steps, int32_t* n_alive,
+                              int32_t* finished);
+/* Copy an instance's state to host arrays in its ORIGINAL particle order
+ * (removed particles keep their last state and get alive[i] = 0).  Any pointer may be NULL. */
+int wcsph_sim_read_instance(wcsph_sim* sim, int32_t slot, float* pos3, float* vel3, float* dens, float* acc3,
+                            float* div_v, float* dt_i, int32_t* alive);
+
+/* Diagnostics for parity checks on an instance's current state, without
+ * advancing it, in ORIGINAL particle order: run the force pass (EoS + hydro)
+ * from the current positions, velocities and densities and return the hydro
+ * acceleration (no gravity), div v, per-particle dt and the neighbour count of
+ * each particle.  density_pass: 0 none, 1 summation, 2 Shepard first. */
+int wcsph_sim_probe_forces(wcsph_sim* sim, int32_t slot, int32_t density_pass, float* acc3, float* div_v, float* dt_i,
+                           float* dens_out, int32_t* n_neighbors);
+/* The sorted order of the last binning: perm[k] = original index of the
+ * particle in sorted slot k of the instance, and the Morton cell key of each slot. */
+int wcsph_sim_read_order(wcsph_sim* sim, int32_t slot, int32_t* perm, uint32_t* cell_key);
+/* Conservation sums over an instance, accumulated on the device in FP64:
+ * out[0] mass, out[1..3] momentum, out[4] kinetic energy, out[5] sum of acc*m. */
+int wcsph_sim_conservation(wcsph_sim* sim, int32_t slot, double* out6);
+
+/* Number of true in-support (ordered) pairs the hydro pass summed in the
+ * last step (0 < r^2 < (2h)^2, i != j), over all instances. */
+int64_t wcsph_sim_last_pairs(wcsph_sim* sim);
+/* Number of kernel launches per step issued by the solver (for accounting). */
+int32_t wcsph_sim_kernels_per_step(wcsph_sim* sim);
+/* The solver's CUDA stream (a cudaStream_t), so callers can record events on it. */
+void* wcsph_sim_stream(wcsph_sim* sim);
+/* Run nsteps steps launched one by one (no graph) with CUDA events around each
+ * phase and accumulate milliseconds: ms[0] step-begin + kick + binning + sort +
+ * permutation, ms[1] density pass + EoS refresh, ms[2] hydro pass, ms[3] whole
+ * steps.  Advances the simulation like wcsph_sim_step. */
+int wcsph_sim_profile_steps(wcsph_sim* sim, int32_t nsteps, double* ms4);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WCSPH_H */

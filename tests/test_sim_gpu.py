@@ -1,0 +1,201 @@
+"""Device-resident solver vs the oracle, through the C ABI on the GPU.
+
+Bit-exact: cell keys, sorted order, neighbour counts (FP32 predicate).
+FP32 forces: relative L2 <= 1e-5 against the FP64 oracle on the same state.
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import rel_l2, small_dam
+from weaklycompressiblesph_b200 import cases
+from weaklycompressiblesph_b200 import _native as N
+from weaklycompressiblesph_b200.sim import Solver
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def f32(a):
+    return np.asarray(a, np.float32)
+
+
+def oracle_forces(oracle_lib, case, pos, vel, dens):
+    """FP64 oracle force pass on an FP32 state."""
+    cfg = oracle_lib.config_from_case(case)
+    p4 = oracle_lib.pos4(f32(pos))
+    v4 = oracle_lib.pos4(f32(vel))
+    d = f32(dens).astype(np.float64)
+    pres, snds = oracle_lib.eos(d, case.phys.gamma, case.phys.rho0, case.phys.c0)
+    acc, dv, dt = oracle_lib.hydro(p4, v4, f32(dens), f32(pres), f32(snds), cfg)
+    cnt, tot = oracle_lib.neighbors(p4, cfg)
+    return acc, dv, dt, cnt, tot
+
+
+@pytest.mark.parametrize("which", ["dam", "periodic"])
+def test_order_and_neighbors_bit_exact(native, oracle_lib, which):
+    case = small_dam(dx=0.04) if which == "dam" else cases.periodic_lattice(n_side=24, dx=0.01, seed=1)
+    with Solver(case.n + 16) as s:
+        k = s.add(case, density_mode=N.DENSITY_CONTINUITY)
+        perm, key = s.order(k)
+        cfg = oracle_lib.config_from_case(case)
+        p4 = oracle_lib.pos4(f32(case.pos))
+        _, okey = oracle_lib.cells(p4, cfg)
+        operm = oracle_lib.sort_perm(okey)
+        np.testing.assert_array_equal(perm, operm)
+        np.testing.assert_array_equal(key, okey[operm])
+        pr = s.probe(k)
+        cnt, tot = oracle_lib.neighbors(p4, cfg)
+        np.testing.assert_array_equal(pr["nbr"], cnt)
+        assert int(pr["nbr"].sum()) == tot
+
+
+@pytest.mark.parametrize("which", ["dam", "periodic"])
+def test_hydro_forces(native, oracle_lib, which):
+    case = small_dam(dx=0.04) if which == "dam" else cases.periodic_lattice(n_side=24, dx=0.01, seed=2)
+    with Solver(case.n) as s:
+        k = s.add(case, density_mode=N.DENSITY_CONTINUITY)
+        pr = s.probe(k)
+        acc, dv, dt, cnt, _ = oracle_forces(oracle_lib, case, case.pos, case.vel, case.dens)
+        assert rel_l2(pr["acc"], acc) < TOL
+        assert rel_l2(pr["div_v"], dv) < TOL
+        np.testing.assert_allclose(pr["dt"], dt, rtol=TOL)
+
+
+@pytest.mark.parametrize("shepard", [0, 1])
+def test_density_pass(native, oracle_lib, shepard):
+    case = small_dam(dx=0.04)
+    with Solver(case.n) as s:
+        k = s.add(case, density_mode=N.DENSITY_CONTINUITY)
+        pr = s.probe(k, density_pass=2 if shepard else 1)
+        cfg = oracle_lib.config_from_case(case)
+        ref = oracle_lib.density(oracle_lib.pos4(f32(case.pos)), f32(case.dens), cfg, shepard)
+        np.testing.assert_allclose(pr["dens"], ref, rtol=TOL)
+
+
+def test_initial_pass_matches_oracle(native, oracle_lib):
+    """Initial force pass (main.cpp:69-78) incl. the Shepard filter and gravity."""
+    case = small_dam(dx=0.04)
+    with Solver(case.n) as s:
+        k = s.add(case)
+        st = s.read(k)
+    cfg = oracle_lib.config_from_case(case)
+    o = oracle_lib.new_state(case)
+    o["pos"][:] = f32(case.pos)
+    o["vel"][:] = f32(case.vel)
+    o["dens"][:] = f32(case.dens)
+    oracle_lib.state_initial(case.n, o, cfg)
+    assert rel_l2(st["acc"], o["acc"]) < TOL
+    assert rel_l2(st["div_v"], o["div_v"]) < TOL
+    np.testing.assert_allclose(st["dens"], o["dens"], rtol=TOL)
+
+
+@pytest.mark.parametrize("mode", [N.DENSITY_SHEPARD, N.DENSITY_SUMMATION, N.DENSITY_CONTINUITY])
+def test_trajectory_vs_fp64(native, oracle_lib, mode):
+    """20 device steps (graph) vs 20 FP64 oracle steps from the same start."""
+    case = small_dam(dx=0.04, vel_sigma=0.05)
+    case.phys.density_mode = mode
+    case.phys.shepard_interval = 7
+    nsteps = 20
+    with Solver(case.n) as s:
+        k = s.add(case)
+        s.step(nsteps)
+        st = s.read(k)
+        status = s.status(k)
+    cfg = oracle_lib.config_from_case(case)
+    o = oracle_lib.new_state(case)
+    o["pos"][:] = f32(case.pos)
+    o["vel"][:] = f32(case.vel)
+    o["dens"][:] = f32(case.dens)
+    oracle_lib.state_initial(case.n, o, cfg)
+    t = 0.0
+    for step in range(nsteps):
+        t += oracle_lib.state_step(case.n, o, case.type, cfg, step)
+    assert status["steps"] == nsteps
+    assert status["time"] == pytest.approx(t, rel=1e-5)
+    disp = o["pos"] - f32(case.pos)
+    assert rel_l2(st["pos"] - f32(case.pos), disp) < 1e-3
+    assert rel_l2(st["vel"], o["vel"]) < 1e-3
+    np.testing.assert_allclose(st["dens"], o["dens"], rtol=1e-5)
+
+
+def test_momentum_conservation_periodic(native):
+    """Pair forces are antisymmetric: in a periodic box sum m a = 0."""
+    case = cases.periodic_lattice(n_side=32, dx=0.01, seed=8)
+    with Solver(case.n) as s:
+        k = s.add(case, density_mode=N.DENSITY_CONTINUITY)
+        pr = s.probe(k)
+    tot = np.abs(pr["acc"]).sum(axis=0)
+    assert np.all(np.abs(pr["acc"].sum(axis=0)) < 1e-5 * tot)
+
+
+def test_instances_independent(native):
+    """An instance gives bit-identical results alone and in a mix."""
+    a = small_dam(dx=0.05, seed=1)
+    b = small_dam(dx=0.04, seed=2, column=(0.3, 0.4, 0.6))
+    c = cases.periodic_lattice(n_side=16, dx=0.01, seed=3)
+    with Solver(a.n) as s:
+        k = s.add(a)
+        s.step(15)
+        alone = s.read(k)
+    with Solver(a.n + b.n + c.n, max_instances=4) as s:
+        kb = s.add(b)
+        s.step(3)
+        ka = s.add(a)
+        kc = s.add(c)
+        s.step(15)
+        mix = s.read(ka)
+        assert s.status(ka)["steps"] == 15 and s.status(kb)["steps"] == 18
+    for key in ("pos", "vel", "dens", "acc"):
+        np.testing.assert_array_equal(alone[key], mix[key])
+
+
+def test_remove_and_reuse_slot(native):
+    a = small_dam(dx=0.05, seed=1)
+    b = small_dam(dx=0.05, seed=2)
+    with Solver(a.n + b.n, max_instances=2) as s:
+        ka = s.add(a)
+        kb = s.add(b)
+        s.step(2)
+        s.remove(ka)
+        s.step(2)
+        kc = s.add(a)  # reuses the drained slot
+        assert kc == ka
+        s.step(2)
+        assert s.status(kb)["steps"] == 6
+        assert s.status(kc)["steps"] == 2
+        with pytest.raises(N.WcsphError):
+            s.add(b)  # capacity exhausted
+
+
+def test_escapees_removed(native):
+    """HYDRO particles outside the kill box are removed (Dam2.h:117-122)."""
+    case = small_dam(dx=0.05)
+    fluid = np.nonzero(case.type == N.HYDRO)[0]
+    case.vel[fluid[:5]] = [0.0, 0.0, 200.0]
+    case.kill_hi = (case.kill_hi[0], case.kill_hi[1], 1.2)
+    with Solver(case.n) as s:
+        k = s.add(case)
+        s.step(40)
+        st = s.read(k)
+        assert s.status(k)["n_alive"] == case.n - 5
+    assert np.all(st["alive"][fluid[:5]] == 0)
+    assert st["alive"].sum() == case.n - 5
+
+
+def test_t_end_finishes(native):
+    case = small_dam(dx=0.05)
+    with Solver(case.n) as s:
+        k = s.add(case, t_end=2e-3)
+        s.step(200)
+        st = s.status(k)
+    assert st["finished"] and st["time"] >= 2e-3
+    assert st["time"] < 2e-3 + 1e-3
+
+
+def test_invalid_configs(native):
+    case = cases.periodic_lattice(n_side=4, dx=0.01)  # box of 0.04 < 3 cells of 2h
+    with Solver(case.n) as s:
+        with pytest.raises(N.WcsphError):
+            s.add(case)
+    with pytest.raises(N.WcsphError):
+        Solver(0)

@@ -1,0 +1,611 @@
+// FDPS multiwalk plugin: wcsph_hydro_dispatch / wcsph_hydro_retrieve and the
+// Shepard-filter pair, the drop-in for GPU_WC::HydrDispatchKernel /
+// GPU_WC::HydrRetrieveKernel (src/kernel.cu:289-409, src/prototype.h:7-10).
+//
+// Data path per dispatch (one CUDA stream per tag):
+//   host:   gather the FP64 fields of each walk's EPI/EPJ records (byte offsets
+//           from wcsph_fdps_layout) into pinned FP32 staging records, with
+//           positions taken relative to the walk's first i-particle (so FP32
+//           keeps full relative precision; the reference instead scales by
+//           L, v0, rho0 into half, src/kernel.cu:317-368).  OpenMP over walks.
+//   H2D:    one async copy per chunk of walks, overlapping the packing of the
+//           next chunk.
+//   device: one CTA per walk; the walk's j-records are staged through shared
+//           memory in tiles and every i of the walk (one thread each) sums over
+//           all of them (walk semantics of src/kernel.cu:251-274 and
+//           src/force.h:38-55).
+//   D2H:    results (FP32 acc, div v, dt) copied back per chunk; retrieve
+//           waits on the tag's event and scatters into the caller's RESULT
+//           records in FP64.
+#include <cuda_runtime.h>
+#include <omp.h>
+#include <algorithm>
+#include <cstdarg>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "wcsph_common.cuh"
+
+namespace wcsph {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_err;
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
+  set_error("CUDA error %d (%s) in %s at %s:%d", (int)e, cudaGetErrorString(e), what, file, line);
+  return (e == cudaErrorMemoryAllocation) ? WCSPH_E_NOMEM
+         : (e == cudaErrorNoDevice || e == cudaErrorNoKernelImageForDevice || e == cudaErrorInsufficientDriver)
+             ? WCSPH_E_NODEVICE
+             : WCSPH_E_CUDA;
+}
+
+// ---------------------------------------------------------- walk kernels
+// Staged records (FP32, 48 B): A = (x, y, z, h) relative to the walk origin,
+// B = (vx, vy, vz, rho), C = (P/rho^2, c, nu, m).  i-records use the same
+// shape (m unused).
+struct WalkPair {
+  float alpha, beta, c_cfl, eps;
+  int vsig_mode, grad_mode;
+};
+
+constexpr int kWalkThreads = 128;  // one thread per i; FDPS Ngroup = 128 (param.h:9)
+constexpr int kWalkTile = 256;     // j-records per shared-memory tile
+
+__device__ __forceinline__ float grad_factor(float r, float h) {  // g(r,h) with gradW = g * dr
+  const float H = 2.0f * h;
+  const float iH = __frcp_rn(H);
+  const float K = (float)(16.0 / kPi) * iH * iH * iH * iH;
+  return spline_F(r * iH) * K / r;
+}
+
+template <int VSIG, int GRAD>
+__global__ void __launch_bounds__(kWalkThreads) k_walk_hydro(const float4* __restrict__ iA, const float4* __restrict__ iB,
+                                                            const float4* __restrict__ iC, const float4* __restrict__ jA,
+                                                            const float4* __restrict__ jB, const float4* __restrict__ jC,
+                                                            const int* __restrict__ ni_displ,
+                                                            const int* __restrict__ nj_displ, int walk0, WalkPair pp,
+                                                            float4* __restrict__ out4, float* __restrict__ out_dt) {
+  __shared__ float4 sA[kWalkTile], sB[kWalkTile], sC[kWalkTile];
+  const int w = walk0 + blockIdx.x;
+  const int i0 = ni_displ[w], i1 = ni_displ[w + 1];
+  const int j0 = nj_displ[w], j1 = nj_displ[w + 1];
+  for (int ib = i0; ib < i1; ib += kWalkThreads) {
+    const int i = ib + threadIdx.x;
+    const bool valid = i < i1;
+    float4 a = make_float4(0.f, 0.f, 0.f, 1.f), b = make_float4(0.f, 0.f, 0.f, 1.f), c = make_float4(0.f, 1.f, 0.f, 0.f);
+    if (valid) {
+      a = iA[i];
+      b = iB[i];
+      c = iC[i];
+    }
+    float ax = 0.f, ay = 0.f, az = 0.f, dv_acc = 0.f, vsig = 0.f;
+    for (int jb = j0; jb < j1; jb += kWalkTile) {
+      const int nt = min(kWalkTile, j1 - jb);
+      __syncthreads();
+      for (int k = threadIdx.x; k < nt; k += kWalkThreads) {
+        sA[k] = jA[jb + k];
+        sB[k] = jB[jb + k];
+        sC[k] = jC[jb + k];
+      }
+      __syncthreads();
+      if (!valid) continue;
+      for (int k = 0; k < nt; ++k) {
+        const float4 A = sA[k];
+        const float dx = a.x - A.x, dy = a.y - A.y, dz = a.z - A.z;
+        const float r2 = dist2(dx, dy, dz);
+        if (!(r2 > 0.0f)) continue;  // force.h:42
+        const float4 B = sB[k];
+        const float hi = a.w, hj = A.w;
+        const float dvx = b.x - B.x, dvy = b.y - B.y, dvz = b.z - B.z;
+        const float drdv = dx * dvx + dy * dvy + dz * dvz;
+        const float den = r2 + pp.eps * hi * hj;
+        const float mu = drdv < 0.0f ? 0.5f * (hi + hj) * drdv / den : 0.0f;
+        vsig = VSIG ? fmaxf(vsig, -mu) : fmaxf(vsig, mu);
+        const float r = sqrtf(r2);
+        float g;
+        if (GRAD == WCSPH_GRAD_SYM) {
+          g = 0.0f;
+          if (r < 2.0f * hi) g += grad_factor(r, hi);
+          if (r < 2.0f * hj) g += grad_factor(r, hj);
+          g *= 0.5f;
+        } else {
+          const float hb = 0.5f * (hi + hj);
+          g = (r < 2.0f * hb) ? grad_factor(r, hb) : 0.0f;
+        }
+        if (g == 0.0f) continue;  // outside the support every term below is zero
+        const float4 C = sC[k];
+        const float rho_sum = b.w + B.w;
+        const float av = (-pp.alpha * 0.5f * (c.y + C.y) * mu + pp.beta * mu * mu) * 2.0f / rho_sum;
+        const float pterm = c.x + C.x + av;
+        const float visc = 2.0f * (c.z + C.z) * (g * r2) / rho_sum / den;
+        const float m = C.w;
+        ax += m * (visc * dvx - pterm * g * dx);
+        ay += m * (visc * dvy - pterm * g * dy);
+        az += m * (visc * dvz - pterm * g * dz);
+        dv_acc -= m * g * drdv;
+      }
+    }
+    if (valid) {
+      out4[i] = make_float4(ax, ay, az, dv_acc / b.w);
+      out_dt[i] = pp.c_cfl * a.w / (c.y + vsig);  // force.h:56 / kernel.cu:279
+    }
+  }
+}
+
+// Shepard filter (force.h:12-29): rho_i = sum m W / sum (m/rho_j) W over the
+// walk's j-list (which contains i itself).  iA = (x,y,z,h); jA = (x,y,z,m/rho), jB.x = m.
+__global__ void __launch_bounds__(kWalkThreads) k_walk_filter(const float4* __restrict__ iA, const float4* __restrict__ jA,
+                                                             const float* __restrict__ jm,
+                                                             const int* __restrict__ ni_displ,
+                                                             const int* __restrict__ nj_displ, int walk0,
+                                                             float* __restrict__ out_dens) {
+  __shared__ float4 sA[kWalkTile];
+  __shared__ float sM[kWalkTile];
+  const int w = walk0 + blockIdx.x;
+  const int i0 = ni_displ[w], i1 = ni_displ[w + 1];
+  const int j0 = nj_displ[w], j1 = nj_displ[w + 1];
+  for (int ib = i0; ib < i1; ib += kWalkThreads) {
+    const int i = ib + threadIdx.x;
+    const bool valid = i < i1;
+    const float4 a = valid ? iA[i] : make_float4(0.f, 0.f, 0.f, 1.f);
+    const float H = 2.0f * a.w, iH = __frcp_rn(H);
+    float one = 0.f, sum = 0.f;
+    for (int jb = j0; jb < j1; jb += kWalkTile) {
+      const int nt = min(kWalkTile, j1 - jb);
+      __syncthreads();
+      for (int k = threadIdx.x; k < nt; k += kWalkThreads) {
+        sA[k] = jA[jb + k];
+        sM[k] = jm[jb + k];
+      }
+      __syncthreads();
+      if (!valid) continue;
+      for (int k = 0; k < nt; ++k) {
+        const float4 A = sA[k];
+        const float dx = a.x - A.x, dy = a.y - A.y, dz = a.z - A.z;
+        const float w_ = spline_w(sqrtf(dist2(dx, dy, dz)) * iH);
+        one += w_ * A.w;
+        sum += w_ * sM[k];
+      }
+    }
+    if (valid) out_dens[i] = sum / one;  // the normalisation Kw cancels
+  }
+}
+
+// ------------------------------------------------------------ plugin state
+struct PinnedBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+static int ensure_pinned(PinnedBuf& b, size_t bytes) {
+  if (b.bytes >= bytes) return 0;
+  const size_t want = std::max(bytes, b.bytes * 3 / 2);
+  if (b.p) cudaFreeHost(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  WCSPH_CUDA(cudaMallocHost(&b.p, want));
+  b.bytes = want;
+  return 0;
+}
+static int ensure_dev(DevBuf& b, size_t bytes) {
+  if (b.bytes >= bytes) return 0;
+  const size_t want = std::max(bytes, b.bytes * 3 / 2);
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  WCSPH_CUDA(cudaMalloc(&b.p, want));
+  b.bytes = want;
+  return 0;
+}
+
+enum Kind { K_NONE = 0, K_HYDRO = 1, K_FILTER = 2 };
+
+struct TagState {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  int kind = K_NONE;  // what the last dispatch enqueued
+  int n_walk = 0;
+  long long ni_total = 0;
+  PinnedBuf h_i, h_j, h_off, h_out;
+  DevBuf d_i, d_j, d_off, d_out;
+};
+
+struct Plugin {
+  bool ready = false;
+  int device = -1;
+  wcsph_fdps_layout layout{};
+  wcsph_pair_params pair{};
+  TagState tags[WCSPH_FDPS_MAX_TAGS];
+};
+
+static Plugin g_plugin;
+static std::mutex g_plugin_mu;
+
+static int plugin_ready() {
+  if (g_plugin.ready) return 0;
+  if (g_plugin.device < 0) {
+    int dev = 0;
+    WCSPH_CUDA(cudaGetDevice(&dev));
+    g_plugin.device = dev;
+  }
+  WCSPH_CUDA(cudaSetDevice(g_plugin.device));
+  for (auto& t : g_plugin.tags) {
+    WCSPH_CUDA(cudaStreamCreateWithFlags(&t.stream, cudaStreamNonBlocking));
+    WCSPH_CUDA(cudaEventCreateWithFlags(&t.done, cudaEventDisableTiming));
+  }
+  g_plugin.ready = true;
+  return 0;
+}
+
+static inline double rd(const void* base, int off) {
+  double v;
+  memcpy(&v, (const char*)base + off, sizeof(double));
+  return v;
+}
+static inline void wr(void* base, int off, double v) { memcpy((char*)base + off, &v, sizeof(double)); }
+
+constexpr int kChunks = 4;  // walks are staged and copied in this many pieces
+
+}  // namespace wcsph
+
+using namespace wcsph;
+
+extern "C" {
+
+int wcsph_abi_version(void) { return WCSPH_ABI_VERSION; }
+const char* wcsph_last_error(void) { return g_err.c_str(); }
+
+void wcsph_fdps_default_layout(wcsph_fdps_layout* o) {
+  // src/class.h:61-263 on x86-64 with PS::F64vec = 3 doubles.
+  *o = wcsph_fdps_layout{96, 0, 24, 48, 56, 64, 72, 80,       // EPI::Hydro
+                         112, 0, 24, 48, 56, 64, 72, 80, 88,  // EPJ::Hydro
+                         40, 0, 24, 32,                       // RESULT::Hydro
+                         32, 0, 24,                           // EPI::Filter
+                         40, 0, 24, 32,                       // EPJ::Filter
+                         8, 0};                               // RESULT::Filter
+}
+
+void wcsph_pair_params_reference_cpu(wcsph_pair_params* o) {
+  *o = wcsph_pair_params{0.01, 0.0, 0.3, 0.01, WCSPH_VSIG_REF_CPU, WCSPH_GRAD_HBAR};
+}
+void wcsph_pair_params_reference_gpu(wcsph_pair_params* o) {
+  *o = wcsph_pair_params{0.01, 0.02, 0.3, 0.01, WCSPH_VSIG_SIGNAL, WCSPH_GRAD_SYM};
+}
+
+int wcsph_init(int32_t device) {
+  std::lock_guard<std::mutex> lk(g_plugin_mu);
+  int n = 0;
+  WCSPH_CUDA(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) {
+    set_error("wcsph_init: device %d out of range (%d devices)", device, n);
+    return WCSPH_E_INVALID;
+  }
+  if (g_plugin.ready && g_plugin.device != device) {
+    set_error("wcsph_init: plugin already bound to device %d", g_plugin.device);
+    return WCSPH_E_STATE;
+  }
+  g_plugin.device = device;
+  return plugin_ready();
+}
+
+int wcsph_finalize(void) {
+  std::lock_guard<std::mutex> lk(g_plugin_mu);
+  if (!g_plugin.ready) return 0;
+  cudaSetDevice(g_plugin.device);
+  for (auto& t : g_plugin.tags) {
+    cudaStreamSynchronize(t.stream);
+    for (PinnedBuf* b : {&t.h_i, &t.h_j, &t.h_off, &t.h_out})
+      if (b->p) cudaFreeHost(b->p), b->p = nullptr, b->bytes = 0;
+    for (DevBuf* b : {&t.d_i, &t.d_j, &t.d_off, &t.d_out})
+      if (b->p) cudaFree(b->p), b->p = nullptr, b->bytes = 0;
+    cudaEventDestroy(t.done);
+    cudaStreamDestroy(t.stream);
+    t = TagState{};
+  }
+  g_plugin.ready = false;
+  return 0;
+}
+
+int wcsph_fdps_configure(const wcsph_fdps_layout* layout, const wcsph_pair_params* params) {
+  std::lock_guard<std::mutex> lk(g_plugin_mu);
+  if (layout) {
+    const wcsph_fdps_layout& L = *layout;
+    const int sz[3] = {L.epi_size, L.epj_size, L.res_size};
+    if (sz[0] <= 0 || sz[1] <= 0 || sz[2] <= 0) {
+      set_error("wcsph_fdps_configure: record sizes must be positive");
+      return WCSPH_E_INVALID;
+    }
+    g_plugin.layout = L;
+  }
+  if (params) {
+    if (params->vsig_mode < 0 || params->vsig_mode > 1 || params->grad_mode < 0 || params->grad_mode > 1) {
+      set_error("wcsph_fdps_configure: bad vsig_mode/grad_mode");
+      return WCSPH_E_INVALID;
+    }
+    g_plugin.pair = *params;
+  }
+  return 0;
+}
+
+}  // extern "C"
+
+namespace wcsph {
+static bool g_configured_once = false;
+static void default_config() {
+  if (g_configured_once) return;
+  wcsph_fdps_default_layout(&g_plugin.layout);
+  wcsph_pair_params_reference_gpu(&g_plugin.pair);
+  g_configured_once = true;
+}
+
+static int check_walk_args(const char* fn, int32_t tag, int32_t n_walk, const void* const* epi, const int32_t* n_epi,
+                           const void* const* epj, const int32_t* n_epj) {
+  if (tag < 0 || tag >= WCSPH_FDPS_MAX_TAGS) {
+    set_error("%s: tag %d outside [0, %d)", fn, tag, WCSPH_FDPS_MAX_TAGS);
+    return WCSPH_E_INVALID;
+  }
+  if (n_walk < 0 || (n_walk > 0 && (!epi || !n_epi || !epj || !n_epj))) {
+    set_error("%s: n_walk %d with null arrays", fn, n_walk);
+    return WCSPH_E_INVALID;
+  }
+  for (int w = 0; w < n_walk; ++w)
+    if (n_epi[w] < 0 || n_epj[w] < 0 || (n_epi[w] > 0 && !epi[w]) || (n_epj[w] > 0 && !epj[w])) {
+      set_error("%s: walk %d has a negative count or a null record pointer", fn, w);
+      return WCSPH_E_INVALID;
+    }
+  return 0;
+}
+
+// Shared dispatch body.  kind selects the record shapes and the kernel.
+static int dispatch_common(int kind, int32_t tag, int32_t n_walk, const void* const* epi, const int32_t* n_epi,
+                           const void* const* epj, const int32_t* n_epj) {
+  const char* fn = kind == K_HYDRO ? "wcsph_hydro_dispatch" : "wcsph_filter_dispatch";
+  default_config();
+  if (int rc = check_walk_args(fn, tag, n_walk, epi, n_epi, epj, n_epj)) return rc;
+  if (int rc = plugin_ready()) return rc;
+  WCSPH_CUDA(cudaSetDevice(g_plugin.device));
+  TagState& T = g_plugin.tags[tag];
+  WCSPH_CUDA(cudaStreamSynchronize(T.stream));  // the tag's previous batch owns the buffers until done
+  const wcsph_fdps_layout& L = g_plugin.layout;
+
+  // Displacements (src/kernel.cu:306-310), 64-bit so huge batches cannot wrap.
+  std::vector<long long> ni_d(n_walk + 1), nj_d(n_walk + 1);
+  ni_d[0] = nj_d[0] = 0;
+  for (int w = 0; w < n_walk; ++w) {
+    ni_d[w + 1] = ni_d[w] + n_epi[w];
+    nj_d[w + 1] = nj_d[w] + n_epj[w];
+  }
+  const long long NI = ni_d[n_walk], NJ = nj_d[n_walk];
+  if (NI > INT32_MAX || NJ > INT32_MAX) {
+    set_error("%s: %lld i / %lld j records exceed the 2^31 limit of one batch", fn, NI, NJ);
+    return WCSPH_E_CAPACITY;
+  }
+  const size_t i_rec = kind == K_HYDRO ? 3 * sizeof(float4) : sizeof(float4);
+  const size_t j_rec = kind == K_HYDRO ? 3 * sizeof(float4) : sizeof(float4) + sizeof(float);
+  const size_t o_rec = kind == K_HYDRO ? sizeof(float4) + sizeof(float) : sizeof(float);
+  if (int rc = ensure_pinned(T.h_i, i_rec * (NI + 1))) return rc;
+  if (int rc = ensure_pinned(T.h_j, j_rec * (NJ + 1))) return rc;
+  if (int rc = ensure_pinned(T.h_off, sizeof(int) * 2 * (n_walk + 1))) return rc;
+  if (int rc = ensure_pinned(T.h_out, o_rec * (NI + 1))) return rc;
+  if (int rc = ensure_dev(T.d_i, i_rec * (NI + 1))) return rc;
+  if (int rc = ensure_dev(T.d_j, j_rec * (NJ + 1))) return rc;
+  if (int rc = ensure_dev(T.d_off, sizeof(int) * 2 * (n_walk + 1))) return rc;
+  if (int rc = ensure_dev(T.d_out, o_rec * (NI + 1))) return rc;
+
+  int* h_ni = (int*)T.h_off.p;
+  int* h_nj = h_ni + (n_walk + 1);
+  for (int w = 0; w <= n_walk; ++w) {
+    h_ni[w] = (int)ni_d[w];
+    h_nj[w] = (int)nj_d[w];
+  }
+  int* d_ni = (int*)T.d_off.p;
+  int* d_nj = d_ni + (n_walk + 1);
+  WCSPH_CUDA(cudaMemcpyAsync(d_ni, h_ni, sizeof(int) * 2 * (n_walk + 1), cudaMemcpyHostToDevice, T.stream));
+
+  // SoA sub-arrays inside the staging buffers.
+  float4* hiA = (float4*)T.h_i.p;
+  float4* hiB = hiA + NI;
+  float4* hiC = hiB + NI;
+  float4* hjA = (float4*)T.h_j.p;
+  float4* hjB = hjA + NJ;
+  float4* hjC = hjB + NJ;
+  float* hjm = (float*)(hjA + NJ);  // filter: m after the A block
+  float4* diA = (float4*)T.d_i.p;
+  float4* djA = (float4*)T.d_j.p;
+
+  const int chunks = n_walk < kChunks * 64 ? 1 : kChunks;
+  for (int ch = 0; ch < chunks; ++ch) {
+    const int w0 = (int)((long long)n_walk * ch / chunks), w1 = (int)((long long)n_walk * (ch + 1) / chunks);
+    if (w0 == w1) continue;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int w = w0; w < w1; ++w) {
+      const char* pi = (const char*)epi[w];
+      const char* pj = (const char*)epj[w];
+      // Walk origin: the first i-particle (or j if the walk has no i).
+      double o[3] = {0, 0, 0};
+      if (kind == K_HYDRO) {
+        if (n_epi[w] > 0) {
+          for (int k = 0; k < 3; ++k) o[k] = rd(pi, L.epi_pos + 8 * k);
+        } else if (n_epj[w] > 0) {
+          for (int k = 0; k < 3; ++k) o[k] = rd(pj, L.epj_pos + 8 * k);
+        }
+        for (int i = 0; i < n_epi[w]; ++i) {
+          const char* r = pi + (size_t)i * L.epi_size;
+          const long long q = ni_d[w] + i;
+          const double dens = rd(r, L.epi_dens);
+          hiA[q] = make_float4((float)(rd(r, L.epi_pos) - o[0]), (float)(rd(r, L.epi_pos + 8) - o[1]),
+                               (float)(rd(r, L.epi_pos + 16) - o[2]), (float)rd(r, L.epi_smth));
+          hiB[q] = make_float4((float)rd(r, L.epi_vel), (float)rd(r, L.epi_vel + 8), (float)rd(r, L.epi_vel + 16),
+                               (float)dens);
+          hiC[q] = make_float4((float)(rd(r, L.epi_pres) / (dens * dens)), (float)rd(r, L.epi_snds),
+                               (float)rd(r, L.epi_visc), 0.f);
+        }
+        for (int j = 0; j < n_epj[w]; ++j) {
+          const char* r = pj + (size_t)j * L.epj_size;
+          const long long q = nj_d[w] + j;
+          const double dens = rd(r, L.epj_dens);
+          hjA[q] = make_float4((float)(rd(r, L.epj_pos) - o[0]), (float)(rd(r, L.epj_pos + 8) - o[1]),
+                               (float)(rd(r, L.epj_pos + 16) - o[2]), (float)rd(r, L.epj_smth));
+          hjB[q] = make_float4((float)rd(r, L.epj_vel), (float)rd(r, L.epj_vel + 8), (float)rd(r, L.epj_vel + 16),
+                               (float)dens);
+          hjC[q] = make_float4((float)(rd(r, L.epj_pres) / (dens * dens)), (float)rd(r, L.epj_snds),
+                               (float)rd(r, L.epj_visc), (float)rd(r, L.epj_mass));
+        }
+      } else {
+        if (n_epi[w] > 0) {
+          for (int k = 0; k < 3; ++k) o[k] = rd(pi, L.fepi_pos + 8 * k);
+        } else if (n_epj[w] > 0) {
+          for (int k = 0; k < 3; ++k) o[k] = rd(pj, L.fepj_pos + 8 * k);
+        }
+        for (int i = 0; i < n_epi[w]; ++i) {
+          const char* r = pi + (size_t)i * L.fepi_size;
+          hiA[ni_d[w] + i] = make_float4((float)(rd(r, L.fepi_pos) - o[0]), (float)(rd(r, L.fepi_pos + 8) - o[1]),
+                                         (float)(rd(r, L.fepi_pos + 16) - o[2]), (float)rd(r, L.fepi_smth));
+        }
+        for (int j = 0; j < n_epj[w]; ++j) {
+          const char* r = pj + (size_t)j * L.fepj_size;
+          const double m = rd(r, L.fepj_mass);
+          hjA[nj_d[w] + j] = make_float4((float)(rd(r, L.fepj_pos) - o[0]), (float)(rd(r, L.fepj_pos + 8) - o[1]),
+                                         (float)(rd(r, L.fepj_pos + 16) - o[2]), (float)(m / rd(r, L.fepj_dens)));
+          hjm[nj_d[w] + j] = (float)m;
+        }
+      }
+    }
+    // H2D of this chunk's records (SoA blocks copied piecewise).
+    const long long a0 = ni_d[w0], a1 = ni_d[w1], b0 = nj_d[w0], b1 = nj_d[w1];
+    const int nblk_i = kind == K_HYDRO ? 3 : 1;
+    for (int s = 0; s < nblk_i; ++s)
+      if (a1 > a0)
+        WCSPH_CUDA(cudaMemcpyAsync(diA + s * NI + a0, hiA + s * NI + a0, sizeof(float4) * (a1 - a0),
+                                   cudaMemcpyHostToDevice, T.stream));
+    if (kind == K_HYDRO) {
+      for (int s = 0; s < 3; ++s)
+        if (b1 > b0)
+          WCSPH_CUDA(cudaMemcpyAsync(djA + s * NJ + b0, hjA + s * NJ + b0, sizeof(float4) * (b1 - b0),
+                                     cudaMemcpyHostToDevice, T.stream));
+    } else if (b1 > b0) {
+      WCSPH_CUDA(cudaMemcpyAsync(djA + b0, hjA + b0, sizeof(float4) * (b1 - b0), cudaMemcpyHostToDevice, T.stream));
+      WCSPH_CUDA(cudaMemcpyAsync((float*)(djA + NJ) + b0, hjm + b0, sizeof(float) * (b1 - b0), cudaMemcpyHostToDevice,
+                                 T.stream));
+    }
+    // One CTA per walk.
+    if (kind == K_HYDRO) {
+      const WalkPair pp{(float)g_plugin.pair.alpha, (float)g_plugin.pair.beta, (float)g_plugin.pair.c_cfl,
+                        (float)g_plugin.pair.eps, g_plugin.pair.vsig_mode, g_plugin.pair.grad_mode};
+      float4* out4 = (float4*)T.d_out.p;
+      float* out_dt = (float*)(out4 + NI);
+      auto kern = pp.vsig_mode ? (pp.grad_mode ? k_walk_hydro<1, 1> : k_walk_hydro<1, 0>)
+                               : (pp.grad_mode ? k_walk_hydro<0, 1> : k_walk_hydro<0, 0>);
+      kern<<<w1 - w0, kWalkThreads, 0, T.stream>>>(diA, diA + NI, diA + 2 * NI, djA, djA + NJ, djA + 2 * NJ, d_ni,
+                                                   d_nj, w0, pp, out4, out_dt);
+      WCSPH_CUDA(cudaGetLastError());
+      if (a1 > a0) {
+        WCSPH_CUDA(cudaMemcpyAsync((float4*)T.h_out.p + a0, out4 + a0, sizeof(float4) * (a1 - a0),
+                                   cudaMemcpyDeviceToHost, T.stream));
+        WCSPH_CUDA(cudaMemcpyAsync((float*)((float4*)T.h_out.p + NI) + a0, out_dt + a0, sizeof(float) * (a1 - a0),
+                                   cudaMemcpyDeviceToHost, T.stream));
+      }
+    } else {
+      float* out = (float*)T.d_out.p;
+      k_walk_filter<<<w1 - w0, kWalkThreads, 0, T.stream>>>(diA, djA, (const float*)(djA + NJ), d_ni, d_nj, w0, out);
+      WCSPH_CUDA(cudaGetLastError());
+      if (a1 > a0)
+        WCSPH_CUDA(cudaMemcpyAsync((float*)T.h_out.p + a0, out + a0, sizeof(float) * (a1 - a0), cudaMemcpyDeviceToHost,
+                                   T.stream));
+    }
+  }
+  WCSPH_CUDA(cudaEventRecord(T.done, T.stream));
+  T.kind = kind;
+  T.n_walk = n_walk;
+  T.ni_total = NI;
+  return 0;
+}
+
+static int retrieve_common(int kind, int32_t tag, int32_t n_walk, const int32_t* n_i, void* const* force) {
+  const char* fn = kind == K_HYDRO ? "wcsph_hydro_retrieve" : "wcsph_filter_retrieve";
+  if (tag < 0 || tag >= WCSPH_FDPS_MAX_TAGS) {
+    set_error("%s: tag %d outside [0, %d)", fn, tag, WCSPH_FDPS_MAX_TAGS);
+    return WCSPH_E_INVALID;
+  }
+  TagState& T = g_plugin.tags[tag];
+  if (!g_plugin.ready || T.kind != kind) {
+    set_error("%s: no pending dispatch of this kind for tag %d", fn, tag);
+    return WCSPH_E_STATE;
+  }
+  if (n_walk != T.n_walk || (n_walk > 0 && (!n_i || !force))) {
+    set_error("%s: n_walk %d does not match the dispatch (%d) or null arrays", fn, n_walk, T.n_walk);
+    return WCSPH_E_INVALID;
+  }
+  std::vector<long long> off(n_walk + 1);
+  off[0] = 0;
+  for (int w = 0; w < n_walk; ++w) off[w + 1] = off[w] + n_i[w];
+  if (off[n_walk] != T.ni_total) {
+    set_error("%s: %lld i-particles requested, %lld dispatched", fn, off[n_walk], T.ni_total);
+    return WCSPH_E_INVALID;
+  }
+  WCSPH_CUDA(cudaEventSynchronize(T.done));
+  const wcsph_fdps_layout& L = g_plugin.layout;
+  const long long NI = T.ni_total;
+  if (kind == K_HYDRO) {
+    const float4* o4 = (const float4*)T.h_out.p;
+    const float* odt = (const float*)(o4 + NI);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int w = 0; w < n_walk; ++w) {
+      char* base = (char*)force[w];
+      for (int i = 0; i < n_i[w]; ++i) {
+        const float4 a = o4[off[w] + i];
+        char* r = base + (size_t)i * L.res_size;
+        wr(r, L.res_acc, a.x);
+        wr(r, L.res_acc + 8, a.y);
+        wr(r, L.res_acc + 16, a.z);
+        wr(r, L.res_div_v, a.w);
+        wr(r, L.res_dt, odt[off[w] + i]);
+      }
+    }
+  } else {
+    const float* od = (const float*)T.h_out.p;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int w = 0; w < n_walk; ++w) {
+      char* base = (char*)force[w];
+      for (int i = 0; i < n_i[w]; ++i) wr(base + (size_t)i * L.fres_size, L.fres_dens, od[off[w] + i]);
+    }
+  }
+  T.kind = K_NONE;
+  return 0;
+}
+}  // namespace wcsph
+
+extern "C" {
+int wcsph_hydro_dispatch(int32_t tag, int32_t n_walk, const void* const* epi, const int32_t* n_epi,
+                         const void* const* epj, const int32_t* n_epj) {
+  std::lock_guard<std::mutex> lk(g_plugin_mu);
+  return dispatch_common(K_HYDRO, tag, n_walk, epi, n_epi, epj, n_epj);
+}
+int wcsph_hydro_retrieve(int32_t tag, int32_t n_walk, const int32_t* n_i, void* const* force) {
+  std::lock_guard<std::mutex> lk(g_plugin_mu);
+  return retrieve_common(K_HYDRO, tag, n_walk, n_i, force);
+}
+int wcsph_filter_dispatch(int32_t tag, int32_t n_walk, const void* const* epi, const int32_t* n_epi,
+                          const void* const* epj, const int32_t* n_epj) {
+  std::lock_guard<std::mutex> lk(g_plugin_mu);
+  return dispatch_common(K_FILTER, tag, n_walk, epi, n_epi, epj, n_epj);
+}
+int wcsph_filter_retrieve(int32_t tag, int32_t n_walk, const int32_t* n_i, void* const* result) {
+  std::lock_guard<std::mutex> lk(g_plugin_mu);
+  return retrieve_common(K_FILTER, tag, n_walk, n_i, result);
+}
+}  // extern "C"

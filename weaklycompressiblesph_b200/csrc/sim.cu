@@ -1,0 +1,758 @@
+// Device-resident solver: host orchestration of the step pipeline and the
+// wcsph_sim_* C ABI.
+//
+// Step (one CUDA graph, main.cpp:89-133 order):
+//   k_step_begin   dt rotation (integral.h:2-12 result of the previous pass), time += dt
+//   k_kick_bin     initialKick + fullDrift + predict (class.h:146-159), Morton cell key
+//   radix sort     (keys, slot) pairs, stable
+//   memset x2      cell table
+//   k_permute      gather main -> alt in sorted order, cell table, EoS j-records
+//   k_density/eos  density pass when an instance wants one this step
+//   k_hydro        pair sums, gravity, finalKick, density floor, next dt
+#include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "sim_kernels.cuh"
+#include "sim_aux.cuh"
+#include "sim_tiled.cuh"
+
+namespace wcsph {
+
+struct HostInst {
+  bool used = false;     // slot holds an instance (active or draining)
+  bool active = false;   // stepping
+  wcsph_instance_desc desc{};
+  int n = 0;
+  int ncell[3] = {0, 0, 0};
+  float cell[3] = {0, 0, 0};
+  int bits = 0;
+};
+
+struct SimImpl {
+  wcsph_sim_options opt{};
+  cudaStream_t s = nullptr;
+  SimArrays buf_main{}, buf_alt{};
+  uint32_t *keys_in = nullptr, *keys_out = nullptr;
+  int *vals_in = nullptr, *vals_out = nullptr;
+  float4 *jA = nullptr, *jB = nullptr;
+  float *jC = nullptr, *rho_new = nullptr;
+  int *cell_start = nullptr, *cell_end = nullptr;
+  InstParams* d_params = nullptr;
+  InstDyn* d_dyn = nullptr;
+  int* d_phase = nullptr;
+  int* d_n_alive = nullptr;
+  unsigned long long* d_pairs = nullptr;
+  double* d_cons = nullptr;
+  float4* diag_acc = nullptr;
+  float *diag_dt = nullptr, *diag_rho = nullptr;
+  int* diag_nbr = nullptr;
+  void* cub_tmp = nullptr;
+  size_t cub_bytes = 0;
+  std::vector<void*> allocs;
+
+  std::vector<HostInst> inst;
+  std::vector<InstParams> h_params;
+  std::vector<int> h_phase;
+  int n_host = 0;
+  int key_bits = 1;
+  long long total_cells = 0;
+  bool any_density = false;
+  cudaGraphExec_t gexec = nullptr;
+  bool graph_dirty = true;
+  int kernels_per_step = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+static int alloc(SimImpl& S, void** p, size_t bytes) {
+  WCSPH_CUDA(cudaMalloc(p, bytes ? bytes : 16));
+  S.allocs.push_back(*p);
+  return 0;
+}
+
+static size_t cub_sort_bytes(long long n) {
+  size_t bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr, (const int*)nullptr,
+                                  (int*)nullptr, (int)n, 0, 32);
+  return bytes;
+}
+
+static size_t per_particle_bytes() {
+  return 2 * (4 * sizeof(float4) + sizeof(int) + sizeof(uint32_t))  // main + alt state
+         + 2 * (sizeof(uint32_t) + sizeof(int))                     // sort keys/values in/out
+         + 2 * sizeof(float4) + 2 * sizeof(float)                   // jA, jB, jC, rho_new
+         + sizeof(float4) + 2 * sizeof(float) + sizeof(int);        // diagnostics
+}
+
+static int64_t device_bytes(const wcsph_sim_options& o) {
+  return (int64_t)per_particle_bytes() * o.max_particles + 2 * sizeof(int) * o.max_cells +
+         (sizeof(InstParams) + sizeof(InstDyn) + sizeof(int)) * (int64_t)o.max_instances + (int64_t)cub_sort_bytes(o.max_particles) +
+         (1 << 20);
+}
+
+static int upload_tables(SimImpl& S) {
+  WCSPH_CUDA(cudaMemcpyAsync(S.d_params, S.h_params.data(), sizeof(InstParams) * S.h_params.size(), cudaMemcpyHostToDevice,
+                             S.s));
+  WCSPH_CUDA(cudaMemcpyAsync(S.d_phase, S.h_phase.data(), sizeof(int) * S.h_phase.size(), cudaMemcpyHostToDevice, S.s));
+  return 0;
+}
+
+// Instance-major key and cell spaces over the used slots.
+static int rebuild_tables(SimImpl& S) {
+  uint64_t key = 0;
+  long long cells = 0;
+  S.any_density = false;
+  for (size_t k = 0; k < S.inst.size(); ++k) {
+    HostInst& I = S.inst[k];
+    InstParams& P = S.h_params[k];
+    if (!I.active) {
+      P.active = 0;
+      continue;
+    }
+    P.key_base = (uint32_t)key;
+    P.cell_base = (int)cells;
+    key += (uint64_t)1 << (3 * I.bits);
+    cells += (long long)I.ncell[0] * I.ncell[1] * I.ncell[2];
+    if (I.desc.density_mode != WCSPH_DENSITY_CONTINUITY) S.any_density = true;
+  }
+  if (key >= 0xffffffffull) {
+    set_error("cell key space of the active instances (%llu) exceeds 32 bits", (unsigned long long)key);
+    return WCSPH_E_CAPACITY;
+  }
+  if (cells > S.opt.max_cells) {
+    set_error("active instances need %lld cells, capacity is %lld", cells, (long long)S.opt.max_cells);
+    return WCSPH_E_CAPACITY;
+  }
+  S.total_cells = cells;
+  int bits = 1;
+  while (bits < 32 && ((uint64_t)1 << bits) <= key) ++bits;  // DeadKey & mask must exceed every live key
+  S.key_bits = bits;
+  S.graph_dirty = true;
+  return upload_tables(S);
+}
+
+static StepArgs make_args(SimImpl& S) {
+  StepArgs a{};
+  a.main = S.buf_main;
+  a.alt = S.buf_alt;
+  a.params = S.d_params;
+  a.dyn = S.d_dyn;
+  a.phase = S.d_phase;
+  a.keys_in = S.keys_in;
+  a.vals_in = S.vals_in;
+  a.keys_out = S.keys_out;
+  a.vals_out = S.vals_out;
+  a.jA = S.jA;
+  a.jB = S.jB;
+  a.jC = S.jC;
+  a.rho_new = S.rho_new;
+  a.cell_start = S.cell_start;
+  a.cell_end = S.cell_end;
+  a.n_alive = S.d_n_alive;
+  a.n_host = S.n_host;
+  a.n_inst = (int)S.inst.size();
+  a.pair_count = S.d_pairs;
+  a.diag_acc = S.diag_acc;
+  a.diag_dt = S.diag_dt;
+  a.diag_nbr = S.diag_nbr;
+  a.diag_rho = S.diag_rho;
+  return a;
+}
+
+constexpr int kBlock = 256;
+static inline int nblk(long long n) { return (int)std::max<long long>(1, (n + kBlock - 1) / kBlock); }
+
+// Enqueue one pass of the pipeline.  init_filter adds the initial Shepard
+// filter after the hydro pass (main.cpp:75).  Returns the kernel-launch count.
+static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, int* launches,
+                        cudaEvent_t* ev = nullptr) {
+  int L = 0;
+  const int n = S.n_host;
+  if (ev) WCSPH_CUDA(cudaEventRecord(ev[0], S.s));
+  k_step_begin<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
+  ++L;
+  if (n > 0) {
+    k_kick_bin<<<nblk(n), kBlock, 0, S.s>>>(a);
+    ++L;
+    size_t bytes = S.cub_bytes;
+    WCSPH_CUDA(cub::DeviceRadixSort::SortPairs(S.cub_tmp, bytes, S.keys_in, S.keys_out, S.vals_in, S.vals_out, n, 0,
+                                               S.key_bits, S.s));
+    L += 2 * ((S.key_bits + 7) / 8) + 1;  // onesweep: histogram + one pass per digit (approximate)
+    if (S.total_cells > 0) {
+      WCSPH_CUDA(cudaMemsetAsync(S.cell_start, 0, sizeof(int) * S.total_cells, S.s));
+      WCSPH_CUDA(cudaMemsetAsync(S.cell_end, 0, sizeof(int) * S.total_cells, S.s));
+    }
+    k_permute<<<nblk(n), kBlock, 0, S.s>>>(a);
+    ++L;
+    if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));
+    if (density) {
+      k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(a);
+      k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
+      L += 2;
+    }
+    if (ev) WCSPH_CUDA(cudaEventRecord(ev[2], S.s));
+    if (S.opt.precision == WCSPH_PREC_FP32) {
+      k_hydro_plain<true><<<nblk(n), kBlock, 0, S.s>>>(a);
+    } else {
+      if (int rc = launch_hydro_tiled(a, n, S.opt.precision, S.s)) return rc;
+    }
+    ++L;
+    if (ev) WCSPH_CUDA(cudaEventRecord(ev[3], S.s));
+    k_copy_dead<<<nblk(n), kBlock, 0, S.s>>>(a);
+    ++L;
+    if (init_filter) {
+      StepArgs b = a;
+      b.init_filter = 1;
+      k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(b);
+      k_apply_init_filter<<<nblk(n), kBlock, 0, S.s>>>(b);
+      L += 2;
+    }
+  }
+  WCSPH_CUDA(cudaGetLastError());
+  if (launches) *launches = L;
+  return 0;
+}
+
+static int sync_compact(SimImpl& S) {
+  WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  int n_alive = 0;
+  WCSPH_CUDA(cudaMemcpy(&n_alive, S.d_n_alive, sizeof(int), cudaMemcpyDeviceToHost));
+  if (n_alive != S.n_host) {
+    S.n_host = n_alive;
+    S.graph_dirty = true;
+  }
+  // Slots whose particles are all gone can be reused.
+  for (auto& I : S.inst)
+    if (I.used && !I.active) I.used = false;
+  return 0;
+}
+
+static int set_all_phases(SimImpl& S, int active_phase) {
+  for (size_t k = 0; k < S.inst.size(); ++k) S.h_phase[k] = S.inst[k].active ? active_phase : PH_IDLE;
+  WCSPH_CUDA(cudaMemcpyAsync(S.d_phase, S.h_phase.data(), sizeof(int) * S.h_phase.size(), cudaMemcpyHostToDevice, S.s));
+  return 0;
+}
+
+static int fill_params(const wcsph_instance_desc& d, HostInst& I, InstParams& P) {
+  if (d.n <= 0 || !(d.h > 0) || !(d.mass > 0) || !(d.rho0 > 0) || !(d.gamma > 0) || !(d.c0 > 0) || d.nu < 0) {
+    set_error("instance: n, h, mass, rho0, gamma, c0 must be positive and nu >= 0");
+    return WCSPH_E_INVALID;
+  }
+  if (d.density_mode < 0 || d.density_mode > 2 || (d.density_mode == 2 && d.shepard_interval <= 0)) {
+    set_error("instance: bad density_mode %d / shepard_interval %d", d.density_mode, d.shepard_interval);
+    return WCSPH_E_INVALID;
+  }
+  if (d.pair.vsig_mode < 0 || d.pair.vsig_mode > 1) {
+    set_error("instance: bad vsig_mode %d", d.pair.vsig_mode);
+    return WCSPH_E_INVALID;
+  }
+  P = InstParams{};
+  const float H = 2.0f * (float)d.h;
+  for (int k = 0; k < 3; ++k) {
+    const float ext = d.hi[k] - d.lo[k];
+    if (!(ext > 0)) {
+      set_error("instance: grid bounds must satisfy lo < hi on every axis");
+      return WCSPH_E_INVALID;
+    }
+    int nc = (int)std::floor(ext / (H * 1.0001f));
+    if (nc < 1) nc = 1;
+    if (d.periodic && nc < 3) {
+      set_error("instance: periodic box needs at least 3 cells of edge >= 2h per axis (got %d on axis %d)", nc, k);
+      return WCSPH_E_INVALID;
+    }
+    if (nc > 1024) {
+      set_error("instance: %d cells on axis %d exceed the 10-bit Morton limit (1024)", nc, k);
+      return WCSPH_E_CAPACITY;
+    }
+    I.ncell[k] = nc;
+    I.cell[k] = d.periodic ? ext / (float)nc : std::max(ext / (float)nc, H * 1.0001f);
+    if (I.cell[k] < H) I.cell[k] = H * 1.0001f;
+    P.lo[k] = d.lo[k];
+    P.inv_cell[k] = 1.0f / I.cell[k];
+    P.ncell[k] = nc;
+    P.L[k] = ext;
+    P.halfL[k] = 0.5f * ext;
+    P.kill_lo[k] = d.kill_lo[k];
+    P.kill_hi[k] = d.kill_hi[k];
+    if (d.kill_lo[k] < d.kill_hi[k]) P.kill_on = 1;
+  }
+  int m = std::max(I.ncell[0], std::max(I.ncell[1], I.ncell[2])) - 1;
+  int bits = 0;
+  while ((1 << bits) <= m) ++bits;
+  I.bits = std::max(bits, 1);
+  P.periodic = d.periodic;
+  P.active = 1;
+  P.density_mode = d.density_mode;
+  P.shepard_interval = d.shepard_interval;
+  P.vsig_mode = d.pair.vsig_mode;
+  const double Hd = 2.0 * d.h;
+  P.h = (float)d.h;
+  P.H2 = H * H;
+  P.inv_H = (float)(1.0 / Hd);
+  P.Kw = (float)(16.0 / kPi / (Hd * Hd * Hd));
+  P.Kg = (float)(16.0 / kPi / (Hd * Hd * Hd * Hd));
+  P.W0 = 0.5f * P.Kw;
+  P.mass = (float)d.mass;
+  P.nu4 = (float)(4.0 * d.nu);
+  P.eh2 = (float)(d.pair.eps * d.h * d.h);
+  P.alpha = (float)d.pair.alpha;
+  P.beta = (float)d.pair.beta;
+  P.c_cfl = (float)d.pair.c_cfl;
+  P.rho0 = (float)d.rho0;
+  P.inv_rho0 = (float)(1.0 / d.rho0);
+  const double B = d.c0 * d.c0 * d.rho0 / d.gamma;
+  P.B = (float)B;
+  P.gamma = (float)d.gamma;
+  P.cs2_coef = (float)(B * d.gamma / d.rho0);
+  P.rho_floor = (float)d.rho_floor;
+  P.g = (float)d.g;
+  P.dt_nu = d.nu > 0 ? (float)(0.125 * d.h * d.h / d.nu) : INFINITY;
+  P.t_end = d.t_end;
+  I.desc = d;
+  I.n = d.n;
+  return 0;
+}
+
+}  // namespace wcsph
+
+using namespace wcsph;
+
+struct wcsph_sim {
+  SimImpl impl;
+};
+
+extern "C" {
+
+int64_t wcsph_sim_device_bytes(const wcsph_sim_options* opt) { return opt ? device_bytes(*opt) : -1; }
+
+int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
+  if (!opt || !out || opt->max_particles <= 0 || opt->max_particles > INT32_MAX - 1 || opt->max_cells <= 0 ||
+      opt->max_cells > INT32_MAX || opt->max_instances <= 0 || opt->max_instances > (int)kInstMask ||
+      opt->precision < 0 || opt->precision > 2) {
+    set_error("wcsph_sim_create: invalid options");
+    return WCSPH_E_INVALID;
+  }
+  int ndev = 0;
+  WCSPH_CUDA(cudaGetDeviceCount(&ndev));
+  if (opt->device < 0 || opt->device >= ndev) {
+    set_error("wcsph_sim_create: device %d out of range (%d devices)", opt->device, ndev);
+    return WCSPH_E_NODEVICE;
+  }
+  WCSPH_CUDA(cudaSetDevice(opt->device));
+  auto* sim = new wcsph_sim();
+  SimImpl& S = sim->impl;
+  S.opt = *opt;
+  auto fail = [&](int rc) {
+    for (void* p : S.allocs) cudaFree(p);
+    if (S.s) cudaStreamDestroy(S.s);
+    delete sim;
+    return rc;
+  };
+  if (cudaStreamCreateWithFlags(&S.s, cudaStreamNonBlocking) != cudaSuccess) return fail(WCSPH_E_CUDA);
+  const size_t N = (size_t)opt->max_particles + 1;
+  int rc = 0;
+  for (SimArrays* A : {&S.buf_main, &S.buf_alt}) {
+    rc |= alloc(S, (void**)&A->pos, N * sizeof(float4));
+    rc |= alloc(S, (void**)&A->vel, N * sizeof(float4));
+    rc |= alloc(S, (void**)&A->vh, N * sizeof(float4));
+    rc |= alloc(S, (void**)&A->acc, N * sizeof(float4));
+    rc |= alloc(S, (void**)&A->pid, N * sizeof(int));
+    rc |= alloc(S, (void**)&A->flags, N * sizeof(uint32_t));
+  }
+  rc |= alloc(S, (void**)&S.keys_in, N * sizeof(uint32_t));
+  rc |= alloc(S, (void**)&S.keys_out, N * sizeof(uint32_t));
+  rc |= alloc(S, (void**)&S.vals_in, N * sizeof(int));
+  rc |= alloc(S, (void**)&S.vals_out, N * sizeof(int));
+  rc |= alloc(S, (void**)&S.jA, N * sizeof(float4));
+  rc |= alloc(S, (void**)&S.jB, N * sizeof(float4));
+  rc |= alloc(S, (void**)&S.jC, N * sizeof(float));
+  rc |= alloc(S, (void**)&S.rho_new, N * sizeof(float));
+  rc |= alloc(S, (void**)&S.diag_acc, N * sizeof(float4));
+  rc |= alloc(S, (void**)&S.diag_dt, N * sizeof(float));
+  rc |= alloc(S, (void**)&S.diag_rho, N * sizeof(float));
+  rc |= alloc(S, (void**)&S.diag_nbr, N * sizeof(int));
+  rc |= alloc(S, (void**)&S.cell_start, (size_t)opt->max_cells * sizeof(int));
+  rc |= alloc(S, (void**)&S.cell_end, (size_t)opt->max_cells * sizeof(int));
+  rc |= alloc(S, (void**)&S.d_params, (size_t)opt->max_instances * sizeof(InstParams));
+  rc |= alloc(S, (void**)&S.d_dyn, (size_t)opt->max_instances * sizeof(InstDyn));
+  rc |= alloc(S, (void**)&S.d_phase, (size_t)opt->max_instances * sizeof(int));
+  rc |= alloc(S, (void**)&S.d_n_alive, sizeof(int));
+  rc |= alloc(S, (void**)&S.d_pairs, sizeof(unsigned long long));
+  rc |= alloc(S, (void**)&S.d_cons, 8 * sizeof(double));
+  S.cub_bytes = cub_sort_bytes((long long)N);
+  rc |= alloc(S, &S.cub_tmp, S.cub_bytes);
+  if (rc) return fail(WCSPH_E_NOMEM);
+  if (cudaMemsetAsync(S.d_dyn, 0, (size_t)opt->max_instances * sizeof(InstDyn), S.s) != cudaSuccess ||
+      cudaMemsetAsync(S.d_n_alive, 0, sizeof(int), S.s) != cudaSuccess ||
+      cudaEventCreate(&S.ev0) != cudaSuccess || cudaEventCreate(&S.ev1) != cudaSuccess)
+    return fail(WCSPH_E_CUDA);
+  *out = sim;
+  return 0;
+}
+
+int wcsph_sim_destroy(wcsph_sim* sim) {
+  if (!sim) return 0;
+  SimImpl& S = sim->impl;
+  cudaSetDevice(S.opt.device);
+  cudaStreamSynchronize(S.s);
+  if (S.gexec) cudaGraphExecDestroy(S.gexec);
+  for (void* p : S.allocs) cudaFree(p);
+  cudaEventDestroy(S.ev0);
+  cudaEventDestroy(S.ev1);
+  cudaStreamDestroy(S.s);
+  delete sim;
+  return 0;
+}
+
+int wcsph_sim_add_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, const float* pos3, const float* vel3,
+                           const float* dens, const int32_t* type, int32_t* slot) {
+  if (!sim || !desc || !pos3 || !vel3 || !dens || !type) {
+    set_error("wcsph_sim_add_instance: null argument");
+    return WCSPH_E_INVALID;
+  }
+  SimImpl& S = sim->impl;
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  if (int rc = sync_compact(S)) return rc;
+  if ((long long)S.n_host + desc->n > S.opt.max_particles) {
+    set_error("wcsph_sim_add_instance: %d + %d particles exceed capacity %lld", S.n_host, desc->n,
+              (long long)S.opt.max_particles);
+    return WCSPH_E_CAPACITY;
+  }
+  int k = -1;
+  for (size_t q = 0; q < S.inst.size(); ++q)
+    if (!S.inst[q].used) {
+      k = (int)q;
+      break;
+    }
+  if (k < 0) {
+    if ((int)S.inst.size() >= S.opt.max_instances) {
+      set_error("wcsph_sim_add_instance: all %d instance slots are in use", S.opt.max_instances);
+      return WCSPH_E_CAPACITY;
+    }
+    k = (int)S.inst.size();
+    S.inst.emplace_back();
+    S.h_params.emplace_back();
+    S.h_phase.push_back(PH_IDLE);
+  }
+  HostInst I;
+  InstParams P;
+  if (int rc = fill_params(*desc, I, P)) return rc;
+  I.used = I.active = true;
+  HostInst saved = S.inst[k];
+  InstParams saved_p = S.h_params[k];
+  S.inst[k] = I;
+  S.h_params[k] = P;
+  if (int rc = rebuild_tables(S)) {
+    S.inst[k] = saved;
+    S.h_params[k] = saved_p;
+    rebuild_tables(S);
+    return rc;
+  }
+  // Append the particles at [n_host, n_host + n).
+  const int n = desc->n, base = S.n_host;
+  std::vector<float4> pos(n), vel(n), acc(n, make_float4(0, 0, 0, 0));
+  std::vector<int> pid(n);
+  std::vector<uint32_t> flags(n);
+  for (int i = 0; i < n; ++i) {
+    pos[i] = make_float4(pos3[3 * i], pos3[3 * i + 1], pos3[3 * i + 2], dens[i]);
+    vel[i] = make_float4(vel3[3 * i], vel3[3 * i + 1], vel3[3 * i + 2], 0.f);
+    pid[i] = i;
+    flags[i] = (uint32_t)k | (type[i] == WCSPH_FREEZE ? kFreezeBit : 0u);
+  }
+  WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.pos + base, pos.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, S.s));
+  WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.vel + base, vel.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, S.s));
+  WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.acc + base, acc.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, S.s));
+  WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.pid + base, pid.data(), sizeof(int) * n, cudaMemcpyHostToDevice, S.s));
+  WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.flags + base, flags.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, S.s));
+  InstDyn dyn{};
+  dyn.dt_next_bits = 0x7f800000u;
+  WCSPH_CUDA(cudaMemcpyAsync(S.d_dyn + k, &dyn, sizeof(InstDyn), cudaMemcpyHostToDevice, S.s));
+  S.n_host = base + n;
+  // Initial force pass for this instance only (main.cpp:69-78).
+  for (size_t q = 0; q < S.inst.size(); ++q) S.h_phase[q] = PH_IDLE;
+  S.h_phase[k] = PH_INIT;
+  if (int rc = upload_tables(S)) return rc;
+  StepArgs a = make_args(S);
+  const bool dens_pass = desc->density_mode == WCSPH_DENSITY_SUMMATION;
+  if (int rc = enqueue_pass(S, a, dens_pass, desc->density_mode == WCSPH_DENSITY_SHEPARD, nullptr)) return rc;
+  if (int rc = set_all_phases(S, PH_STEP)) return rc;
+  WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  S.graph_dirty = true;
+  if (slot) *slot = k;
+  return 0;
+}
+
+int wcsph_sim_remove_instance(wcsph_sim* sim, int32_t slot) {
+  if (!sim) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  if (slot < 0 || slot >= (int)S.inst.size() || !S.inst[slot].active) {
+    set_error("wcsph_sim_remove_instance: slot %d is not active", slot);
+    return WCSPH_E_INVALID;
+  }
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  S.inst[slot].active = false;  // particles are marked dead by the next binning
+  S.h_phase[slot] = PH_IDLE;
+  return rebuild_tables(S);
+}
+
+int wcsph_sim_step(wcsph_sim* sim, int32_t nsteps) {
+  if (!sim || nsteps < 0) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  if (nsteps == 0) return 0;
+  StepArgs a = make_args(S);
+  if (!S.opt.use_graph) {
+    WCSPH_CUDA(cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s));
+    for (int t = 0; t < nsteps; ++t) {
+      if (t == nsteps - 1) WCSPH_CUDA(cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s));
+      if (int rc = enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step)) return rc;
+    }
+    return 0;
+  }
+  if (S.graph_dirty || !S.gexec) {
+    if (S.gexec) {
+      cudaGraphExecDestroy(S.gexec);
+      S.gexec = nullptr;
+    }
+    cudaGraph_t g;
+    WCSPH_CUDA(cudaStreamBeginCapture(S.s, cudaStreamCaptureModeThreadLocal));
+    WCSPH_CUDA(cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s));
+    int rc = enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step);
+    cudaError_t e = cudaStreamEndCapture(S.s, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    e = cudaGraphInstantiate(&S.gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+    S.graph_dirty = false;
+  }
+  for (int t = 0; t < nsteps; ++t) WCSPH_CUDA(cudaGraphLaunch(S.gexec, S.s));
+  return 0;
+}
+
+int wcsph_sim_synchronize(wcsph_sim* sim) {
+  if (!sim) return WCSPH_E_INVALID;
+  WCSPH_CUDA(cudaSetDevice(sim->impl.opt.device));
+  WCSPH_CUDA(cudaStreamSynchronize(sim->impl.s));
+  return 0;
+}
+
+int wcsph_sim_instance_status(wcsph_sim* sim, int32_t slot, double* time, int64_t* steps, int32_t* n_alive,
+                              int32_t* finished) {
+  if (!sim) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  if (slot < 0 || slot >= (int)S.inst.size() || !S.inst[slot].used) {
+    set_error("wcsph_sim_instance_status: slot %d is not in use", slot);
+    return WCSPH_E_INVALID;
+  }
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  InstDyn d;
+  WCSPH_CUDA(cudaMemcpy(&d, S.d_dyn + slot, sizeof(InstDyn), cudaMemcpyDeviceToHost));
+  if (time) *time = d.time;
+  if (steps) *steps = d.steps;
+  if (n_alive) *n_alive = d.range_hi > d.range_lo ? d.range_hi - d.range_lo : 0;
+  if (finished) *finished = d.finished;
+  return 0;
+}
+
+}  // extern "C"
+
+namespace wcsph {
+// Copy the instance's slice [range_lo, range_hi) of `src` arrays to host in
+// original order.  Extra tail particles (dead, not yet compacted) are scanned too.
+static int read_slice(SimImpl& S, int slot, const SimArrays& A, InstDyn& d, std::vector<float4>& pos,
+                      std::vector<float4>& vel, std::vector<float4>& acc, std::vector<int>& pid,
+                      std::vector<uint32_t>& flags) {
+  WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  WCSPH_CUDA(cudaMemcpy(&d, S.d_dyn + slot, sizeof(InstDyn), cudaMemcpyDeviceToHost));
+  int n_alive = 0;
+  WCSPH_CUDA(cudaMemcpy(&n_alive, S.d_n_alive, sizeof(int), cudaMemcpyDeviceToHost));
+  const int lo = d.range_hi > d.range_lo ? d.range_lo : 0, hi = d.range_hi > d.range_lo ? d.range_hi : 0;
+  const int nl = hi - lo, nt = S.n_host - n_alive;
+  pos.resize(nl + nt);
+  vel.resize(nl + nt);
+  acc.resize(nl + nt);
+  pid.resize(nl + nt);
+  flags.resize(nl + nt);
+  auto cp = [&](void* dst, const void* src, size_t el, int off, int cnt) -> int {
+    if (cnt > 0) WCSPH_CUDA(cudaMemcpy(dst, (const char*)src + el * off, el * cnt, cudaMemcpyDeviceToHost));
+    return 0;
+  };
+  int rc = 0;
+  rc |= cp(pos.data(), A.pos, sizeof(float4), lo, nl);
+  rc |= cp(vel.data(), A.vel, sizeof(float4), lo, nl);
+  rc |= cp(acc.data(), A.acc, sizeof(float4), lo, nl);
+  rc |= cp(pid.data(), A.pid, sizeof(int), lo, nl);
+  rc |= cp(flags.data(), A.flags, sizeof(uint32_t), lo, nl);
+  rc |= cp(pos.data() + nl, A.pos, sizeof(float4), n_alive, nt);
+  rc |= cp(vel.data() + nl, A.vel, sizeof(float4), n_alive, nt);
+  rc |= cp(acc.data() + nl, A.acc, sizeof(float4), n_alive, nt);
+  rc |= cp(pid.data() + nl, A.pid, sizeof(int), n_alive, nt);
+  rc |= cp(flags.data() + nl, A.flags, sizeof(uint32_t), n_alive, nt);
+  return rc;
+}
+}  // namespace wcsph
+
+extern "C" {
+
+int wcsph_sim_read_instance(wcsph_sim* sim, int32_t slot, float* pos3, float* vel3, float* dens, float* acc3,
+                            float* div_v, float* dt_i, int32_t* alive) {
+  if (!sim) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  if (slot < 0 || slot >= (int)S.inst.size() || !S.inst[slot].used) {
+    set_error("wcsph_sim_read_instance: slot %d is not in use", slot);
+    return WCSPH_E_INVALID;
+  }
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  std::vector<float4> pos, vel, acc;
+  std::vector<int> pid;
+  std::vector<uint32_t> flags;
+  InstDyn d;
+  if (int rc = read_slice(S, slot, S.buf_main, d, pos, vel, acc, pid, flags)) return rc;
+  const int n = S.inst[slot].n;
+  if (alive)
+    for (int i = 0; i < n; ++i) alive[i] = 0;
+  for (size_t q = 0; q < pid.size(); ++q) {
+    if ((int)(flags[q] & kInstMask) != slot) continue;
+    const int i = pid[q];
+    if (i < 0 || i >= n) continue;
+    if (pos3) pos3[3 * i] = pos[q].x, pos3[3 * i + 1] = pos[q].y, pos3[3 * i + 2] = pos[q].z;
+    if (vel3) vel3[3 * i] = vel[q].x, vel3[3 * i + 1] = vel[q].y, vel3[3 * i + 2] = vel[q].z;
+    if (dens) dens[i] = pos[q].w;
+    if (acc3) acc3[3 * i] = acc[q].x, acc3[3 * i + 1] = acc[q].y, acc3[3 * i + 2] = acc[q].z;
+    if (div_v) div_v[i] = acc[q].w;
+    if (dt_i) dt_i[i] = 0.0f;
+    if (alive) alive[i] = (flags[q] & kDeadBit) ? 0 : 1;
+  }
+  return 0;
+}
+
+int wcsph_sim_probe_forces(wcsph_sim* sim, int32_t slot, int32_t density_pass, float* acc3, float* div_v, float* dt_i,
+                           float* dens_out, int32_t* n_neighbors) {
+  if (!sim || density_pass < 0 || density_pass > 2) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  if (slot < 0 || slot >= (int)S.inst.size() || !S.inst[slot].active) {
+    set_error("wcsph_sim_probe_forces: slot %d is not active", slot);
+    return WCSPH_E_INVALID;
+  }
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  for (size_t q = 0; q < S.inst.size(); ++q) S.h_phase[q] = PH_IDLE;
+  S.h_phase[slot] = PH_PROBE;
+  if (int rc = upload_tables(S)) return rc;
+  StepArgs a = make_args(S);
+  a.probe_density = density_pass;
+  int rc = enqueue_pass(S, a, density_pass != 0, false, nullptr);
+  int rc2 = set_all_phases(S, PH_STEP);
+  if (rc) return rc;
+  if (rc2) return rc2;
+  WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  InstDyn d;
+  WCSPH_CUDA(cudaMemcpy(&d, S.d_dyn + slot, sizeof(InstDyn), cudaMemcpyDeviceToHost));
+  const int lo = d.range_lo, nl = d.range_hi > d.range_lo ? d.range_hi - d.range_lo : 0;
+  std::vector<float4> dacc(nl);
+  std::vector<float> ddt(nl), drho(nl);
+  std::vector<int> dn(nl), pid(nl);
+  if (nl > 0) {
+    WCSPH_CUDA(cudaMemcpy(dacc.data(), S.diag_acc + lo, sizeof(float4) * nl, cudaMemcpyDeviceToHost));
+    WCSPH_CUDA(cudaMemcpy(ddt.data(), S.diag_dt + lo, sizeof(float) * nl, cudaMemcpyDeviceToHost));
+    WCSPH_CUDA(cudaMemcpy(drho.data(), S.diag_rho + lo, sizeof(float) * nl, cudaMemcpyDeviceToHost));
+    WCSPH_CUDA(cudaMemcpy(dn.data(), S.diag_nbr + lo, sizeof(int) * nl, cudaMemcpyDeviceToHost));
+    WCSPH_CUDA(cudaMemcpy(pid.data(), S.buf_main.pid + lo, sizeof(int) * nl, cudaMemcpyDeviceToHost));
+  }
+  const int n = S.inst[slot].n;
+  for (int q = 0; q < nl; ++q) {
+    const int i = pid[q];
+    if (i < 0 || i >= n) continue;
+    if (acc3) acc3[3 * i] = dacc[q].x, acc3[3 * i + 1] = dacc[q].y, acc3[3 * i + 2] = dacc[q].z;
+    if (div_v) div_v[i] = dacc[q].w;
+    if (dt_i) dt_i[i] = ddt[q];
+    if (dens_out) dens_out[i] = drho[q];
+    if (n_neighbors) n_neighbors[i] = dn[q];
+  }
+  S.graph_dirty = true;
+  return 0;
+}
+
+int wcsph_sim_read_order(wcsph_sim* sim, int32_t slot, int32_t* perm, uint32_t* cell_key) {
+  if (!sim) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  if (slot < 0 || slot >= (int)S.inst.size() || !S.inst[slot].active) {
+    set_error("wcsph_sim_read_order: slot %d is not active", slot);
+    return WCSPH_E_INVALID;
+  }
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  InstDyn d;
+  WCSPH_CUDA(cudaMemcpy(&d, S.d_dyn + slot, sizeof(InstDyn), cudaMemcpyDeviceToHost));
+  const int lo = d.range_lo, nl = d.range_hi > d.range_lo ? d.range_hi - d.range_lo : 0;
+  if (nl > 0) {
+    if (perm) WCSPH_CUDA(cudaMemcpy(perm, S.buf_main.pid + lo, sizeof(int) * nl, cudaMemcpyDeviceToHost));
+    if (cell_key) {
+      WCSPH_CUDA(cudaMemcpy(cell_key, S.keys_out + lo, sizeof(uint32_t) * nl, cudaMemcpyDeviceToHost));
+      const uint32_t base = S.h_params[slot].key_base;
+      for (int q = 0; q < nl; ++q) cell_key[q] -= base;
+    }
+  }
+  return nl;
+}
+
+int wcsph_sim_conservation(wcsph_sim* sim, int32_t slot, double* out6) {
+  if (!sim || !out6) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  const int n = (slot >= 0 && slot < (int)S.inst.size()) ? S.inst[slot].n : 0;
+  if (n <= 0) {
+    set_error("wcsph_sim_conservation: slot %d is not in use", slot);
+    return WCSPH_E_INVALID;
+  }
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  return launch_conservation(S.buf_main, S.d_dyn, S.d_params, slot, S.d_cons, S.s, out6);
+}
+
+int64_t wcsph_sim_last_pairs(wcsph_sim* sim) {
+  if (!sim) return -1;
+  SimImpl& S = sim->impl;
+  if (cudaSetDevice(S.opt.device) != cudaSuccess || cudaStreamSynchronize(S.s) != cudaSuccess) return -1;
+  unsigned long long c = 0;
+  if (cudaMemcpy(&c, S.d_pairs, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  return (int64_t)c;
+}
+
+int32_t wcsph_sim_kernels_per_step(wcsph_sim* sim) { return sim ? sim->impl.kernels_per_step : -1; }
+
+void* wcsph_sim_stream(wcsph_sim* sim) { return sim ? (void*)sim->impl.s : nullptr; }
+
+int wcsph_sim_profile_steps(wcsph_sim* sim, int32_t nsteps, double* ms4) {
+  if (!sim || !ms4 || nsteps < 0) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  cudaEvent_t ev[4];
+  for (auto& e : ev) WCSPH_CUDA(cudaEventCreate(&e));
+  for (int k = 0; k < 4; ++k) ms4[k] = 0.0;
+  StepArgs a = make_args(S);
+  int rc = 0;
+  for (int t = 0; t < nsteps && !rc; ++t) {
+    if (cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s) != cudaSuccess) rc = WCSPH_E_CUDA;
+    if (!rc) rc = enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step, ev);
+    if (!rc && cudaEventSynchronize(ev[3]) != cudaSuccess) rc = WCSPH_E_CUDA;
+    float x[3];
+    if (!rc) {
+      cudaEventElapsedTime(&x[0], ev[0], ev[1]);
+      cudaEventElapsedTime(&x[1], ev[1], ev[2]);
+      cudaEventElapsedTime(&x[2], ev[2], ev[3]);
+      ms4[0] += x[0];
+      ms4[1] += x[1];
+      ms4[2] += x[2];
+      ms4[3] += x[0] + x[1] + x[2];
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (rc == WCSPH_E_CUDA) set_error("wcsph_sim_profile_steps: CUDA error %s", cudaGetErrorString(cudaGetLastError()));
+  return rc;
+}
+
+}  // extern "C"

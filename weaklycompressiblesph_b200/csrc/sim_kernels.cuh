@@ -1,0 +1,416 @@
+// Device-resident solver kernels: binning, permutation, density, EoS, hydro.
+//
+// Data layout in HBM (structure of arrays, sorted by cell every step):
+//   state "main" and "alt" buffers (float4 each, double-buffered by the sort):
+//     pos = (x, y, z, rho)   vel = (vx, vy, vz, -)   vh = (vx_half, ..., -)
+//     acc = (ax, ay, az, div v)   pid (original index)   flags (instance | FREEZE | dead)
+//   j-records written after the EoS, read by the pair kernels (36 B / particle):
+//     jA = (x, y, z, P/rho^2)   jB = (vx, vy, vz, rho)   jC = c
+//   cell table: start/end per linear cell, instance-major.
+#pragma once
+#include "wcsph_common.cuh"
+
+namespace wcsph {
+
+struct SimArrays {
+  float4 *pos, *vel, *vh, *acc;  // one buffer set
+  int* pid;
+  uint32_t* flags;
+};
+
+struct StepArgs {
+  SimArrays main, alt;
+  const InstParams* params;
+  InstDyn* dyn;
+  const int* phase;       // per-instance phase for this launch
+  uint32_t* keys_in;
+  int* vals_in;
+  const uint32_t* keys_out;
+  const int* vals_out;
+  float4 *jA, *jB;
+  float* jC;
+  float* rho_new;         // density pass output
+  int *cell_start, *cell_end;
+  int* n_alive;           // device count of live particles after binning
+  int n_host;             // particle slots in use (upper bound of live)
+  int n_inst;
+  unsigned long long* pair_count;
+  int init_filter;        // initial-pass Shepard filter launch (main.cpp:75)
+  int probe_density;      // density pass of a probe launch: 0 none, 1 summation, 2 Shepard
+  // diagnostics (probe phase)
+  float4* diag_acc;
+  float* diag_dt;
+  int* diag_nbr;
+  float* diag_rho;
+};
+
+__device__ __forceinline__ float bits_f(unsigned b) { return __uint_as_float(b); }
+
+// ------------------------------------------------------------ step begin
+// One thread per instance: rotate dt, advance time, mark finished.
+__global__ void k_step_begin(StepArgs a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < a.n_inst) {
+    InstDyn& d = a.dyn[k];
+    const InstParams& P = a.params[k];
+    const int ph = a.phase[k];
+    d.range_lo = 0x7fffffff;
+    d.range_hi = 0;
+    if (ph == PH_STEP && P.active) {
+      const float dt = d.finished ? 0.0f : bits_f(d.dt_next_bits);
+      d.dt_cur = dt;
+      d.dt_next_bits = 0x7f800000u;  // +inf
+      if (dt > 0.0f) {
+        d.time += (double)dt;
+        d.steps += 1;
+        if (P.t_end > 0.0 && d.time >= P.t_end) d.finished = 1;
+      }
+    } else if (ph == PH_INIT) {
+      d.dt_cur = 0.0f;
+      d.dt_next_bits = 0x7f800000u;
+    } else {
+      d.dt_cur = 0.0f;
+    }
+  }
+  if (k == 0) *a.n_alive = a.n_host;
+}
+
+// ------------------------------------------------------- kick + binning
+// KDK first half (class.h:146-159 as main.cpp:98-103 runs it), periodic wrap,
+// escapee removal (Dam2.h:117-122), then the Morton cell key of each particle.
+__global__ void k_kick_bin(StepArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.n_host) return;
+  uint32_t f = a.main.flags[p];
+  const int inst = f & kInstMask;
+  const InstParams& P = a.params[inst];
+  bool dead = (f & kDeadBit) || !P.active;
+  float4 x = a.main.pos[p];
+  float4 v = a.main.vel[p];
+  float4 vh = v;
+  if (!dead) {
+    const int ph = a.phase[inst];
+    const float dt = a.dyn[inst].dt_cur;
+    if (ph == PH_STEP && dt > 0.0f) {
+      const float4 acc = a.main.acc[p];
+      x.w += -x.w * dt * acc.w;  // continuity, FREEZE included (class.h:151)
+      if (!(f & kFreezeBit)) {
+        const float hdt = 0.5f * dt;
+        vh = make_float4(v.x + hdt * acc.x, v.y + hdt * acc.y, v.z + hdt * acc.z, 0.f);
+        x.x += dt * vh.x;
+        x.y += dt * vh.y;
+        x.z += dt * vh.z;
+        v = make_float4(v.x + dt * acc.x, v.y + dt * acc.y, v.z + dt * acc.z, 0.f);
+        if (P.periodic) {
+          float* c = &x.x;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const float hi = P.lo[k] + P.L[k];
+            if (c[k] >= hi) c[k] = __fsub_rn(c[k], P.L[k]);
+            else if (c[k] < P.lo[k]) c[k] = __fadd_rn(c[k], P.L[k]);
+          }
+        }
+        if (P.kill_on) {
+          const float* c = &x.x;
+#pragma unroll
+          for (int k = 0; k < 3; ++k)
+            if (P.kill_lo[k] < P.kill_hi[k] && (c[k] < P.kill_lo[k] || c[k] > P.kill_hi[k])) dead = true;
+        }
+      }
+      a.main.pos[p] = x;
+      a.main.vel[p] = v;
+    }
+  }
+  a.main.vh[p] = vh;
+  uint32_t key = kDeadKey;
+  if (dead) {
+    if (!(f & kDeadBit)) a.main.flags[p] = f | kDeadBit;
+  } else {
+    const int cx = cell_of(x.x, P.lo[0], P.inv_cell[0], P.ncell[0]);
+    const int cy = cell_of(x.y, P.lo[1], P.inv_cell[1], P.ncell[1]);
+    const int cz = cell_of(x.z, P.lo[2], P.inv_cell[2], P.ncell[2]);
+    key = P.key_base + morton3(cx, cy, cz);
+  }
+  a.keys_in[p] = key;
+  a.vals_in[p] = p;
+}
+
+// ------------------------------------------------- permutation + tables
+// Gather the state into sorted order (main -> alt), fill the cell table and
+// the instance ranges, count live particles, and write the j-records with the
+// Tait EoS (EoS.h:80-86) of the current density.
+__global__ void k_permute(StepArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.n_host) return;
+  const int src = a.vals_out[p];
+  const uint32_t key = a.keys_out[p];
+  const float4 x = a.main.pos[src];
+  const float4 v = a.main.vel[src];
+  a.alt.pos[p] = x;
+  a.alt.vel[p] = v;
+  a.alt.vh[p] = a.main.vh[src];
+  a.alt.acc[p] = a.main.acc[src];
+  a.alt.pid[p] = a.main.pid[src];
+  const uint32_t f = a.main.flags[src];
+  a.alt.flags[p] = f;
+  const uint32_t kprev = p > 0 ? a.keys_out[p - 1] : 0u;
+  const uint32_t knext = p + 1 < a.n_host ? a.keys_out[p + 1] : kDeadKey;
+  if (key == kDeadKey) {
+    if (p == 0 || kprev != kDeadKey) *a.n_alive = p;
+    return;
+  }
+  const int inst = f & kInstMask;
+  const InstParams& P = a.params[inst];
+  const uint32_t local = key - P.key_base;
+  const int cx = compact3(local), cy = compact3(local >> 1), cz = compact3(local >> 2);
+  const int lin = P.cell_base + (cz * P.ncell[1] + cy) * P.ncell[0] + cx;
+  if (p == 0 || kprev != key) a.cell_start[lin] = p;
+  if (knext != key) a.cell_end[lin] = p + 1;
+  // instance ranges (keys are instance-major, so each instance is contiguous)
+  if (p == 0 || kprev == kDeadKey || (int)(a.main.flags[a.vals_out[p - 1]] & kInstMask) != inst)
+    a.dyn[inst].range_lo = p;
+  if (knext == kDeadKey || (int)(a.main.flags[a.vals_out[p + 1]] & kInstMask) != inst) a.dyn[inst].range_hi = p + 1;
+  float pres, snds;
+  tait(P, x.w, pres, snds);
+  a.jA[p] = make_float4(x.x, x.y, x.z, pres / (x.w * x.w));
+  a.jB[p] = make_float4(v.x, v.y, v.z, x.w);
+  a.jC[p] = snds;
+}
+
+// Density pass of an instance in the current launch: 0 none, 1 summation, 2 Shepard.
+__device__ __forceinline__ int density_kind(const StepArgs& a, const InstParams& P, const InstDyn& d, int ph) {
+  if (ph == PH_IDLE || !P.active) return 0;
+  if (ph == PH_PROBE) return a.probe_density;
+  if (ph == PH_INIT) {
+    if (a.init_filter) return P.density_mode == WCSPH_DENSITY_SHEPARD ? 2 : 0;
+    return P.density_mode == WCSPH_DENSITY_SUMMATION ? 1 : 0;
+  }
+  if (d.dt_cur <= 0.0f) return 0;  // finished: the state no longer changes
+  if (P.density_mode == WCSPH_DENSITY_SUMMATION) return 1;
+  if (P.density_mode == WCSPH_DENSITY_SHEPARD && P.shepard_interval > 0 &&
+      ((d.steps - 1) % P.shepard_interval) == 0)  // main.cpp:105, step index before increment
+    return 2;
+  return 0;
+}
+
+// Does the hydro pass run for an instance in the current launch?
+__device__ __forceinline__ bool wants_force(const InstParams& P, const InstDyn& d, int ph) {
+  if (!P.active) return false;
+  return ph == PH_INIT || ph == PH_PROBE || (ph == PH_STEP && d.dt_cur > 0.0f);
+}
+
+// Neighbour-cell iteration shared by the plain kernels.  Calls body(q, dx, dy, dz, r2)
+// for every in-support j (0 < r2 < (2h)^2, FP32 predicate of the oracle).
+template <typename Body>
+__device__ __forceinline__ void for_each_neighbor(const StepArgs& a, const InstParams& P, float xi, float yi, float zi,
+                                                  Body&& body) {
+  const int cx = cell_of(xi, P.lo[0], P.inv_cell[0], P.ncell[0]);
+  const int cy = cell_of(yi, P.lo[1], P.inv_cell[1], P.ncell[1]);
+  const int cz = cell_of(zi, P.lo[2], P.inv_cell[2], P.ncell[2]);
+  const float H2 = P.H2;
+  for (int oz = -1; oz <= 1; ++oz) {
+    int z = cz + oz;
+    if (P.periodic) z = z < 0 ? z + P.ncell[2] : (z >= P.ncell[2] ? z - P.ncell[2] : z);
+    else if (z < 0 || z >= P.ncell[2]) continue;
+    for (int oy = -1; oy <= 1; ++oy) {
+      int y = cy + oy;
+      if (P.periodic) y = y < 0 ? y + P.ncell[1] : (y >= P.ncell[1] ? y - P.ncell[1] : y);
+      else if (y < 0 || y >= P.ncell[1]) continue;
+      const int row = P.cell_base + (z * P.ncell[1] + y) * P.ncell[0];
+      for (int ox = -1; ox <= 1; ++ox) {
+        int x = cx + ox;
+        if (P.periodic) x = x < 0 ? x + P.ncell[0] : (x >= P.ncell[0] ? x - P.ncell[0] : x);
+        else if (x < 0 || x >= P.ncell[0]) continue;
+        const int lin = row + x;
+        const int s = a.cell_start[lin], e = a.cell_end[lin];
+        for (int q = s; q < e; ++q) {
+          const float4 J = __ldg(&a.jA[q]);
+          float dx = xi - J.x, dy = yi - J.y, dz = zi - J.z;
+          if (P.periodic) {
+            dx = wrap_d(dx, P.L[0], P.halfL[0]);
+            dy = wrap_d(dy, P.L[1], P.halfL[1]);
+            dz = wrap_d(dz, P.L[2], P.halfL[2]);
+          }
+          const float r2 = dist2(dx, dy, dz);
+          if (r2 > 0.0f && r2 < H2) body(q, J, dx, dy, dz, r2);
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------- density pass
+// Summation rho_i = m sum_j W_ij (self included) or the Shepard filter of
+// force.h:12-29, sum m W / sum (m/rho_j) W, from the pre-filter densities.
+__global__ void k_density_plain(StepArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= *a.n_alive) return;
+  const int inst = a.alt.flags[p] & kInstMask;
+  const InstParams& P = a.params[inst];
+  const int kind = density_kind(a, P, a.dyn[inst], a.phase[inst]);
+  if (!kind) return;
+  const float4 I = a.jA[p];
+  const float rho_i = a.jB[p].w;
+  float sum = 0.5f, one = 0.5f / rho_i;  // self term: w(0) = 1/2
+  const float iH = P.inv_H;
+  const bool shep = kind == 2;
+  for_each_neighbor(a, P, I.x, I.y, I.z, [&](int q, const float4&, float, float, float, float r2) {
+    const float w = spline_w(sqrtf(r2) * iH);
+    sum += w;
+    if (shep) one += w / __ldg(&a.jB[q].w);
+  });
+  a.rho_new[p] = shep ? sum / one : P.mass * P.Kw * sum;
+}
+
+// Refresh the j-records of particles whose density was just recomputed.
+__global__ void k_eos(StepArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= *a.n_alive) return;
+  const int inst = a.alt.flags[p] & kInstMask;
+  const InstParams& P = a.params[inst];
+  const int ph = a.phase[inst];
+  if (!density_kind(a, P, a.dyn[inst], ph)) return;
+  const float rho = a.rho_new[p];
+  float pres, snds;
+  tait(P, rho, pres, snds);
+  a.jA[p].w = pres / (rho * rho);
+  a.jB[p].w = rho;
+  a.jC[p] = snds;
+  if (ph != PH_PROBE) a.alt.pos[p].w = rho;
+}
+
+// Warp-aggregated atomic min of a positive float into dt_next of an instance.
+__device__ __forceinline__ void dt_min(InstDyn* dyn, int inst, float v, bool valid) {
+  const unsigned full = 0xffffffffu;
+  const int inst0 = __shfl_sync(full, inst, 0);
+  const bool uniform = __all_sync(full, inst == inst0 || !valid);
+  if (uniform) {
+    float m = valid ? v : __int_as_float(0x7f800000);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(full, m, o));
+    if ((threadIdx.x & 31) == 0 && m < __int_as_float(0x7f800000))
+      atomicMin(&dyn[inst0].dt_next_bits, __float_as_uint(m));
+  } else if (valid) {
+    atomicMin(&dyn[inst].dt_next_bits, __float_as_uint(v));
+  }
+}
+
+// ------------------------------------------------------------ hydro pass
+// One thread per i-particle (the plain FP32 path).  Restates force.h:38-57
+// for uniform h, m, nu within an instance:
+//   a_i  = m sum_j [ -(P_i/rho_i^2 + P_j/rho_j^2 + Pi_ij) g + 4 nu g r^2 / ((rho_i+rho_j)(r^2+eps h^2)) dv ] ...
+// with gradW = g dr; div v_i = -m/rho_i sum_j g (dr.dv); dt_i = C h / (c_i + v_sig).
+// The epilogue adds gravity (Dam2.h:104-108), does the final kick
+// (class.h:160-163), the density floor (Dam2.h:111), and folds the CFL limits
+// of integral.h:2-12 into the instance's next dt.
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_hydro_plain(StepArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = *a.n_alive;
+  const bool in = p < n;
+  int inst = 0;
+  float dt_cand = 0.0f;
+  bool dt_valid = false;
+  unsigned cnt = 0;
+  if (in) {
+    const uint32_t f = a.alt.flags[p];
+    inst = f & kInstMask;
+    const InstParams& P = a.params[inst];
+    const int ph = a.phase[inst];
+    float4 x = a.alt.pos[p];
+    float4 v = a.alt.vel[p];
+    float4 acc = a.alt.acc[p];
+    if (wants_force(P, a.dyn[inst], ph)) {
+      const float4 I = a.jA[p];
+      const float4 IB = a.jB[p];
+      const float ci = a.jC[p];
+      const float rho_i = IB.w, po_i = I.w;
+      float ax = 0.f, ay = 0.f, az = 0.f, dsum = 0.f, vsig = 0.f;
+      const float h = P.h, eh2 = P.eh2, Kg = P.Kg, iH = P.inv_H, alpha = P.alpha, beta = P.beta, nu4 = P.nu4;
+      const int vs = P.vsig_mode;
+      for_each_neighbor(a, P, I.x, I.y, I.z, [&](int q, const float4& J, float dx, float dy, float dz, float r2) {
+        ++cnt;
+        const float4 JB = __ldg(&a.jB[q]);
+        const float cj = __ldg(&a.jC[q]);
+        const float rinv = rsqrtf(r2);
+        const float g = spline_F(r2 * rinv * iH) * Kg * rinv;
+        const float dvx = IB.x - JB.x, dvy = IB.y - JB.y, dvz = IB.z - JB.z;
+        const float drdv = dx * dvx + dy * dvy + dz * dvz;
+        const float rden = __frcp_rn(r2 + eh2);
+        const float mu = drdv < 0.0f ? h * drdv * rden : 0.0f;
+        const float rs = __frcp_rn(rho_i + JB.w);
+        const float av = (beta * mu - alpha * 0.5f * (ci + cj)) * mu * 2.0f * rs;
+        vsig = vs ? fmaxf(vsig, -mu) : fmaxf(vsig, mu);
+        const float pg = (po_i + J.w + av) * g;
+        const float visc = nu4 * g * r2 * rs * rden;
+        ax += visc * dvx - pg * dx;
+        ay += visc * dvy - pg * dy;
+        az += visc * dvz - pg * dz;
+        dsum += g * drdv;
+      });
+      const float m = P.mass;
+      ax *= m;
+      ay *= m;
+      az *= m;
+      const float divv = -m * dsum / rho_i;
+      const float dt_i = P.c_cfl * h / (ci + vsig);
+      if (ph == PH_PROBE) {
+        a.diag_acc[p] = make_float4(ax, ay, az, divv);
+        a.diag_dt[p] = dt_i;
+        a.diag_nbr[p] = (int)cnt;
+        a.diag_rho[p] = rho_i;
+      } else {
+        az -= P.g;
+        const bool hydro = !(f & kFreezeBit);
+        if (hydro) {
+          const float amag = sqrtf(ax * ax + ay * ay + az * az);
+          dt_cand = fminf(fminf(dt_i, 0.25f * sqrtf(h / amag)), P.dt_nu);
+          dt_valid = true;
+          if (ph == PH_STEP) {
+            const float hdt = 0.5f * a.dyn[inst].dt_cur;
+            const float4 vh = a.alt.vh[p];
+            v = make_float4(vh.x + hdt * ax, vh.y + hdt * ay, vh.z + hdt * az, 0.f);
+          }
+        }
+        acc = make_float4(ax, ay, az, divv);
+        x.w = fmaxf(x.w, P.rho_floor);
+      }
+    }
+    a.main.pos[p] = x;
+    a.main.vel[p] = v;
+    a.main.acc[p] = acc;
+    a.main.pid[p] = a.alt.pid[p];
+    a.main.flags[p] = f;
+  }
+  dt_min(a.dyn, inst, dt_cand, dt_valid);
+  if (COUNT) {
+    unsigned long long c = cnt;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(a.pair_count, c);
+  }
+}
+
+// Dead tail [n_alive, n_host): carry the slots over to main unchanged so that
+// removed particles keep their last state until the host compacts.
+__global__ void k_copy_dead(StepArgs a) {
+  const int p = *a.n_alive + blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.n_host) return;
+  a.main.pos[p] = a.alt.pos[p];
+  a.main.vel[p] = a.alt.vel[p];
+  a.main.acc[p] = a.alt.acc[p];
+  a.main.pid[p] = a.alt.pid[p];
+  a.main.flags[p] = a.alt.flags[p];
+}
+
+// Initial Shepard filter of main.cpp:75 (after the initial hydro pass).
+__global__ void k_apply_init_filter(StepArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= *a.n_alive) return;
+  const int inst = a.main.flags[p] & kInstMask;
+  const InstParams& P = a.params[inst];
+  if (a.phase[inst] != PH_INIT || P.density_mode != WCSPH_DENSITY_SHEPARD) return;
+  a.main.pos[p].w = fmaxf(a.rho_new[p], P.rho_floor);
+}
+
+}  // namespace wcsph

@@ -1,0 +1,133 @@
+// Shared device-side definitions: cubic-spline kernel, Tait EoS, instance
+// parameter records, Morton keys, error plumbing.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/wcsph.h"
+
+namespace wcsph {
+
+// ---------------------------------------------------------------- errors ---
+void set_error(const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+
+#define WCSPH_CUDA(call)                                                 \
+  do {                                                                   \
+    cudaError_t e_ = (call);                                             \
+    if (e_ != cudaSuccess) return ::wcsph::cuda_fail(e_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+// ------------------------------------------------------- cubic spline ---
+// 3-D cubic spline of the reference (kernel.h:27-55), support H = 2h:
+//   W(r)     = [(1-s)+^3 - 4 (1/2-s)+^3] * Kw,      Kw = 16 / (pi H^3)
+//   gradW(r) = dr * [12 (1/2-s)+^2 - 3 (1-s)+^2] * Kw / (r H) = g * dr
+constexpr double kPi = 3.14159265358979323846;
+
+__device__ __forceinline__ float spline_F(float s) {  // 12 (1/2-s)+^2 - 3 (1-s)+^2
+  const float a = fmaxf(1.0f - s, 0.0f), b = fmaxf(0.5f - s, 0.0f);
+  return 12.0f * b * b - 3.0f * a * a;
+}
+__device__ __forceinline__ float spline_w(float s) {  // (1-s)+^3 - 4 (1/2-s)+^3
+  const float a = fmaxf(1.0f - s, 0.0f), b = fmaxf(0.5f - s, 0.0f);
+  return a * a * a - 4.0f * b * b * b;
+}
+
+// ------------------------------------------------------------- Morton ---
+__host__ __device__ __forceinline__ uint32_t spread3(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+__host__ __device__ __forceinline__ uint32_t compact3(uint32_t v) {
+  v &= 0x09249249u;
+  v = (v | (v >> 2)) & 0x030C30C3u;
+  v = (v | (v >> 4)) & 0x0300F00Fu;
+  v = (v | (v >> 8)) & 0x030000FFu;
+  v = (v | (v >> 16)) & 0x3ffu;
+  return v;
+}
+__host__ __device__ __forceinline__ uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+  return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
+}
+
+// Cell of a coordinate, FP32, clamped (the oracle evaluates the same expression).
+__device__ __forceinline__ int cell_of(float x, float lo, float inv, int n) {
+  int c = (int)floorf(__fmul_rn(__fsub_rn(x, lo), inv));
+  return c < 0 ? 0 : (c >= n ? n - 1 : c);
+}
+
+// FP32 minimum image on one axis.
+__device__ __forceinline__ float wrap_d(float d, float L, float halfL) {
+  if (d > halfL) d = __fsub_rn(d, L);
+  else if (d < -halfL) d = __fadd_rn(d, L);
+  return d;
+}
+
+// Squared distance as the neighbour predicate defines it.
+__device__ __forceinline__ float dist2(float dx, float dy, float dz) {
+  return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+}
+
+// -------------------------------------------------- instance parameters ---
+// Static per-instance record (uploaded when the instance set changes).
+struct InstParams {
+  float lo[3], inv_cell[3];
+  float L[3], halfL[3];   // periodic box edge and half edge
+  int ncell[3];
+  int cell_base;          // first linear cell of this instance in the global table
+  uint32_t key_base;      // first Morton key of this instance in the global key space
+  int periodic;
+  int active;
+  int density_mode, shepard_interval, vsig_mode, kill_on;
+  // physics in FP32, precomputed
+  float h, H2, inv_H, Kg, Kw, W0, mass, nu4, eh2, alpha, beta, c_cfl;
+  float rho0, inv_rho0, B, gamma, cs2_coef /* B*gamma/rho0 */, rho_floor, g;
+  float dt_nu;            // 0.125 h^2 / nu (or +inf)
+  float kill_lo[3], kill_hi[3];
+  double t_end;
+};
+
+// Dynamic per-instance record (lives on the device, advanced by kernels).
+struct InstDyn {
+  double time;
+  long long steps;
+  float dt_cur;          // dt of the step in flight
+  unsigned dt_next_bits; // atomicMin target: bits of a positive float
+  int finished;
+  int phase;             // 0 idle, 1 step, 2 initial force pass, 3 probe
+  int range_lo, range_hi;// [first, last+1) sorted slot of this instance after binning
+  int n_alive;
+  int pad_;
+};
+
+enum Phase { PH_IDLE = 0, PH_STEP = 1, PH_INIT = 2, PH_PROBE = 3 };
+
+// Particle flags word: bits 0-15 instance slot, bit 16 FREEZE, bit 17 dead.
+constexpr uint32_t kInstMask = 0xffffu;
+constexpr uint32_t kFreezeBit = 1u << 16;
+constexpr uint32_t kDeadBit = 1u << 17;
+constexpr uint32_t kDeadKey = 0xffffffffu;
+
+// Tait EoS (EoS.h:75-90).  x = rho/rho0.
+__device__ __forceinline__ void tait(const InstParams& P, float rho, float& pres, float& snds) {
+  const float x = rho * P.inv_rho0;
+  float xg, xg1;
+  if (P.gamma == 7.0f) {
+    const float x2 = x * x, x3 = x2 * x;
+    xg1 = x3 * x3;
+    xg = xg1 * x;
+  } else {
+    xg = powf(x, P.gamma);
+    xg1 = powf(x, P.gamma - 1.0f);
+  }
+  pres = fmaxf(P.B * (xg - 1.0f), 0.0f);
+  snds = sqrtf(fmaxf(P.cs2_coef * xg1, 1.0e-16f));
+}
+
+}  // namespace wcsph

@@ -1,0 +1,147 @@
+"""Device-resident solver: Python mirror of the wcsph_sim_* C ABI.
+
+A ``Solver`` owns device memory for up to ``max_particles`` particles and any
+number of independent simulation instances that advance together, each with
+its own CFL timestep (the reference's main loop, src/main.cpp:89-133, run on
+the device for every instance at once).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .cases import Case
+
+
+# The fastest pair-sum variant this build ships (used when callers ask for "best").
+BEST_PRECISION = "fp32"
+
+
+def _f32(a, shape):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32).reshape(shape))
+
+
+class Solver:
+    def __init__(self, max_particles, precision=N.PREC_FP32, max_cells=None, max_instances=64, device=0,
+                 use_graph=True):
+        o = N.SimOptions()
+        o.device = device
+        o.precision = precision
+        o.max_particles = int(max_particles)
+        o.max_cells = int(max_cells if max_cells is not None else max(1 << 20, 2 * max_particles))
+        o.max_instances = int(max_instances)
+        o.use_graph = 1 if use_graph else 0
+        self.opt = o
+        h = C.c_void_p()
+        N.call("wcsph_sim_create", C.byref(o), C.byref(h))
+        self._h = h
+        self.slots = {}
+
+    @staticmethod
+    def device_bytes(max_particles, max_cells=None, max_instances=64):
+        o = N.SimOptions(0, 0, int(max_particles), int(max_cells or max(1 << 20, 2 * max_particles)),
+                         int(max_instances), 1)
+        return int(N.lib().wcsph_sim_device_bytes(C.byref(o)))
+
+    def close(self):
+        if self._h:
+            N.lib().wcsph_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- instances ---------------------------------------------------------
+    def add(self, case: Case, density_mode=None, t_end=None) -> int:
+        d = case.desc(density_mode=density_mode, t_end=t_end)
+        pos = _f32(case.pos, (-1, 3))
+        vel = _f32(case.vel, (-1, 3))
+        dens = _f32(case.dens, (-1,))
+        typ = np.ascontiguousarray(case.type, dtype=np.int32)
+        slot = C.c_int32()
+        N.call("wcsph_sim_add_instance", self._h, C.byref(d), N.ptr(pos, C.c_float), N.ptr(vel, C.c_float),
+               N.ptr(dens, C.c_float), N.ptr(typ, C.c_int32), C.byref(slot))
+        self.slots[slot.value] = case
+        return slot.value
+
+    def remove(self, slot):
+        N.call("wcsph_sim_remove_instance", self._h, slot)
+        self.slots.pop(slot, None)
+
+    # -- stepping ----------------------------------------------------------
+    def step(self, nsteps=1):
+        N.call("wcsph_sim_step", self._h, int(nsteps))
+
+    def synchronize(self):
+        N.call("wcsph_sim_synchronize", self._h)
+
+    def status(self, slot):
+        t = C.c_double()
+        s = C.c_int64()
+        n = C.c_int32()
+        f = C.c_int32()
+        N.call("wcsph_sim_instance_status", self._h, slot, C.byref(t), C.byref(s), C.byref(n), C.byref(f))
+        return dict(time=t.value, steps=s.value, n_alive=n.value, finished=bool(f.value))
+
+    def read(self, slot):
+        n = self.slots[slot].n
+        out = dict(pos=np.zeros((n, 3), np.float32), vel=np.zeros((n, 3), np.float32),
+                   dens=np.zeros(n, np.float32), acc=np.zeros((n, 3), np.float32),
+                   div_v=np.zeros(n, np.float32), alive=np.zeros(n, np.int32))
+        N.call("wcsph_sim_read_instance", self._h, slot, N.ptr(out["pos"], C.c_float), N.ptr(out["vel"], C.c_float),
+               N.ptr(out["dens"], C.c_float), N.ptr(out["acc"], C.c_float), N.ptr(out["div_v"], C.c_float), None,
+               N.ptr(out["alive"], C.c_int32))
+        return out
+
+    def probe(self, slot, density_pass=0):
+        """Force pass on the current state without advancing it (original order).
+        Returns acc (hydro only, no gravity), div_v, dt_i, dens used, neighbour counts."""
+        n = self.slots[slot].n
+        out = dict(acc=np.zeros((n, 3), np.float32), div_v=np.zeros(n, np.float32), dt=np.zeros(n, np.float32),
+                   dens=np.zeros(n, np.float32), nbr=np.zeros(n, np.int32))
+        N.call("wcsph_sim_probe_forces", self._h, slot, int(density_pass), N.ptr(out["acc"], C.c_float),
+               N.ptr(out["div_v"], C.c_float), N.ptr(out["dt"], C.c_float), N.ptr(out["dens"], C.c_float),
+               N.ptr(out["nbr"], C.c_int32))
+        return out
+
+    def order(self, slot):
+        n = self.slots[slot].n
+        perm = np.zeros(n, np.int32)
+        key = np.zeros(n, np.uint32)
+        m = N.lib().wcsph_sim_read_order(self._h, slot, N.ptr(perm, C.c_int32), N.ptr(key, C.c_uint32))
+        if m < 0:
+            N.check("wcsph_sim_read_order", m)
+        return perm[:m], key[:m]
+
+    def conservation(self, slot):
+        out = np.zeros(6, np.float64)
+        N.call("wcsph_sim_conservation", self._h, slot, N.ptr(out, C.c_double))
+        return out
+
+    def last_pairs(self):
+        return int(N.lib().wcsph_sim_last_pairs(self._h))
+
+    def kernels_per_step(self):
+        return int(N.lib().wcsph_sim_kernels_per_step(self._h))
+
+    def stream(self):
+        """The solver's cudaStream_t as an integer handle."""
+        return int(N.lib().wcsph_sim_stream(self._h) or 0)
+
+    def profile_steps(self, nsteps):
+        """Advance nsteps eagerly with CUDA events per phase; returns ms summed
+        over the steps: [binning+sort+permute, density, hydro, total]."""
+        ms = np.zeros(4, np.float64)
+        N.call("wcsph_sim_profile_steps", self._h, int(nsteps), N.ptr(ms, C.c_double))
+        return ms
