@@ -169,8 +169,9 @@ def test_remove_and_reuse_slot(native):
 
 def test_escapees_removed(native):
     """HYDRO particles outside the kill box are removed (Dam2.h:117-122)."""
-    case = small_dam(dx=0.05)
+    case = small_dam(dx=0.05, vel_sigma=0.0)
     fluid = np.nonzero(case.type == N.HYDRO)[0]
+    fluid = fluid[np.argsort(-case.pos[fluid, 2], kind="stable")]  # top surface first
     case.vel[fluid[:5]] = [0.0, 0.0, 200.0]
     case.kill_hi = (case.kill_hi[0], case.kill_hi[1], 1.2)
     with Solver(case.n) as s:
