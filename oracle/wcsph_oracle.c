@@ -207,24 +207,29 @@ static void table_free(cell_table* T) {
   free(T->cxyz);
 }
 
-/* FP32 minimum-image difference on one axis. */
-static inline float wrap_d(float d, float L, float halfL) {
-  if (d > halfL) d -= L;
-  else if (d < -halfL) d += L;
-  return d;
+/* Periodic images.  A candidate j is visited through one of the 27 cells
+ * around i's cell; when that cell index wraps past the box edge on an axis,
+ * j is taken at its image x_j + s L with s = +1 (wrapped past the high edge)
+ * or s = -1 (past the low edge).  The FP32 displacement is
+ *   d = x_i - (x_j + s L)           (two rounded operations, as on the device)
+ * With at least 3 cells of edge >= 2h per periodic axis this is the minimum
+ * image of every in-support pair.  Neighbour entries carry the shifts:
+ *   entry = j * 27 + (sx+1) + 3 (sy+1) + 9 (sz+1).                           */
+#define ENC(j, sx, sy, sz) ((j) * 27 + ((sx) + 1) + 3 * ((sy) + 1) + 9 * ((sz) + 1))
+static inline int ent_j(int e) { return e / 27; }
+static inline void ent_s(int e, int s[3]) {
+  const int c = e % 27;
+  s[0] = c % 3 - 1;
+  s[1] = (c / 3) % 3 - 1;
+  s[2] = c / 9 - 1;
 }
 
 /* The neighbour predicate, FP32, exactly as the device evaluates it:
- *   d = x_i - x_j (min image if periodic),  r2 = fma(dz,dz, fma(dy,dy, dx*dx)),
- *   in support  <=>  0 < r2 < H2,  H = 2*(float)h,  H2 = H*H.                */
-static inline int in_support(const float* pi, const float* pj, const orc_config* cfg, float H2, float d[3]) {
-  for (int k = 0; k < 3; ++k) {
-    d[k] = pi[k] - pj[k];
-    if (cfg->periodic) {
-      const float L = cfg->hi[k] - cfg->lo[k];
-      d[k] = wrap_d(d[k], L, 0.5f * L);
-    }
-  }
+ *   r2 = fma(dz,dz, fma(dy,dy, dx*dx)),  in support <=> 0 < r2 < H2,
+ *   H = 2*(float)h, H2 = H*H.                                                */
+static inline int in_support(const float* pi, const float* pj, const float sh[3], float H2) {
+  float d[3];
+  for (int k = 0; k < 3; ++k) d[k] = pi[k] - (pj[k] + sh[k]);
   const float r2 = fmaf(d[2], d[2], fmaf(d[1], d[1], d[0] * d[0]));
   return r2 > 0.0f && r2 < H2;
 }
@@ -234,38 +239,35 @@ static inline float support2(const orc_config* cfg) {
   return H * H;
 }
 
-/* Visit the in-support neighbours of i in ascending j order. */
-typedef void (*visit_fn)(int i, int j, const float d[3], void* ctx);
-
 static int cmp_int(const void* a, const void* b) { return (*(const int*)a > *(const int*)b) - (*(const int*)a < *(const int*)b); }
 
+/* Encoded in-support neighbours of i, ascending j. */
 static int gather_neighbors(int i, const float* pos4, const orc_config* cfg, const cell_table* T, float H2, int* buf,
                             int cap) {
-  const int nx = cfg->ncell[0], ny = cfg->ncell[1], nz = cfg->ncell[2];
+  const int nc[3] = {cfg->ncell[0], cfg->ncell[1], cfg->ncell[2]};
+  float L[3];
+  for (int k = 0; k < 3; ++k) L[k] = cfg->hi[k] - cfg->lo[k];
   int m = 0;
   const int* c = T->cxyz[i];
-  int seen[27], nseen = 0;
   for (int dz = -1; dz <= 1; ++dz)
     for (int dy = -1; dy <= 1; ++dy)
       for (int dx = -1; dx <= 1; ++dx) {
-        int x = c[0] + dx, y = c[1] + dy, z = c[2] + dz;
-        if (cfg->periodic) {
-          x = (x + nx) % nx;
-          y = (y + ny) % ny;
-          z = (z + nz) % nz;
-        } else if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) {
-          continue;
+        int q[3] = {c[0] + dx, c[1] + dy, c[2] + dz}, s[3] = {0, 0, 0};
+        int skip = 0;
+        for (int k = 0; k < 3; ++k) {
+          if (q[k] < 0 || q[k] >= nc[k]) {
+            if (!cfg->periodic) skip = 1;
+            else if (q[k] < 0) q[k] += nc[k], s[k] = -1;
+            else q[k] -= nc[k], s[k] = 1;
+          }
         }
-        const int lin = (z * ny + y) * nx + x;
-        int dup = 0;
-        for (int s = 0; s < nseen; ++s) dup |= seen[s] == lin;
-        if (dup) continue;
-        seen[nseen++] = lin;
+        if (skip) continue;
+        const float sh[3] = {s[0] * L[0], s[1] * L[1], s[2] * L[2]};
+        const int lin = (q[2] * nc[1] + q[1]) * nc[0] + q[0];
         for (int p = T->start[lin]; p < T->start[lin + 1]; ++p) {
           const int j = T->idx[p];
-          float d[3];
-          if (in_support(&pos4[4 * i], &pos4[4 * j], cfg, H2, d)) {
-            if (m < cap) buf[m] = j;
+          if (in_support(&pos4[4 * i], &pos4[4 * j], sh, H2)) {
+            if (m < cap) buf[m] = ENC(j, s[0], s[1], s[2]);
             ++m;
           }
         }
@@ -291,33 +293,26 @@ int64_t orc_neighbors(int n, const float* pos4, const orc_config* cfg, int32_t* 
     if (list) {
       if (m > cap || m > NB_CAP) overflow = 1;
       const int mm = m < cap ? m : cap;
-      for (int k = 0; k < mm && k < NB_CAP; ++k) list[(int64_t)i * cap + k] = buf[k];
+      for (int k = 0; k < mm && k < NB_CAP; ++k) list[(int64_t)i * cap + k] = ent_j(buf[k]);
     }
   }
   table_free(&T);
   return overflow ? -1 : total;
 }
 
-/* Periodic image offset (0 or +-L per axis) that the FP32 wrap chose for the
- * pair (i, j): the FP64 displacement is then  x_i - x_j + off. */
-static inline void image_offset(const float* pi, const float* pj, const orc_config* cfg, double off[3]) {
-  for (int a = 0; a < 3; ++a) {
-    off[a] = 0.0;
-    if (cfg->periodic) {
-      const float L = cfg->hi[a] - cfg->lo[a];
-      const float draw = pi[a] - pj[a];
-      const float df = wrap_d(draw, L, 0.5f * L);
-      const double Ld = (double)cfg->hi[a] - (double)cfg->lo[a];
-      if (df != draw) off[a] = (df < draw) ? -Ld : Ld;
-    }
-  }
+/* Image offset s L (FP64) of a neighbour entry. */
+static inline void image_offset(int e, const orc_config* cfg, double off[3]) {
+  int s[3];
+  ent_s(e, s);
+  for (int a = 0; a < 3; ++a) off[a] = s[a] * ((double)cfg->hi[a] - (double)cfg->lo[a]);
 }
 
-/* FP64 displacement i - j of the FP32 positions, with the chosen image. */
-static inline void disp64(const float* pi, const float* pj, const orc_config* cfg, double d[3]) {
+/* FP64 displacement x_i - (x_j + s L) of FP32 positions. */
+static inline void disp64(const float* pos4, int i, int e, const orc_config* cfg, double d[3]) {
   double off[3];
-  image_offset(pi, pj, cfg, off);
-  for (int a = 0; a < 3; ++a) d[a] = (double)pi[a] - (double)pj[a] + off[a];
+  image_offset(e, cfg, off);
+  const int j = ent_j(e);
+  for (int a = 0; a < 3; ++a) d[a] = (double)pos4[4 * i + a] - ((double)pos4[4 * j + a] + off[a]);
 }
 
 void orc_density(int n, const float* pos4, const float* dens_in, const orc_config* cfg, int shepard,
@@ -334,9 +329,9 @@ void orc_density(int n, const float* pos4, const float* dens_in, const orc_confi
     /* self term first (FDPS gather lists contain i itself, force.h:16-20) */
     double sum = m * W0, one = shepard ? m / (double)dens_in[i] * W0 : 0.0;
     for (int k = 0; k < cnt && k < NB_CAP; ++k) {
-      const int j = buf[k];
+      const int j = ent_j(buf[k]);
       double d[3];
-      disp64(&pos4[4 * i], &pos4[4 * j], cfg, d);
+      disp64(pos4, i, buf[k], cfg, d);
       const double W = orc_W(sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]), h);
       sum += m * W;
       if (shepard) one += m / (double)dens_in[j] * W;
@@ -359,9 +354,9 @@ void orc_hydro(int n, const float* pos4, const float* vel4, const float* dens, c
     pair_acc A = {{0, 0, 0}, 0, 0};
     const double rhoi = dens[i], poi = (double)pres[i] / (rhoi * rhoi);
     for (int k = 0; k < cnt && k < NB_CAP; ++k) {
-      const int j = buf[k];
+      const int j = ent_j(buf[k]);
       double dr[3], dv[3];
-      disp64(&pos4[4 * i], &pos4[4 * j], cfg, dr);
+      disp64(pos4, i, buf[k], cfg, dr);
       for (int a = 0; a < 3; ++a) dv[a] = (double)vel4[4 * i + a] - (double)vel4[4 * j + a];
       const double rhoj = dens[j];
       pair_term(&cfg->pair, dr, dv, h, h, rhoi, rhoj, poi, (double)pres[j] / (rhoj * rhoj), snds[i], snds[j], nu, nu,
@@ -412,10 +407,10 @@ static void force_pass(int n, const double* pos3, const double* vel3, double* de
     for (int i = 0; i < n; ++i) {
       double sum = m * W0, one = m / dens[i] * W0;
       for (int k = 0; k < cnts[i]; ++k) {
-        const int j = lists[(size_t)i * NB_CAP + k];
+        const int e = lists[(size_t)i * NB_CAP + k], j = ent_j(e);
         double d[3];
-        image_offset(&p4[4 * i], &p4[4 * j], cfg, d);
-        for (int a = 0; a < 3; ++a) d[a] += pos3[3 * i + a] - pos3[3 * j + a];
+        image_offset(e, cfg, d);
+        for (int a = 0; a < 3; ++a) d[a] = pos3[3 * i + a] - (pos3[3 * j + a] + d[a]);
         const double W = orc_W(sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]), h);
         sum += m * W;
         one += m / dens[j] * W;
@@ -433,11 +428,11 @@ static void force_pass(int n, const double* pos3, const double* vel3, double* de
     pair_acc A = {{0, 0, 0}, 0, 0};
     const double poi = pres[i] / (dens[i] * dens[i]);
     for (int k = 0; k < cnts[i]; ++k) {
-      const int j = lists[(size_t)i * NB_CAP + k];
+      const int e = lists[(size_t)i * NB_CAP + k], j = ent_j(e);
       double dr[3], dv[3];
-      image_offset(&p4[4 * i], &p4[4 * j], cfg, dr);
+      image_offset(e, cfg, dr);
       for (int a = 0; a < 3; ++a) {
-        dr[a] += pos3[3 * i + a] - pos3[3 * j + a];
+        dr[a] = pos3[3 * i + a] - (pos3[3 * j + a] + dr[a]);
         dv[a] = vel3[3 * i + a] - vel3[3 * j + a];
       }
       pair_term(&cfg->pair, dr, dv, h, h, dens[i], dens[j], poi, pres[j] / (dens[j] * dens[j]), snds[i], snds[j], nu,

@@ -13,6 +13,12 @@ from weaklycompressiblesph_b200.sim import Solver
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-5
+PRECISIONS = [N.PREC_FP32, N.PREC_TILED]
+
+
+@pytest.fixture(params=PRECISIONS, ids=["fp32", "tiled"])
+def prec(request):
+    return request.param
 
 
 def f32(a):
@@ -32,9 +38,9 @@ def oracle_forces(oracle_lib, case, pos, vel, dens):
 
 
 @pytest.mark.parametrize("which", ["dam", "periodic"])
-def test_order_and_neighbors_bit_exact(native, oracle_lib, which):
+def test_order_and_neighbors_bit_exact(prec, native, oracle_lib, which):
     case = small_dam(dx=0.04) if which == "dam" else cases.periodic_lattice(n_side=24, dx=0.01, seed=1)
-    with Solver(case.n + 16) as s:
+    with Solver(case.n + 16, precision=prec) as s:
         k = s.add(case, density_mode=N.DENSITY_CONTINUITY)
         perm, key = s.order(k)
         cfg = oracle_lib.config_from_case(case)
@@ -50,9 +56,9 @@ def test_order_and_neighbors_bit_exact(native, oracle_lib, which):
 
 
 @pytest.mark.parametrize("which", ["dam", "periodic"])
-def test_hydro_forces(native, oracle_lib, which):
+def test_hydro_forces(prec, native, oracle_lib, which):
     case = small_dam(dx=0.04) if which == "dam" else cases.periodic_lattice(n_side=24, dx=0.01, seed=2)
-    with Solver(case.n) as s:
+    with Solver(case.n, precision=prec) as s:
         k = s.add(case, density_mode=N.DENSITY_CONTINUITY)
         pr = s.probe(k)
         acc, dv, dt, cnt, _ = oracle_forces(oracle_lib, case, case.pos, case.vel, case.dens)
@@ -62,9 +68,9 @@ def test_hydro_forces(native, oracle_lib, which):
 
 
 @pytest.mark.parametrize("shepard", [0, 1])
-def test_density_pass(native, oracle_lib, shepard):
+def test_density_pass(prec, native, oracle_lib, shepard):
     case = small_dam(dx=0.04)
-    with Solver(case.n) as s:
+    with Solver(case.n, precision=prec) as s:
         k = s.add(case, density_mode=N.DENSITY_CONTINUITY)
         pr = s.probe(k, density_pass=2 if shepard else 1)
         cfg = oracle_lib.config_from_case(case)
@@ -72,10 +78,10 @@ def test_density_pass(native, oracle_lib, shepard):
         np.testing.assert_allclose(pr["dens"], ref, rtol=TOL)
 
 
-def test_initial_pass_matches_oracle(native, oracle_lib):
+def test_initial_pass_matches_oracle(prec, native, oracle_lib):
     """Initial force pass (main.cpp:69-78) incl. the Shepard filter and gravity."""
     case = small_dam(dx=0.04)
-    with Solver(case.n) as s:
+    with Solver(case.n, precision=prec) as s:
         k = s.add(case)
         st = s.read(k)
     cfg = oracle_lib.config_from_case(case)
@@ -90,13 +96,13 @@ def test_initial_pass_matches_oracle(native, oracle_lib):
 
 
 @pytest.mark.parametrize("mode", [N.DENSITY_SHEPARD, N.DENSITY_SUMMATION, N.DENSITY_CONTINUITY])
-def test_trajectory_vs_fp64(native, oracle_lib, mode):
+def test_trajectory_vs_fp64(prec, native, oracle_lib, mode):
     """20 device steps (graph) vs 20 FP64 oracle steps from the same start."""
     case = small_dam(dx=0.04, vel_sigma=0.05)
     case.phys.density_mode = mode
     case.phys.shepard_interval = 7
     nsteps = 20
-    with Solver(case.n) as s:
+    with Solver(case.n, precision=prec) as s:
         k = s.add(case)
         s.step(nsteps)
         st = s.read(k)
@@ -118,26 +124,26 @@ def test_trajectory_vs_fp64(native, oracle_lib, mode):
     np.testing.assert_allclose(st["dens"], o["dens"], rtol=1e-5)
 
 
-def test_momentum_conservation_periodic(native):
+def test_momentum_conservation_periodic(prec, native):
     """Pair forces are antisymmetric: in a periodic box sum m a = 0."""
     case = cases.periodic_lattice(n_side=32, dx=0.01, seed=8)
-    with Solver(case.n) as s:
+    with Solver(case.n, precision=prec) as s:
         k = s.add(case, density_mode=N.DENSITY_CONTINUITY)
         pr = s.probe(k)
     tot = np.abs(pr["acc"]).sum(axis=0)
     assert np.all(np.abs(pr["acc"].sum(axis=0)) < 1e-5 * tot)
 
 
-def test_instances_independent(native):
+def test_instances_independent(prec, native):
     """An instance gives bit-identical results alone and in a mix."""
     a = small_dam(dx=0.05, seed=1)
     b = small_dam(dx=0.04, seed=2, column=(0.3, 0.4, 0.6))
     c = cases.periodic_lattice(n_side=16, dx=0.01, seed=3)
-    with Solver(a.n) as s:
+    with Solver(a.n, precision=prec) as s:
         k = s.add(a)
         s.step(15)
         alone = s.read(k)
-    with Solver(a.n + b.n + c.n, max_instances=4) as s:
+    with Solver(a.n + b.n + c.n, max_instances=4, precision=prec) as s:
         kb = s.add(b)
         s.step(3)
         ka = s.add(a)
@@ -149,10 +155,10 @@ def test_instances_independent(native):
         np.testing.assert_array_equal(alone[key], mix[key])
 
 
-def test_remove_and_reuse_slot(native):
+def test_remove_and_reuse_slot(prec, native):
     a = small_dam(dx=0.05, seed=1)
     b = small_dam(dx=0.05, seed=2)
-    with Solver(a.n + b.n, max_instances=2) as s:
+    with Solver(a.n + b.n, max_instances=2, precision=prec) as s:
         ka = s.add(a)
         kb = s.add(b)
         s.step(2)
@@ -167,14 +173,14 @@ def test_remove_and_reuse_slot(native):
             s.add(b)  # capacity exhausted
 
 
-def test_escapees_removed(native):
+def test_escapees_removed(prec, native):
     """HYDRO particles outside the kill box are removed (Dam2.h:117-122)."""
     case = small_dam(dx=0.05, vel_sigma=0.0)
     fluid = np.nonzero(case.type == N.HYDRO)[0]
     fluid = fluid[np.argsort(-case.pos[fluid, 2], kind="stable")]  # top surface first
     case.vel[fluid[:5]] = [0.0, 0.0, 200.0]
     case.kill_hi = (case.kill_hi[0], case.kill_hi[1], 1.2)
-    with Solver(case.n) as s:
+    with Solver(case.n, precision=prec) as s:
         k = s.add(case)
         s.step(40)
         st = s.read(k)
@@ -183,9 +189,9 @@ def test_escapees_removed(native):
     assert st["alive"].sum() == case.n - 5
 
 
-def test_t_end_finishes(native):
+def test_t_end_finishes(prec, native):
     case = small_dam(dx=0.05)
-    with Solver(case.n) as s:
+    with Solver(case.n, precision=prec) as s:
         k = s.add(case, t_end=2e-3)
         s.step(200)
         st = s.status(k)
@@ -195,7 +201,7 @@ def test_t_end_finishes(native):
 
 def test_invalid_configs(native):
     case = cases.periodic_lattice(n_side=4, dx=0.01)  # box of 0.04 < 3 cells of 2h
-    with Solver(case.n) as s:
+    with Solver(case.n, precision=prec) as s:
         with pytest.raises(N.WcsphError):
             s.add(case)
     with pytest.raises(N.WcsphError):

@@ -46,6 +46,8 @@ struct SimImpl {
   InstDyn* d_dyn = nullptr;
   int* d_phase = nullptr;
   int* d_n_alive = nullptr;
+  int* run_list = nullptr;
+  int* d_counters = nullptr;  // [0] run_count, [1] work_counter
   unsigned long long* d_pairs = nullptr;
   double* d_cons = nullptr;
   float4* diag_acc = nullptr;
@@ -85,7 +87,8 @@ static size_t per_particle_bytes() {
   return 2 * (4 * sizeof(float4) + sizeof(int) + sizeof(uint32_t))  // main + alt state
          + 2 * (sizeof(uint32_t) + sizeof(int))                     // sort keys/values in/out
          + 2 * sizeof(float4) + 2 * sizeof(float)                   // jA, jB, jC, rho_new
-         + sizeof(float4) + 2 * sizeof(float) + sizeof(int);        // diagnostics
+         + sizeof(float4) + 2 * sizeof(float) + sizeof(int)         // diagnostics
+         + sizeof(int);                                             // non-empty cell list
 }
 
 static int64_t device_bytes(const wcsph_sim_options& o) {
@@ -156,6 +159,9 @@ static StepArgs make_args(SimImpl& S) {
   a.n_host = S.n_host;
   a.n_inst = (int)S.inst.size();
   a.pair_count = S.d_pairs;
+  a.run_list = S.run_list;
+  a.run_count = S.d_counters;
+  a.work_counter = S.d_counters + 1;
   a.diag_acc = S.diag_acc;
   a.diag_dt = S.diag_dt;
   a.diag_nbr = S.diag_nbr;
@@ -186,6 +192,7 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
       WCSPH_CUDA(cudaMemsetAsync(S.cell_start, 0, sizeof(int) * S.total_cells, S.s));
       WCSPH_CUDA(cudaMemsetAsync(S.cell_end, 0, sizeof(int) * S.total_cells, S.s));
     }
+    WCSPH_CUDA(cudaMemsetAsync(S.d_counters, 0, 2 * sizeof(int), S.s));
     k_permute<<<nblk(n), kBlock, 0, S.s>>>(a);
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));
@@ -381,6 +388,8 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
   rc |= alloc(S, (void**)&S.d_dyn, (size_t)opt->max_instances * sizeof(InstDyn));
   rc |= alloc(S, (void**)&S.d_phase, (size_t)opt->max_instances * sizeof(int));
   rc |= alloc(S, (void**)&S.d_n_alive, sizeof(int));
+  rc |= alloc(S, (void**)&S.run_list, N * sizeof(int));
+  rc |= alloc(S, (void**)&S.d_counters, 4 * sizeof(int));
   rc |= alloc(S, (void**)&S.d_pairs, sizeof(unsigned long long));
   rc |= alloc(S, (void**)&S.d_cons, 8 * sizeof(double));
   S.cub_bytes = cub_sort_bytes((long long)N);

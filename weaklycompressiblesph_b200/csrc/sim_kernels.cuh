@@ -35,6 +35,9 @@ struct StepArgs {
   int n_host;             // particle slots in use (upper bound of live)
   int n_inst;
   unsigned long long* pair_count;
+  int* run_list;          // linear index of every non-empty cell (unordered)
+  int* run_count;         // number of entries in run_list
+  int* work_counter;      // cells taken so far by the persistent tiled kernels
   int init_filter;        // initial-pass Shepard filter launch (main.cpp:75)
   int probe_density;      // density pass of a probe launch: 0 none, 1 summation, 2 Shepard
   // diagnostics (probe phase)
@@ -164,7 +167,10 @@ __global__ void k_permute(StepArgs a) {
   const uint32_t local = key - P.key_base;
   const int cx = compact3(local), cy = compact3(local >> 1), cz = compact3(local >> 2);
   const int lin = P.cell_base + (cz * P.ncell[1] + cy) * P.ncell[0] + cx;
-  if (p == 0 || kprev != key) a.cell_start[lin] = p;
+  if (p == 0 || kprev != key) {
+    a.cell_start[lin] = p;
+    a.run_list[atomicAdd(a.run_count, 1)] = lin;
+  }
   if (knext != key) a.cell_end[lin] = p + 1;
   // instance ranges (keys are instance-major, so each instance is contiguous)
   if (p == 0 || kprev == kDeadKey || (int)(a.main.flags[a.vals_out[p - 1]] & kInstMask) != inst)
@@ -209,28 +215,25 @@ __device__ __forceinline__ void for_each_neighbor(const StepArgs& a, const InstP
   const int cz = cell_of(zi, P.lo[2], P.inv_cell[2], P.ncell[2]);
   const float H2 = P.H2;
   for (int oz = -1; oz <= 1; ++oz) {
-    int z = cz + oz;
-    if (P.periodic) z = z < 0 ? z + P.ncell[2] : (z >= P.ncell[2] ? z - P.ncell[2] : z);
-    else if (z < 0 || z >= P.ncell[2]) continue;
+    int z;
+    float sz;
+    if (!neighbor_cell(P, 2, cz + oz, z, sz)) continue;
     for (int oy = -1; oy <= 1; ++oy) {
-      int y = cy + oy;
-      if (P.periodic) y = y < 0 ? y + P.ncell[1] : (y >= P.ncell[1] ? y - P.ncell[1] : y);
-      else if (y < 0 || y >= P.ncell[1]) continue;
+      int y;
+      float sy;
+      if (!neighbor_cell(P, 1, cy + oy, y, sy)) continue;
       const int row = P.cell_base + (z * P.ncell[1] + y) * P.ncell[0];
       for (int ox = -1; ox <= 1; ++ox) {
-        int x = cx + ox;
-        if (P.periodic) x = x < 0 ? x + P.ncell[0] : (x >= P.ncell[0] ? x - P.ncell[0] : x);
-        else if (x < 0 || x >= P.ncell[0]) continue;
+        int x;
+        float sx;
+        if (!neighbor_cell(P, 0, cx + ox, x, sx)) continue;
         const int lin = row + x;
         const int s = a.cell_start[lin], e = a.cell_end[lin];
         for (int q = s; q < e; ++q) {
           const float4 J = __ldg(&a.jA[q]);
-          float dx = xi - J.x, dy = yi - J.y, dz = zi - J.z;
-          if (P.periodic) {
-            dx = wrap_d(dx, P.L[0], P.halfL[0]);
-            dy = wrap_d(dy, P.L[1], P.halfL[1]);
-            dz = wrap_d(dz, P.L[2], P.halfL[2]);
-          }
+          const float dx = __fsub_rn(xi, __fadd_rn(J.x, sx));
+          const float dy = __fsub_rn(yi, __fadd_rn(J.y, sy));
+          const float dz = __fsub_rn(zi, __fadd_rn(J.z, sz));
           const float r2 = dist2(dx, dy, dz);
           if (r2 > 0.0f && r2 < H2) body(q, J, dx, dy, dz, r2);
         }
@@ -295,6 +298,61 @@ __device__ __forceinline__ void dt_min(InstDyn* dyn, int inst, float v, bool val
   }
 }
 
+// Epilogue shared by the hydro kernels: finish particle p from its pair sums
+// (acc sums without the mass factor, sum g (dr.dv), v_sig, pair count).
+// Adds gravity to every particle (Dam2.h:104-108), does the final kick of
+// HYDRO particles (class.h:160-163), the density floor (Dam2.h:111), and
+// folds the CFL limits of integral.h:2-12 into dt_cand.  Writes main[p].
+__device__ __forceinline__ void finish_hydro(const StepArgs& a, int p, const InstParams& P, int inst, int ph,
+                                             uint32_t f, float ax, float ay, float az, float dsum, float vsig,
+                                             unsigned cnt, float& dt_cand, bool& dt_valid) {
+  float4 x = a.alt.pos[p];
+  float4 v = a.alt.vel[p];
+  float4 acc;
+  const float rho_i = a.jB[p].w, ci = a.jC[p];
+  const float m = P.mass, h = P.h;
+  ax *= m;
+  ay *= m;
+  az *= m;
+  const float divv = -m * dsum / rho_i;
+  const float dt_i = P.c_cfl * h / (ci + vsig);
+  if (ph == PH_PROBE) {
+    a.diag_acc[p] = make_float4(ax, ay, az, divv);
+    a.diag_dt[p] = dt_i;
+    a.diag_nbr[p] = (int)cnt;
+    a.diag_rho[p] = rho_i;
+    acc = a.alt.acc[p];
+  } else {
+    az -= P.g;
+    if (!(f & kFreezeBit)) {
+      const float amag = sqrtf(ax * ax + ay * ay + az * az);
+      const float c = fminf(fminf(dt_i, 0.25f * sqrtf(h / amag)), P.dt_nu);
+      dt_cand = dt_valid ? fminf(dt_cand, c) : c;
+      dt_valid = true;
+      if (ph == PH_STEP) {
+        const float hdt = 0.5f * a.dyn[inst].dt_cur;
+        const float4 vh = a.alt.vh[p];
+        v = make_float4(vh.x + hdt * ax, vh.y + hdt * ay, vh.z + hdt * az, 0.f);
+      }
+    }
+    acc = make_float4(ax, ay, az, divv);
+    x.w = fmaxf(x.w, P.rho_floor);
+  }
+  a.main.pos[p] = x;
+  a.main.vel[p] = v;
+  a.main.acc[p] = acc;
+  a.main.pid[p] = a.alt.pid[p];
+  a.main.flags[p] = f;
+}
+
+__device__ __forceinline__ void copy_state(const StepArgs& a, int p) {
+  a.main.pos[p] = a.alt.pos[p];
+  a.main.vel[p] = a.alt.vel[p];
+  a.main.acc[p] = a.alt.acc[p];
+  a.main.pid[p] = a.alt.pid[p];
+  a.main.flags[p] = a.alt.flags[p];
+}
+
 // ------------------------------------------------------------ hydro pass
 // One thread per i-particle (the plain FP32 path).  Restates force.h:38-57
 // for uniform h, m, nu within an instance:
@@ -317,9 +375,6 @@ __global__ void __launch_bounds__(256) k_hydro_plain(StepArgs a) {
     inst = f & kInstMask;
     const InstParams& P = a.params[inst];
     const int ph = a.phase[inst];
-    float4 x = a.alt.pos[p];
-    float4 v = a.alt.vel[p];
-    float4 acc = a.alt.acc[p];
     if (wants_force(P, a.dyn[inst], ph)) {
       const float4 I = a.jA[p];
       const float4 IB = a.jB[p];
@@ -348,39 +403,10 @@ __global__ void __launch_bounds__(256) k_hydro_plain(StepArgs a) {
         az += visc * dvz - pg * dz;
         dsum += g * drdv;
       });
-      const float m = P.mass;
-      ax *= m;
-      ay *= m;
-      az *= m;
-      const float divv = -m * dsum / rho_i;
-      const float dt_i = P.c_cfl * h / (ci + vsig);
-      if (ph == PH_PROBE) {
-        a.diag_acc[p] = make_float4(ax, ay, az, divv);
-        a.diag_dt[p] = dt_i;
-        a.diag_nbr[p] = (int)cnt;
-        a.diag_rho[p] = rho_i;
-      } else {
-        az -= P.g;
-        const bool hydro = !(f & kFreezeBit);
-        if (hydro) {
-          const float amag = sqrtf(ax * ax + ay * ay + az * az);
-          dt_cand = fminf(fminf(dt_i, 0.25f * sqrtf(h / amag)), P.dt_nu);
-          dt_valid = true;
-          if (ph == PH_STEP) {
-            const float hdt = 0.5f * a.dyn[inst].dt_cur;
-            const float4 vh = a.alt.vh[p];
-            v = make_float4(vh.x + hdt * ax, vh.y + hdt * ay, vh.z + hdt * az, 0.f);
-          }
-        }
-        acc = make_float4(ax, ay, az, divv);
-        x.w = fmaxf(x.w, P.rho_floor);
-      }
+      finish_hydro(a, p, P, inst, ph, f, ax, ay, az, dsum, vsig, cnt, dt_cand, dt_valid);
+    } else {
+      copy_state(a, p);
     }
-    a.main.pos[p] = x;
-    a.main.vel[p] = v;
-    a.main.acc[p] = acc;
-    a.main.pid[p] = a.alt.pid[p];
-    a.main.flags[p] = f;
   }
   dt_min(a.dyn, inst, dt_cand, dt_valid);
   if (COUNT) {

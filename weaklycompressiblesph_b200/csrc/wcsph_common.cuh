@@ -62,12 +62,10 @@ __device__ __forceinline__ int cell_of(float x, float lo, float inv, int n) {
   return c < 0 ? 0 : (c >= n ? n - 1 : c);
 }
 
-// FP32 minimum image on one axis.
-__device__ __forceinline__ float wrap_d(float d, float L, float halfL) {
-  if (d > halfL) d = __fsub_rn(d, L);
-  else if (d < -halfL) d = __fadd_rn(d, L);
-  return d;
-}
+// Periodic images: a candidate j visited through a neighbour cell whose index
+// wrapped past the box edge on an axis is taken at x_j + s L (s = +1 past the
+// high edge, -1 past the low edge); the displacement is x_i - (x_j + s L),
+// two rounded FP32 operations.  The oracle uses the same convention.
 
 // Squared distance as the neighbour predicate defines it.
 __device__ __forceinline__ float dist2(float dx, float dy, float dz) {
@@ -113,6 +111,24 @@ constexpr uint32_t kInstMask = 0xffffu;
 constexpr uint32_t kFreezeBit = 1u << 16;
 constexpr uint32_t kDeadBit = 1u << 17;
 constexpr uint32_t kDeadKey = 0xffffffffu;
+
+// Neighbour cell q (may be out of range by one) on axis k: wrapped index and
+// image shift s L; false when it lies outside a non-periodic grid.
+__device__ __forceinline__ bool neighbor_cell(const InstParams& P, int k, int q, int& out, float& shift) {
+  shift = 0.0f;
+  if (q < 0) {
+    if (!P.periodic) return false;
+    out = q + P.ncell[k];
+    shift = -P.L[k];
+  } else if (q >= P.ncell[k]) {
+    if (!P.periodic) return false;
+    out = q - P.ncell[k];
+    shift = P.L[k];
+  } else {
+    out = q;
+  }
+  return true;
+}
 
 // Tait EoS (EoS.h:75-90).  x = rho/rho0.
 __device__ __forceinline__ void tait(const InstParams& P, float rho, float& pres, float& snds) {
