@@ -201,7 +201,7 @@ def test_t_end_finishes(prec, native):
 
 def test_invalid_configs(native):
     case = cases.periodic_lattice(n_side=4, dx=0.01)  # box of 0.04 < 3 cells of 2h
-    with Solver(case.n, precision=prec) as s:
+    with Solver(case.n) as s:
         with pytest.raises(N.WcsphError):
             s.add(case)
     with pytest.raises(N.WcsphError):

@@ -4,19 +4,24 @@
 //      candidate list; their j-records (x, y, z pre-shifted by the periodic
 //      image, P/rho^2) are staged into the warp's shared-memory tile with
 //      coalesced loads (a cell's particles are contiguous after the sort).
-//   2. For every i of the cell (two at a time) the warp scans the tile with
-//      one candidate per lane, evaluates the FP32 support predicate, and
-//      ballot-compacts the in-support candidates into a per-i queue.
-//   3. The queue is consumed 32 pairs at a time (dense lanes, no predicate
-//      divergence); velocities, densities and sound speeds of those j are
-//      gathered from global memory by index (they lie in a few contiguous
-//      runs, so the loads coalesce well); partial sums are reduced with warp
-//      shuffles and accumulated per i in shared memory.
-//   4. Lane l finishes i = batch + l: gravity, final kick, density floor,
-//      next-dt fold, state write (the same epilogue as the plain kernel).
+//   2. The cell's i-particles are taken two at a time.  The warp scans the
+//      tile with one candidate per lane and evaluates the FP32 support
+//      predicate for both i in packed f32x2 arithmetic (bit-identical to the
+//      scalar predicate), then ballot-compacts the in-support candidates into
+//      one queue per i.
+//   3. The two queues are consumed together, lane k taking pair k of each
+//      queue (dense lanes, no predicate divergence), with the pair terms of
+//      the two i-particles evaluated in packed f32x2 arithmetic; j velocities,
+//      densities and sound speeds are gathered from global memory by index
+//      (a few contiguous runs, so the loads coalesce).  Partial sums are
+//      combined with a butterfly reduce-scatter (9 shuffles for 8 sums) and
+//      accumulated per i in shared memory.
+//   4. Lane l finishes i = batch + l with the epilogue shared with the plain
+//      kernel (gravity, final kick, density floor, next-dt fold, state write).
 // Work is distributed dynamically: warps take cells from the list of
 // non-empty cells through a global counter (persistent grid).
 #pragma once
+#include "f32x2.cuh"
 #include "sim_kernels.cuh"
 
 namespace wcsph {
@@ -37,64 +42,112 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
-__device__ __forceinline__ float warp_sum(float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
 __device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
 
-// Sum the pair terms of one i over its compacted queue (lane-strided) and
-// add the warp totals into res (ax, ay, az, sum g drdv, v_sig, count).
-__device__ __forceinline__ void hydro_queue(const StepArgs& a, const InstParams& P, int i, const float4& I,
-                                            const unsigned short* q, int nq, const float4* tp, const int* tg,
-                                            float* res, int lane) {
-  const float4 IB = __ldg(&a.jB[i]);
-  const float ci = __ldg(&a.jC[i]);
-  const float rho_i = IB.w, po_i = I.w;
-  const float h = P.h, eh2 = P.eh2, Kg = P.Kg, iH = P.inv_H, alpha = P.alpha, beta = P.beta, nu4 = P.nu4;
-  const int vs = P.vsig_mode;
-  float ax = 0.f, ay = 0.f, az = 0.f, dsum = 0.f, vsig = 0.f;
-  for (int k = lane; k < nq; k += 32) {
-    const int t = q[k];
-    const float4 J = tp[t];
-    const int g = tg[t];
-    const float4 JB = __ldg(&a.jB[g]);
-    const float cj = __ldg(&a.jC[g]);
-    const float dx = __fsub_rn(I.x, J.x), dy = __fsub_rn(I.y, J.y), dz = __fsub_rn(I.z, J.z);
-    const float r2 = dist2(dx, dy, dz);
-    const float rinv = rsqrtf(r2);
-    const float gr = spline_F(r2 * rinv * iH) * Kg * rinv;
-    const float dvx = IB.x - JB.x, dvy = IB.y - JB.y, dvz = IB.z - JB.z;
-    const float drdv = dx * dvx + dy * dvy + dz * dvz;
-    const float rden = __frcp_rn(r2 + eh2);
-    const float mu = drdv < 0.0f ? h * drdv * rden : 0.0f;
-    const float rs = __frcp_rn(rho_i + JB.w);
-    const float av = (beta * mu - alpha * 0.5f * (ci + cj)) * mu * 2.0f * rs;
-    vsig = vs ? fmaxf(vsig, -mu) : fmaxf(vsig, mu);
-    const float pg = (po_i + J.w + av) * gr;
-    const float visc = nu4 * gr * r2 * rs * rden;
-    ax += visc * dvx - pg * dx;
-    ay += visc * dvy - pg * dy;
-    az += visc * dvz - pg * dz;
-    dsum += gr * drdv;
+// Butterfly reduce-scatter of 8 per-lane sums: returns, in every lane, the
+// warp total of slot ((lane >> 2) & 7).  9 shuffles instead of 40.
+__device__ __forceinline__ float butterfly8(const float v[8], int lane) {
+  const unsigned full = 0xffffffffu;
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+  float w[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float send = b4 ? v[k] : v[k + 4];
+    const float keep = b4 ? v[k + 4] : v[k];
+    w[k] = keep + __shfl_xor_sync(full, send, 16);
   }
-  ax = warp_sum(ax);
-  ay = warp_sum(ay);
-  az = warp_sum(az);
-  dsum = warp_sum(dsum);
-  vsig = warp_max(vsig);
+  float x[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const float send = b3 ? w[k] : w[k + 2];
+    const float keep = b3 ? w[k + 2] : w[k];
+    x[k] = keep + __shfl_xor_sync(full, send, 8);
+  }
+  const float send = b2 ? x[0] : x[1];
+  float y = (b2 ? x[1] : x[0]) + __shfl_xor_sync(full, send, 4);
+  y += __shfl_xor_sync(full, y, 2);
+  y += __shfl_xor_sync(full, y, 1);
+  return y;
+}
+
+// Pair terms of i_a (low half) and i_b (high half) over their queues; adds
+// the warp totals into res[0] (i_a) and res[1] (i_b): ax, ay, az, sum g drdv,
+// v_sig, count.  Lanes past a queue's end contribute exactly zero.
+__device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParams& P, int ia, int ib, bool has_b,
+                                              const float4& IA, const float4& IBp, const unsigned short* qa, int na,
+                                              const unsigned short* qb, int nb, const float4* tp, const int* tg,
+                                              float (*res)[6], int lane) {
+  const float4 VA = __ldg(&a.jB[ia]), VB = __ldg(&a.jB[ib]);
+  const f2 X = pk(IA.x, IBp.x), Y = pk(IA.y, IBp.y), Z = pk(IA.z, IBp.z);
+  const f2 VX = pk(VA.x, VB.x), VY = pk(VA.y, VB.y), VZ = pk(VA.z, VB.z);
+  const f2 RHO = pk(VA.w, VB.w), PO = pk(IA.w, IBp.w);
+  const f2 CI = pk(__ldg(&a.jC[ia]), __ldg(&a.jC[ib]));
+  const float H2 = P.H2;
+  const f2 IH = dup(P.inv_H), KG = dup(P.Kg), EH2 = dup(P.eh2), HH = dup(P.h), NU4 = dup(P.nu4);
+  const f2 ONE = dup(1.0f), HALF = dup(0.5f), TWELVE = dup(12.0f), MTHREE = dup(-3.0f), TWO = dup(2.0f);
+  const f2 BETA = dup(P.beta), MHALPHA = dup(-0.5f * P.alpha), MONE = dup(-1.0f);
+  const int vs = P.vsig_mode;
+  const int nbq = has_b ? nb : 0;
+  const int n = max(na, nbq);
+  f2 AX = 0ull, AY = 0ull, AZ = 0ull, DS = 0ull;
+  float vsa = 0.f, vsb = 0.f;
+  for (int k = lane; k < n; k += 32) {
+    const bool va = k < na, vb = k < nbq;
+    const int ta = va ? qa[k] : 0, tb = vb ? qb[k] : 0;
+    const float4 Ja = tp[ta], Jb = tp[tb];
+    const int ga = tg[ta], gb = tg[tb];
+    const float4 JBa = __ldg(&a.jB[ga]), JBb = __ldg(&a.jB[gb]);
+    const f2 CJ = pk(__ldg(&a.jC[ga]), __ldg(&a.jC[gb]));
+    const f2 DX = sub2(X, pk(Ja.x, Jb.x)), DY = sub2(Y, pk(Ja.y, Jb.y)), DZ = sub2(Z, pk(Ja.z, Jb.z));
+    const f2 R2raw = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
+    const f2 R2 = pk(va ? lo(R2raw) : H2, vb ? hi(R2raw) : H2);  // finite stand-in for idle halves
+    const f2 W = pk(va ? 1.0f : 0.0f, vb ? 1.0f : 0.0f);
+    const f2 RINV = rsqrt2(R2);
+    const f2 S = mul2(mul2(R2, RINV), IH);
+    const f2 A = max0_2(sub2(ONE, S)), B = max0_2(sub2(HALF, S));
+    const f2 F = fma2(TWELVE, mul2(B, B), mul2(MTHREE, mul2(A, A)));  // 12 (1/2-s)+^2 - 3 (1-s)+^2
+    const f2 G = mul2(mul2(F, KG), mul2(RINV, W));                     // gradW = G * dr
+    const f2 DVX = sub2(VX, pk(JBa.x, JBb.x)), DVY = sub2(VY, pk(JBa.y, JBb.y)), DVZ = sub2(VZ, pk(JBa.z, JBb.z));
+    const f2 DRDV = fma2(DZ, DVZ, fma2(DY, DVY, mul2(DX, DVX)));
+    const f2 RDEN = rcp2(add2(R2, EH2));
+    const f2 MUr = mul2(mul2(DRDV, RDEN), HH);
+    const f2 MU = pk(va && lo(DRDV) < 0.0f ? lo(MUr) : 0.0f, vb && hi(DRDV) < 0.0f ? hi(MUr) : 0.0f);
+    const f2 RS = rcp2(add2(RHO, pk(JBa.w, JBb.w)));
+    const f2 AV = mul2(mul2(fma2(BETA, MU, mul2(MHALPHA, add2(CI, CJ))), MU), mul2(RS, TWO));
+    if (vs) {
+      vsa = fmaxf(vsa, -lo(MU));
+      vsb = fmaxf(vsb, -hi(MU));
+    } else {
+      vsa = fmaxf(vsa, lo(MU));
+      vsb = fmaxf(vsb, hi(MU));
+    }
+    const f2 NPG = mul2(mul2(add2(add2(PO, pk(Ja.w, Jb.w)), AV), G), MONE);
+    const f2 VISC = mul2(mul2(mul2(NU4, G), R2), mul2(RS, RDEN));
+    AX = fma2(NPG, DX, fma2(VISC, DVX, AX));
+    AY = fma2(NPG, DY, fma2(VISC, DVY, AY));
+    AZ = fma2(NPG, DZ, fma2(VISC, DVZ, AZ));
+    DS = fma2(G, DRDV, DS);
+  }
+  const float v8[8] = {lo(AX), lo(AY), lo(AZ), lo(DS), hi(AX), hi(AY), hi(AZ), hi(DS)};
+  const float y = butterfly8(v8, lane);
+  vsa = warp_max(vsa);
+  vsb = warp_max(vsb);
+  if ((lane & 3) == 0) {
+    const int slot = lane >> 2;
+    if (slot < 4) res[0][slot] += y;
+    else if (has_b) res[1][slot - 4] += y;
+  }
   if (lane == 0) {
-    res[0] += ax;
-    res[1] += ay;
-    res[2] += az;
-    res[3] += dsum;
-    res[4] = fmaxf(res[4], vsig);
-    res[5] += (float)nq;
+    res[0][4] = fmaxf(res[0][4], vsa);
+    res[0][5] += (float)na;
+    if (has_b) {
+      res[1][4] = fmaxf(res[1][4], vsb);
+      res[1][5] += (float)nb;
+    }
   }
 }
 
@@ -149,6 +202,7 @@ __global__ void __launch_bounds__(kTiledWarps * 32) k_hydro_tiled(StepArgs a) {
     }
     const int T = __shfl_sync(full, incl, 31);
     const int excl = incl - nb_cnt;
+    const unsigned nonempty = __ballot_sync(full, nb_cnt > 0);
     const float H2 = P.H2;
     float dt_cand = 0.f;
     bool dt_valid = false;
@@ -159,13 +213,14 @@ __global__ void __launch_bounds__(kTiledWarps * 32) k_hydro_tiled(StepArgs a) {
       for (int t0 = 0; t0 < T; t0 += kTile) {
         const int tn = min(kTile, T - t0);
         __syncwarp();
-        for (int k = 0; k < 27; ++k) {
+        for (unsigned m = nonempty; m; m &= m - 1) {
+          const int k = __ffs(m) - 1;
           const int ck = __shfl_sync(full, nb_cnt, k);
           const int sk = __shfl_sync(full, nb_start, k);
           const int ek = __shfl_sync(full, excl, k);
           const float sx = __shfl_sync(full, shx, k), sy = __shfl_sync(full, shy, k), sz = __shfl_sync(full, shz, k);
-          const int lo = max(ek, t0), hi = min(ek + ck, t0 + tn);
-          for (int u = lo + lane; u < hi; u += 32) {
+          const int lo_ = max(ek, t0), hi_ = min(ek + ck, t0 + tn);
+          for (int u = lo_ + lane; u < hi_; u += 32) {
             const int g = sk + (u - ek);
             const float4 J = __ldg(&a.jA[g]);
             tp[u - t0] = make_float4(__fadd_rn(J.x, sx), __fadd_rn(J.y, sy), __fadd_rn(J.z, sz), J.w);
@@ -179,14 +234,16 @@ __global__ void __launch_bounds__(kTiledWarps * 32) k_hydro_tiled(StepArgs a) {
           const int ibb = has_b ? ia + 1 : ia;
           const float4 IA = __ldg(&a.jA[ia]);
           const float4 IB = __ldg(&a.jA[ibb]);
+          const f2 X = pk(IA.x, IB.x), Y = pk(IA.y, IB.y), Z = pk(IA.z, IB.z);
           int na = 0, nb = 0;
           for (int tb = 0; tb < tn; tb += 32) {
             const int t = tb + lane;
             bool ina = false, inb = false;
             if (t < tn) {
               const float4 J = tp[t];
-              const float r2a = dist2(__fsub_rn(IA.x, J.x), __fsub_rn(IA.y, J.y), __fsub_rn(IA.z, J.z));
-              const float r2b = dist2(__fsub_rn(IB.x, J.x), __fsub_rn(IB.y, J.y), __fsub_rn(IB.z, J.z));
+              const f2 DX = sub2(X, dup(J.x)), DY = sub2(Y, dup(J.y)), DZ = sub2(Z, dup(J.z));
+              const f2 R2 = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));  // == dist2 per half
+              const float r2a = lo(R2), r2b = hi(R2);
               ina = r2a > 0.0f && r2a < H2;
               inb = has_b && r2b > 0.0f && r2b < H2;
             }
@@ -197,8 +254,7 @@ __global__ void __launch_bounds__(kTiledWarps * 32) k_hydro_tiled(StepArgs a) {
             nb += __popc(bb);
           }
           __syncwarp();
-          hydro_queue(a, P, ia, IA, qa, na, tp, tg, res[ii], lane);
-          if (has_b) hydro_queue(a, P, ibb, IB, qb, nb, tp, tg, res[ii + 1], lane);
+          hydro_queues2(a, P, ia, ibb, has_b, IA, IB, qa, na, qb, nb, tp, tg, &res[ii], lane);
           __syncwarp();
         }
       }
