@@ -362,7 +362,7 @@ __device__ __forceinline__ void copy_state(const StepArgs& a, int p) {
 // (class.h:160-163), the density floor (Dam2.h:111), and folds the CFL limits
 // of integral.h:2-12 into the instance's next dt.
 template <bool COUNT>
-__global__ void __launch_bounds__(256, 2) k_hydro_plain(StepArgs a) {
+__global__ void __launch_bounds__(256) k_hydro_plain(StepArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = *a.n_alive;
   const bool in = p < n;
