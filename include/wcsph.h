@@ -122,6 +122,28 @@ int wcsph_hydro_dispatch(int32_t tag, int32_t n_walk, const void* const* epi, co
  * writes acc, dt and div_v of n_i[w] RESULT records at force[w]. */
 int wcsph_hydro_retrieve(int32_t tag, int32_t n_walk, const int32_t* n_i, void* const* force);
 
+/* Allocation-free walk pair sum.  No counterpart in the reference: it is for
+ * callers that cannot allocate device memory (code running inside CUDA graph
+ * capture, hosts with a fixed device-memory budget or their own allocator).
+ * Everything is device-resident and caller-owned:
+ *   d_n_epi, d_n_epj  n_walk int32 walk sizes
+ *   d_epi             sum(n_epi) records of three float4:
+ *                     (x, y, z, h) (x relative to any origin shared by the walk),
+ *                     (vx, vy, vz, rho), (P/rho^2, c, nu, 0)
+ *   d_epj             sum(n_epj) records of three float4, the last (P/rho^2, c, nu, m)
+ *   d_out             sum(n_epi) results of two float4: (ax, ay, az, div_v), (dt, 0, 0, 0)
+ * with the pair variant of params, launched on `stream` (a cudaStream_t,
+ * NULL for the legacy stream).  The only scratch, the per-walk displacement
+ * tables, is a static device array of WCSPH_NOALLOC_MAX_WALKS walks (about
+ * 512 KB per GPU, kept until exit); larger n_walk returns WCSPH_E_CAPACITY.
+ * The first call on a device looks the array up (cudaGetSymbolAddress), so
+ * make that first call before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU (different streams, no ordering) race.
+ * Calls no cudaMalloc, cudaFree or allocating library routine. */
+#define WCSPH_NOALLOC_MAX_WALKS 65536
+int wcsph_hydro_walks_noalloc(int32_t n_walk, const int32_t* d_n_epi, const int32_t* d_n_epj, const void* d_epi,
+                              const void* d_epj, void* d_out, const wcsph_pair_params* params, void* stream);
+
 /* Shepard density filter in the same dispatch/retrieve shape (the reference
  * runs STD::ApplyFilter, src/force.h:10-30, on the CPU through
  * calcForceAllAndWriteBack; its Gather j-lists contain i itself). */

@@ -81,6 +81,7 @@ _SIGS = {
     "wcsph_fdps_configure": (C.c_int, [C.POINTER(FdpsLayout), C.POINTER(PairParams)]),
     "wcsph_hydro_dispatch": (C.c_int, [C.c_int32, C.c_int32, PP, I32P, PP, I32P]),
     "wcsph_hydro_retrieve": (C.c_int, [C.c_int32, C.c_int32, I32P, PP]),
+    "wcsph_hydro_walks_noalloc": (C.c_int, [C.c_int32, P, P, P, P, P, C.POINTER(PairParams), P]),
     "wcsph_filter_dispatch": (C.c_int, [C.c_int32, C.c_int32, PP, I32P, PP, I32P]),
     "wcsph_filter_retrieve": (C.c_int, [C.c_int32, C.c_int32, I32P, PP]),
     "wcsph_sim_create": (C.c_int, [C.POINTER(SimOptions), C.POINTER(C.c_void_p)]),

@@ -609,3 +609,197 @@ int wcsph_filter_retrieve(int32_t tag, int32_t n_walk, const int32_t* n_i, void*
   return retrieve_common(K_FILTER, tag, n_walk, n_i, result);
 }
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free walk pair sum.
+//
+// For callers that cannot allocate device memory: code running while a CUDA
+// graph is being captured (a cudaMalloc there breaks the capture), hosts that
+// hand the plugin a fixed memory budget and forbid growth, and embedders whose
+// allocator owns every device byte.  The caller passes device-resident inputs
+// and outputs; the only scratch this path needs, the per-walk displacement
+// tables (exclusive prefix sums of the walk sizes), lives in the file-scope
+// array below, sized for WCSPH_NOALLOC_MAX_WALKS walks (about 512 KB, held on
+// every GPU that loads the library until the process exits).
+namespace wcsph {
+
+static __device__ __align__(256) int g_noalloc_displ[2 * (WCSPH_NOALLOC_MAX_WALKS + 1)];
+
+// Exclusive prefix sums of the two count arrays into g_noalloc_displ-shaped
+// scratch: displ[0..n] for i-counts, displ[n+1 .. 2n+1] for j-counts.  One
+// block; every entry it later reads is written, so nothing needs clearing.
+__global__ void __launch_bounds__(1024) k_noalloc_displ(int n, const int* __restrict__ n_epi,
+                                                       const int* __restrict__ n_epj, int* displ) {
+  __shared__ int warp_tot[2][32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int per = (n + 1023) / 1024;
+  const int b = min(n, tid * per), e = min(n, b + per);
+  int si = 0, sj = 0;
+  for (int k = b; k < e; ++k) {
+    si += n_epi[k];
+    sj += n_epj[k];
+  }
+  int ii = si, ij = sj;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int ti = __shfl_up_sync(0xffffffffu, ii, o), tj = __shfl_up_sync(0xffffffffu, ij, o);
+    if (lane >= o) ii += ti, ij += tj;
+  }
+  if (lane == 31) warp_tot[0][warp] = ii, warp_tot[1][warp] = ij;
+  __syncthreads();
+  if (warp == 0) {
+    int wi = warp_tot[0][lane], wj = warp_tot[1][lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int ti = __shfl_up_sync(0xffffffffu, wi, o), tj = __shfl_up_sync(0xffffffffu, wj, o);
+      if (lane >= o) wi += ti, wj += tj;
+    }
+    warp_tot[0][lane] = wi;
+    warp_tot[1][lane] = wj;
+  }
+  __syncthreads();
+  int oi = ii - si + (warp > 0 ? warp_tot[0][warp - 1] : 0);
+  int oj = ij - sj + (warp > 0 ? warp_tot[1][warp - 1] : 0);
+  for (int k = b; k < e; ++k) {
+    displ[k] = oi;
+    displ[n + 1 + k] = oj;
+    oi += n_epi[k];
+    oj += n_epj[k];
+  }
+  if (tid == 1023) {
+    displ[n] = oi;
+    displ[2 * n + 1] = oj;
+  }
+}
+
+// The walk pair sum of k_walk_hydro with records interleaved per particle
+// (three float4 per record) and results as two float4 per i-particle.
+template <int VSIG, int GRAD>
+__global__ void __launch_bounds__(kWalkThreads) k_walk_hydro_interleaved(const float4* __restrict__ ei,
+                                                                        const float4* __restrict__ ej,
+                                                                        const int* __restrict__ displ, int n_walk,
+                                                                        WalkPair pp, float4* __restrict__ out) {
+  __shared__ float4 sA[kWalkTile], sB[kWalkTile], sC[kWalkTile];
+  const int w = blockIdx.x;
+  const int i0 = displ[w], i1 = displ[w + 1];
+  const int j0 = displ[n_walk + 1 + w], j1 = displ[n_walk + 2 + w];
+  for (int ib = i0; ib < i1; ib += kWalkThreads) {
+    const int i = ib + threadIdx.x;
+    const bool valid = i < i1;
+    float4 a = make_float4(0.f, 0.f, 0.f, 1.f), b = make_float4(0.f, 0.f, 0.f, 1.f), c = make_float4(0.f, 1.f, 0.f, 0.f);
+    if (valid) {
+      a = ei[3 * (size_t)i];
+      b = ei[3 * (size_t)i + 1];
+      c = ei[3 * (size_t)i + 2];
+    }
+    float ax = 0.f, ay = 0.f, az = 0.f, dv_acc = 0.f, vsig = 0.f;
+    for (int jb = j0; jb < j1; jb += kWalkTile) {
+      const int nt = min(kWalkTile, j1 - jb);
+      __syncthreads();
+      for (int k = threadIdx.x; k < nt; k += kWalkThreads) {
+        sA[k] = ej[3 * (size_t)(jb + k)];
+        sB[k] = ej[3 * (size_t)(jb + k) + 1];
+        sC[k] = ej[3 * (size_t)(jb + k) + 2];
+      }
+      __syncthreads();
+      if (!valid) continue;
+      for (int k = 0; k < nt; ++k) {
+        const float4 A = sA[k];
+        const float dx = a.x - A.x, dy = a.y - A.y, dz = a.z - A.z;
+        const float r2 = dist2(dx, dy, dz);
+        if (!(r2 > 0.0f)) continue;
+        const float4 B = sB[k];
+        const float hi = a.w, hj = A.w;
+        const float dvx = b.x - B.x, dvy = b.y - B.y, dvz = b.z - B.z;
+        const float drdv = dx * dvx + dy * dvy + dz * dvz;
+        const float den = r2 + pp.eps * hi * hj;
+        const float mu = drdv < 0.0f ? 0.5f * (hi + hj) * drdv / den : 0.0f;
+        vsig = VSIG ? fmaxf(vsig, -mu) : fmaxf(vsig, mu);
+        const float r = sqrtf(r2);
+        float g;
+        if (GRAD == WCSPH_GRAD_SYM) {
+          g = 0.0f;
+          if (r < 2.0f * hi) g += grad_factor(r, hi);
+          if (r < 2.0f * hj) g += grad_factor(r, hj);
+          g *= 0.5f;
+        } else {
+          const float hb = 0.5f * (hi + hj);
+          g = (r < 2.0f * hb) ? grad_factor(r, hb) : 0.0f;
+        }
+        if (g == 0.0f) continue;
+        const float4 C = sC[k];
+        const float rho_sum = b.w + B.w;
+        const float av = (-pp.alpha * 0.5f * (c.y + C.y) * mu + pp.beta * mu * mu) * 2.0f / rho_sum;
+        const float pterm = c.x + C.x + av;
+        const float visc = 2.0f * (c.z + C.z) * (g * r2) / rho_sum / den;
+        const float m = C.w;
+        ax += m * (visc * dvx - pterm * g * dx);
+        ay += m * (visc * dvy - pterm * g * dy);
+        az += m * (visc * dvz - pterm * g * dz);
+        dv_acc -= m * g * drdv;
+      }
+    }
+    if (valid) {
+      out[2 * (size_t)i] = make_float4(ax, ay, az, dv_acc / b.w);
+      out[2 * (size_t)i + 1] = make_float4(pp.c_cfl * a.w / (c.y + vsig), 0.f, 0.f, 0.f);
+    }
+  }
+}
+
+// Device address of the scratch array, looked up once per device.
+static int* g_noalloc_ptr[64];
+static std::mutex g_noalloc_mu;
+
+static int noalloc_scratch(int** out) {
+  int dev = 0;
+  WCSPH_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_error("wcsph_hydro_walks_noalloc: device ordinal %d is beyond the supported 64", dev);
+    return WCSPH_E_NODEVICE;
+  }
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_displ);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_displ)", __FILE__, __LINE__);
+    g_noalloc_ptr[dev] = (int*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return 0;
+}
+
+}  // namespace wcsph
+
+extern "C" int wcsph_hydro_walks_noalloc(int32_t n_walk, const int32_t* d_n_epi, const int32_t* d_n_epj,
+                                         const void* d_epi, const void* d_epj, void* d_out,
+                                         const wcsph_pair_params* params, void* stream) {
+  if (n_walk < 0 || !params) {
+    set_error("wcsph_hydro_walks_noalloc: n_walk %d < 0 or null params", n_walk);
+    return WCSPH_E_INVALID;
+  }
+  if (n_walk > WCSPH_NOALLOC_MAX_WALKS) {
+    set_error("wcsph_hydro_walks_noalloc: %d walks exceed the allocation-free limit of %d walks per call", n_walk,
+              WCSPH_NOALLOC_MAX_WALKS);
+    return WCSPH_E_CAPACITY;
+  }
+  if (params->vsig_mode < 0 || params->vsig_mode > 1 || params->grad_mode < 0 || params->grad_mode > 1) {
+    set_error("wcsph_hydro_walks_noalloc: bad vsig_mode/grad_mode");
+    return WCSPH_E_INVALID;
+  }
+  if (n_walk == 0) return 0;
+  if (!d_n_epi || !d_n_epj || !d_epi || !d_epj || !d_out) {
+    set_error("wcsph_hydro_walks_noalloc: null device pointer");
+    return WCSPH_E_INVALID;
+  }
+  int* displ = nullptr;
+  if (int rc = noalloc_scratch(&displ)) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  k_noalloc_displ<<<1, 1024, 0, s>>>(n_walk, d_n_epi, d_n_epj, displ);
+  const WalkPair pp{(float)params->alpha, (float)params->beta, (float)params->c_cfl, (float)params->eps,
+                    params->vsig_mode, params->grad_mode};
+  auto kern = pp.vsig_mode ? (pp.grad_mode ? k_walk_hydro_interleaved<1, 1> : k_walk_hydro_interleaved<1, 0>)
+                           : (pp.grad_mode ? k_walk_hydro_interleaved<0, 1> : k_walk_hydro_interleaved<0, 0>);
+  kern<<<n_walk, kWalkThreads, 0, s>>>((const float4*)d_epi, (const float4*)d_epj, displ, n_walk, pp, (float4*)d_out);
+  WCSPH_CUDA(cudaGetLastError());
+  return 0;
+}
