@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--workload", default="dam1m", choices=["dam1m", "dam16k", "periodic8m"])
     ap.add_argument("--precision", default="best", choices=["best", "fp32", "tiled", "half2"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison run")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
@@ -310,7 +311,7 @@ def main():
     value = pairs_all / (ms * 1e-3)
     steps_per_s = 1e3 / ms
     plain = None
-    if prec != "fp32":
+    if prec != "fp32" and not args.no_plain:
         p = run_device(case, "fp32", max(10, args.steps // 4), args.warmup, local)
         plain = {"value": p["pairs_per_step"] / (p["ms_per_step"] * 1e-3), "steps_per_s": 1e3 / p["ms_per_step"],
                  "ms_per_step": p["ms_per_step"]}
