@@ -1,21 +1,23 @@
 // Tiled pair kernels (WCSPH_PREC_TILED): one warp per non-empty cell.
 //
 //   1. The 27 neighbour cells of the warp's cell are flattened into one
-//      candidate list; their j-records (x, y, z pre-shifted by the periodic
-//      image, P/rho^2) are staged into the warp's shared-memory tile with
-//      coalesced loads (a cell's particles are contiguous after the sort).
-//   2. The cell's i-particles are taken two at a time.  The warp scans the
-//      tile with one candidate per lane and evaluates the FP32 support
-//      predicate for both i in packed f32x2 arithmetic (bit-identical to the
-//      scalar predicate), then ballot-compacts the in-support candidates into
-//      one queue per i.
+//      candidate list and staged into the warp's shared-memory tile as
+//      structure-of-arrays x[], y[], z[] (pre-shifted by the periodic image)
+//      and e[] (global slot | image code << 27), with coalesced loads (a
+//      cell's particles are contiguous after the sort).
+//   2. The cell's i-particles are taken two at a time.  Each lane tests two
+//      adjacent candidates against both i: one 64-bit shared load yields the
+//      candidate pair already packed, and the four FP32 support predicates are
+//      evaluated with packed f32x2 arithmetic (bit-identical to the scalar
+//      predicate).  In-support candidates are ballot-compacted into one queue
+//      per i.
 //   3. The two queues are consumed together, lane k taking pair k of each
-//      queue (dense lanes, no predicate divergence), with the pair terms of
-//      the two i-particles evaluated in packed f32x2 arithmetic; j velocities,
-//      densities and sound speeds are gathered from global memory by index
-//      (a few contiguous runs, so the loads coalesce).  Partial sums are
-//      combined with a butterfly reduce-scatter (9 shuffles for 8 sums) and
-//      accumulated per i in shared memory.
+//      queue (dense lanes, no predicate divergence), with the pair terms of the
+//      two i-particles evaluated in packed f32x2 arithmetic; j records are
+//      gathered from global memory by the slot in the queue entry (a few
+//      contiguous runs, so the loads coalesce).  Partial sums are combined
+//      with a butterfly reduce-scatter (9 shuffles for 8 sums) and accumulated
+//      per i in shared memory.
 //   4. Lane l finishes i = batch + l with the epilogue shared with the plain
 //      kernel (gravity, final kick, density floor, next-dt fold, state write).
 // Work is distributed dynamically: warps take cells from the list of
@@ -27,13 +29,15 @@
 namespace wcsph {
 
 constexpr int kTiledWarps = 4;
-constexpr int kTile = 512;
+constexpr int kTile = 512;                 // candidates staged per pass (multiple of 64)
+constexpr uint32_t kSlotMask = (1u << 27) - 1;
+constexpr int kMaxTiledParticles = 1 << 27;  // queue entries hold the slot in 27 bits
 
 struct TiledSmem {
-  float4 pos[kTiledWarps][kTile];                // staged j: shifted x, y, z and P/rho^2
-  int gidx[kTiledWarps][kTile];                  // global slot of each staged j
-  unsigned short q[kTiledWarps][2][kTile];       // per-i compacted candidate queues
-  float res[kTiledWarps][32][6];                 // per-i accumulators of the current batch
+  float x[kTiledWarps][kTile], y[kTiledWarps][kTile], z[kTiledWarps][kTile];  // staged candidates
+  uint32_t e[kTiledWarps][kTile];            // slot | image code << 27
+  uint32_t q[kTiledWarps][2][kTile];         // per-i compacted queues of entries
+  float res[kTiledWarps][32][6];             // per-i accumulators of the current batch
 };
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -74,13 +78,19 @@ __device__ __forceinline__ float butterfly8(const float v[8], int lane) {
   return y;
 }
 
+// Image shift of a queue entry's code ((sx+1) + 3 (sy+1) + 9 (sz+1)).
+__device__ __forceinline__ void entry_shift(const InstParams& P, uint32_t code, float& sx, float& sy, float& sz) {
+  sx = (float)((int)(code % 3u) - 1) * P.L[0];
+  sy = (float)((int)((code / 3u) % 3u) - 1) * P.L[1];
+  sz = (float)((int)(code / 9u) - 1) * P.L[2];
+}
+
 // Pair terms of i_a (low half) and i_b (high half) over their queues; adds
 // the warp totals into res[0] (i_a) and res[1] (i_b): ax, ay, az, sum g drdv,
 // v_sig, count.  Lanes past a queue's end contribute exactly zero.
 __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParams& P, int ia, int ib, bool has_b,
-                                              const float4& IA, const float4& IBp, const unsigned short* qa, int na,
-                                              const unsigned short* qb, int nb, const float4* tp, const int* tg,
-                                              float (*res)[6], int lane) {
+                                              const float4& IA, const float4& IBp, const uint32_t* qa, int na,
+                                              const uint32_t* qb, int nb, float (*res)[6], int lane) {
   const float4 VA = __ldg(&a.jB[ia]), VB = __ldg(&a.jB[ib]);
   const f2 X = pk(IA.x, IBp.x), Y = pk(IA.y, IBp.y), Z = pk(IA.z, IBp.z);
   const f2 VX = pk(VA.x, VB.x), VY = pk(VA.y, VB.y), VZ = pk(VA.z, VB.z);
@@ -91,18 +101,29 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
   const f2 ONE = dup(1.0f), HALF = dup(0.5f), TWELVE = dup(12.0f), MTHREE = dup(-3.0f), TWO = dup(2.0f);
   const f2 BETA = dup(P.beta), MHALPHA = dup(-0.5f * P.alpha), MONE = dup(-1.0f);
   const int vs = P.vsig_mode;
+  const bool per = P.periodic;
   const int nbq = has_b ? nb : 0;
   const int n = max(na, nbq);
   f2 AX = 0ull, AY = 0ull, AZ = 0ull, DS = 0ull;
   float vsa = 0.f, vsb = 0.f;
   for (int k = lane; k < n; k += 32) {
     const bool va = k < na, vb = k < nbq;
-    const int ta = va ? qa[k] : 0, tb = vb ? qb[k] : 0;
-    const float4 Ja = tp[ta], Jb = tp[tb];
-    const int ga = tg[ta], gb = tg[tb];
+    // idle halves read i_a's own record (always a valid slot; weight 0 below)
+    const uint32_t self = (uint32_t)ia | (13u << 27);
+    const uint32_t ea = va ? qa[k] : self, eb = vb ? qb[k] : self;
+    const int ga = ea & kSlotMask, gb = eb & kSlotMask;
+    const float4 Ja = __ldg(&a.jA[ga]), Jb = __ldg(&a.jA[gb]);
     const float4 JBa = __ldg(&a.jB[ga]), JBb = __ldg(&a.jB[gb]);
     const f2 CJ = pk(__ldg(&a.jC[ga]), __ldg(&a.jC[gb]));
-    const f2 DX = sub2(X, pk(Ja.x, Jb.x)), DY = sub2(Y, pk(Ja.y, Jb.y)), DZ = sub2(Z, pk(Ja.z, Jb.z));
+    float jxa = Ja.x, jya = Ja.y, jza = Ja.z, jxb = Jb.x, jyb = Jb.y, jzb = Jb.z;
+    if (per) {  // the same rounded image position the scan tested
+      float sx, sy, sz;
+      entry_shift(P, ea >> 27, sx, sy, sz);
+      jxa = __fadd_rn(jxa, sx), jya = __fadd_rn(jya, sy), jza = __fadd_rn(jza, sz);
+      entry_shift(P, eb >> 27, sx, sy, sz);
+      jxb = __fadd_rn(jxb, sx), jyb = __fadd_rn(jyb, sy), jzb = __fadd_rn(jzb, sz);
+    }
+    const f2 DX = sub2(X, pk(jxa, jxb)), DY = sub2(Y, pk(jya, jyb)), DZ = sub2(Z, pk(jza, jzb));
     const f2 R2raw = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
     const f2 R2 = pk(va ? lo(R2raw) : H2, vb ? hi(R2raw) : H2);  // finite stand-in for idle halves
     const f2 W = pk(va ? 1.0f : 0.0f, vb ? 1.0f : 0.0f);
@@ -151,15 +172,26 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
   }
 }
 
+// Append the in-support candidates (even/odd halves of the lane's pair) to a queue.
+__device__ __forceinline__ void append2(uint32_t* q, int& n, bool he, bool ho, uint32_t ee, uint32_t eo, unsigned lt) {
+  const unsigned me = __ballot_sync(0xffffffffu, he), mo = __ballot_sync(0xffffffffu, ho);
+  const int p = n + __popc(me & lt) + __popc(mo & lt);
+  if (he) q[p] = ee;
+  if (ho) q[p + (he ? 1 : 0)] = eo;
+  n += __popc(me) + __popc(mo);
+}
+
 __global__ void __launch_bounds__(kTiledWarps * 32) k_hydro_tiled(StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TiledSmem& S = *reinterpret_cast<TiledSmem*>(smem_raw);
   const unsigned full = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float4* tp = S.pos[warp];
-  int* tg = S.gidx[warp];
-  unsigned short* qa = S.q[warp][0];
-  unsigned short* qb = S.q[warp][1];
+  float* tx = S.x[warp];
+  float* ty = S.y[warp];
+  float* tz = S.z[warp];
+  uint32_t* te = S.e[warp];
+  uint32_t* qa = S.q[warp][0];
+  uint32_t* qb = S.q[warp][1];
   float(*res)[6] = S.res[warp];
   const int nrun = *a.run_count;
   const unsigned lt = lanemask_lt();
@@ -182,9 +214,10 @@ __global__ void __launch_bounds__(kTiledWarps * 32) k_hydro_tiled(StepArgs a) {
     const int nx = P.ncell[0], ny = P.ncell[1];
     const int local = lin - P.cell_base;
     const int cx = local % nx, cy = (local / nx) % ny, cz = local / (nx * ny);
-    // neighbour cells: lane k < 27 owns offset (k%3-1, k/3%3-1, k/9-1)
+    // neighbour cells: lane k < 27 owns offset (k%3-1, k/3%3-1, k/9-1), image code k
     int nb_start = 0, nb_cnt = 0;
     float shx = 0.f, shy = 0.f, shz = 0.f;
+    uint32_t code = 13;
     if (lane < 27) {
       int x, y, z;
       if (neighbor_cell(P, 0, cx + lane % 3 - 1, x, shx) && neighbor_cell(P, 1, cy + (lane / 3) % 3 - 1, y, shy) &&
@@ -192,6 +225,8 @@ __global__ void __launch_bounds__(kTiledWarps * 32) k_hydro_tiled(StepArgs a) {
         const int l2 = P.cell_base + (z * ny + y) * nx + x;
         nb_start = a.cell_start[l2];
         nb_cnt = a.cell_end[l2] - nb_start;
+        code = (uint32_t)((shx > 0.f) - (shx < 0.f) + 1) + 3u * (uint32_t)((shy > 0.f) - (shy < 0.f) + 1) +
+               9u * (uint32_t)((shz > 0.f) - (shz < 0.f) + 1);
       }
     }
     int incl = nb_cnt;
@@ -212,6 +247,7 @@ __global__ void __launch_bounds__(kTiledWarps * 32) k_hydro_tiled(StepArgs a) {
       for (int k = 0; k < 6; ++k) res[lane][k] = 0.f;
       for (int t0 = 0; t0 < T; t0 += kTile) {
         const int tn = min(kTile, T - t0);
+        const int tn64 = (tn + 63) & ~63;
         __syncwarp();
         for (unsigned m = nonempty; m; m &= m - 1) {
           const int k = __ffs(m) - 1;
@@ -219,13 +255,22 @@ __global__ void __launch_bounds__(kTiledWarps * 32) k_hydro_tiled(StepArgs a) {
           const int sk = __shfl_sync(full, nb_start, k);
           const int ek = __shfl_sync(full, excl, k);
           const float sx = __shfl_sync(full, shx, k), sy = __shfl_sync(full, shy, k), sz = __shfl_sync(full, shz, k);
+          const uint32_t ck27 = __shfl_sync(full, code, k) << 27;
           const int lo_ = max(ek, t0), hi_ = min(ek + ck, t0 + tn);
           for (int u = lo_ + lane; u < hi_; u += 32) {
             const int g = sk + (u - ek);
             const float4 J = __ldg(&a.jA[g]);
-            tp[u - t0] = make_float4(__fadd_rn(J.x, sx), __fadd_rn(J.y, sy), __fadd_rn(J.z, sz), J.w);
-            tg[u - t0] = g;
+            tx[u - t0] = __fadd_rn(J.x, sx);
+            ty[u - t0] = __fadd_rn(J.y, sy);
+            tz[u - t0] = __fadd_rn(J.z, sz);
+            te[u - t0] = (uint32_t)g | ck27;
           }
+        }
+        for (int u = tn + lane; u < tn64; u += 32) {  // pad to a multiple of 64: never in support
+          tx[u] = 1.0e30f;
+          ty[u] = 1.0e30f;
+          tz[u] = 1.0e30f;
+          te[u] = 0u;
         }
         __syncwarp();
         for (int ii = 0; ii < nbat; ii += 2) {
@@ -234,27 +279,24 @@ __global__ void __launch_bounds__(kTiledWarps * 32) k_hydro_tiled(StepArgs a) {
           const int ibb = has_b ? ia + 1 : ia;
           const float4 IA = __ldg(&a.jA[ia]);
           const float4 IB = __ldg(&a.jA[ibb]);
-          const f2 X = pk(IA.x, IB.x), Y = pk(IA.y, IB.y), Z = pk(IA.z, IB.z);
+          const f2 XA = dup(IA.x), YA = dup(IA.y), ZA = dup(IA.z);
+          const f2 XB = dup(IB.x), YB = dup(IB.y), ZB = dup(IB.z);
           int na = 0, nb = 0;
-          for (int tb = 0; tb < tn; tb += 32) {
-            const int t = tb + lane;
-            bool ina = false, inb = false;
-            if (t < tn) {
-              const float4 J = tp[t];
-              const f2 DX = sub2(X, dup(J.x)), DY = sub2(Y, dup(J.y)), DZ = sub2(Z, dup(J.z));
-              const f2 R2 = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));  // == dist2 per half
-              const float r2a = lo(R2), r2b = hi(R2);
-              ina = r2a > 0.0f && r2a < H2;
-              inb = has_b && r2b > 0.0f && r2b < H2;
-            }
-            const unsigned ba = __ballot_sync(full, ina), bb = __ballot_sync(full, inb);
-            if (ina) qa[na + __popc(ba & lt)] = (unsigned short)t;
-            if (inb) qb[nb + __popc(bb & lt)] = (unsigned short)t;
-            na += __popc(ba);
-            nb += __popc(bb);
+          for (int tb = 2 * lane; tb < tn64; tb += 64) {
+            const f2 CX = *reinterpret_cast<const f2*>(&tx[tb]);
+            const f2 CY = *reinterpret_cast<const f2*>(&ty[tb]);
+            const f2 CZ = *reinterpret_cast<const f2*>(&tz[tb]);
+            const uint2 E = *reinterpret_cast<const uint2*>(&te[tb]);
+            f2 DX = sub2(XA, CX), DY = sub2(YA, CY), DZ = sub2(ZA, CZ);
+            const f2 RA = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));  // == dist2 per half
+            DX = sub2(XB, CX), DY = sub2(YB, CY), DZ = sub2(ZB, CZ);
+            const f2 RB = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
+            const float ra0 = lo(RA), ra1 = hi(RA), rb0 = lo(RB), rb1 = hi(RB);
+            append2(qa, na, ra0 > 0.0f && ra0 < H2, ra1 > 0.0f && ra1 < H2, E.x, E.y, lt);
+            append2(qb, nb, has_b && rb0 > 0.0f && rb0 < H2, has_b && rb1 > 0.0f && rb1 < H2, E.x, E.y, lt);
           }
           __syncwarp();
-          hydro_queues2(a, P, ia, ibb, has_b, IA, IB, qa, na, qb, nb, tp, tg, &res[ii], lane);
+          hydro_queues2(a, P, ia, ibb, has_b, IA, IB, qa, na, qb, nb, &res[ii], lane);
           __syncwarp();
         }
       }
@@ -280,10 +322,13 @@ struct TiledLaunch {
 };
 
 inline int launch_hydro_tiled(const StepArgs& a, int n, int precision, cudaStream_t s) {
-  (void)n;
   if (precision != WCSPH_PREC_TILED) {
     set_error("precision %d is not built in this library", precision);
     return WCSPH_E_INVALID;
+  }
+  if (n > kMaxTiledParticles) {
+    set_error("the tiled path holds at most %d particles per solver (got %d)", kMaxTiledParticles, n);
+    return WCSPH_E_CAPACITY;
   }
   static TiledLaunch L[16];
   int dev = 0;
