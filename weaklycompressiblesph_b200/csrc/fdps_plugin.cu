@@ -320,8 +320,25 @@ int wcsph_finalize(void) {
   return 0;
 }
 
+}  // extern "C"
+
+namespace wcsph {
+// Defaults (class.h layout, kernel.cu pair semantics) are installed once,
+// before the first explicit configuration or dispatch, never after.
+static bool g_configured_once = false;
+static void default_config() {
+  if (g_configured_once) return;
+  wcsph_fdps_default_layout(&g_plugin.layout);
+  wcsph_pair_params_reference_gpu(&g_plugin.pair);
+  g_configured_once = true;
+}
+}  // namespace wcsph
+
+extern "C" {
+
 int wcsph_fdps_configure(const wcsph_fdps_layout* layout, const wcsph_pair_params* params) {
   std::lock_guard<std::mutex> lk(g_plugin_mu);
+  default_config();
   if (layout) {
     const wcsph_fdps_layout& L = *layout;
     const int sz[3] = {L.epi_size, L.epj_size, L.res_size};
@@ -344,13 +361,6 @@ int wcsph_fdps_configure(const wcsph_fdps_layout* layout, const wcsph_pair_param
 }  // extern "C"
 
 namespace wcsph {
-static bool g_configured_once = false;
-static void default_config() {
-  if (g_configured_once) return;
-  wcsph_fdps_default_layout(&g_plugin.layout);
-  wcsph_pair_params_reference_gpu(&g_plugin.pair);
-  g_configured_once = true;
-}
 
 static int check_walk_args(const char* fn, int32_t tag, int32_t n_walk, const void* const* epi, const int32_t* n_epi,
                            const void* const* epj, const int32_t* n_epj) {

@@ -162,6 +162,7 @@ static StepArgs make_args(SimImpl& S) {
   a.run_list = S.run_list;
   a.run_count = S.d_counters;
   a.work_counter = S.d_counters + 1;
+  a.work_counter2 = S.d_counters + 2;
   a.diag_acc = S.diag_acc;
   a.diag_dt = S.diag_dt;
   a.diag_nbr = S.diag_nbr;
@@ -192,20 +193,27 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
       WCSPH_CUDA(cudaMemsetAsync(S.cell_start, 0, sizeof(int) * S.total_cells, S.s));
       WCSPH_CUDA(cudaMemsetAsync(S.cell_end, 0, sizeof(int) * S.total_cells, S.s));
     }
-    WCSPH_CUDA(cudaMemsetAsync(S.d_counters, 0, 2 * sizeof(int), S.s));
+    WCSPH_CUDA(cudaMemsetAsync(S.d_counters, 0, 3 * sizeof(int), S.s));
     k_permute<<<nblk(n), kBlock, 0, S.s>>>(a);
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));
     if (density) {
-      k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(a);
+      if (S.opt.precision == WCSPH_PREC_FP32) {
+        k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(a);
+      } else {
+        if (int rc = launch_pair_tiled<PASS_DENSITY>(a, n, S.s)) return rc;
+      }
       k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
       L += 2;
     }
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[2], S.s));
     if (S.opt.precision == WCSPH_PREC_FP32) {
       k_hydro_plain<true><<<nblk(n), kBlock, 0, S.s>>>(a);
+    } else if (S.opt.precision == WCSPH_PREC_TILED) {
+      if (int rc = launch_pair_tiled<PASS_HYDRO>(a, n, S.s)) return rc;
     } else {
-      if (int rc = launch_hydro_tiled(a, n, S.opt.precision, S.s)) return rc;
+      set_error("precision %d is not built in this library", S.opt.precision);
+      return WCSPH_E_INVALID;
     }
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[3], S.s));
@@ -214,7 +222,12 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
     if (init_filter) {
       StepArgs b = a;
       b.init_filter = 1;
-      k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(b);
+      if (S.opt.precision == WCSPH_PREC_FP32) {
+        k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(b);
+      } else {
+        WCSPH_CUDA(cudaMemsetAsync(S.d_counters + 2, 0, sizeof(int), S.s));
+        if (int rc = launch_pair_tiled<PASS_DENSITY>(b, n, S.s)) return rc;
+      }
       k_apply_init_filter<<<nblk(n), kBlock, 0, S.s>>>(b);
       L += 2;
     }
