@@ -64,6 +64,7 @@ struct SimImpl {
   int key_bits = 1;
   long long total_cells = 0;
   bool any_density = false;
+  bool density_tiled = false;  // density pass kernel: per-thread (default) or tiled, chosen by the autotuner
   cudaGraphExec_t gexec = nullptr;
   bool graph_dirty = true;
   int kernels_per_step = 0;
@@ -198,7 +199,7 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));
     if (density) {
-      if (S.opt.precision == WCSPH_PREC_FP32) {
+      if (!S.density_tiled) {
         k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(a);
       } else {
         if (int rc = launch_pair_tiled<PASS_DENSITY>(a, n, S.s)) return rc;
@@ -222,7 +223,7 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
     if (init_filter) {
       StepArgs b = a;
       b.init_filter = 1;
-      if (S.opt.precision == WCSPH_PREC_FP32) {
+      if (!S.density_tiled) {
         k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(b);
       } else {
         WCSPH_CUDA(cudaMemsetAsync(S.d_counters + 2, 0, sizeof(int), S.s));
