@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--precision", default="best", choices=["best", "fp32", "tiled", "half2"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison run")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble and serving samples")
+    ap.add_argument("--ensemble-steps", type=int, default=60)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
@@ -291,8 +293,56 @@ def cpu_reference(case, walks, epi, epj, seconds, pairs_total):
     return pairs / el, desc, cores
 
 
+def measure_ensemble(device, steps=None):
+    """Config 4 sample: 64 seeded dam breaks (fluid counts log-uniform in
+    [1e4, 5e5]) stepping together, vs the same instances one at a time on the
+    plain FP32 path; `steps` timed steps each (the config runs 2000)."""
+    from weaklycompressiblesph_b200 import cases, ensemble
+    steps = steps or ARGS.ensemble_steps
+    ens = cases.ensemble_cases(count=64, seed=2024)
+    b = ensemble.run_batched(ens, steps=steps, warmup=3, device=device)
+    s = ensemble.run_serial(ens, steps=steps, warmup=3, precision="fp32", device=device)
+    return {"instances": len(ens), "particles": b["particles"], "steps": steps,
+            "batched_particle_steps_per_s": b["particle_steps_per_s"],
+            "serial_plain_particle_steps_per_s": s["particle_steps_per_s"],
+            "speedup_vs_serial_plain": b["particle_steps_per_s"] / s["particle_steps_per_s"],
+            "sample": f"{steps} timed steps per instance (config: 2000)"}
+
+
+def measure_serving(device):
+    """Config 5 sample: Poisson(20/s) dam-break requests, fluid counts
+    log-uniform in [2e4, 2e5] (config: up to 2e6), each run to t = 0.02 s
+    (config: 1.0 s), admitted by a 150 GB HBM budget; p50/p99
+    time-to-completion and aggregate particle-steps/s, vs the same requests
+    one at a time on the plain FP32 path."""
+    from weaklycompressiblesph_b200 import _native as N
+    from weaklycompressiblesph_b200 import cases
+    from weaklycompressiblesph_b200.serving import Server, run_alone
+    reqs = cases.serving_requests(count=16, rate=20.0, seed=7, n_min=2e4, n_max=2e5, t_end=0.02)
+    total = sum(c.n for _, c in reqs)
+    with Server(budget_bytes=150e9, max_particles=total + 1024, device=device, read_results=False) as srv:
+        out = srv.run(reqs)
+    el = 0.0
+    ps = 0
+    for _, c in reqs:
+        t, steps, _ = run_alone(c, precision=N.PREC_FP32, device=device)
+        el += t
+        ps += c.n * steps
+    return {"requests": len(reqs), "particles": total, "p50_s": out["p50_s"], "p99_s": out["p99_s"],
+            "wall_s": out["wall_s"], "particle_steps_per_s": out["particle_steps_per_s"],
+            "serial_plain_particle_steps_per_s": ps / el,
+            "speedup_vs_serial_plain": out["particle_steps_per_s"] / (ps / el),
+            "sample": "16 requests, counts log-uniform [2e4, 2e5], t_end 0.02 s, Poisson 20/s, budget 150 GB "
+                      "(config: counts to 2e6, t_end 1.0 s)"}
+
+
+ARGS = None
+
+
 def main():
+    global ARGS
     args = parse()
+    ARGS = args
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
         if rank != 0:
@@ -337,6 +387,10 @@ def main():
             v, desc, cores = cpu_reference(case, e["walks"], e["epi"], e["epj"], args.cpu_seconds,
                                            dev["pairs_per_step"])
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc}
+    ens = srv = None
+    if rank == 0 and not args.no_ensemble:
+        ens = measure_ensemble(local)
+        srv = measure_serving(local)
     if rank != 0:
         barrier(pg)
         return 0
@@ -362,6 +416,8 @@ def main():
                      "model": f"{bpp} B per true pair (j-record) / hydro kernel time", "peak_kind": peak_kind},
         "cpu_baseline": cpu,
         "e2e": e2e,
+        "ensemble": ens,
+        "serving": srv,
         "gpu_launches": dev["kernels_per_step"] * args.steps,
         "clocks": dev.get("clocks"),
         "sim_time_s": dev["status"]["time"],

@@ -26,6 +26,7 @@ namespace wcsph {
 struct HostInst {
   bool used = false;     // slot holds an instance (active or draining)
   bool active = false;   // stepping
+  bool drained = false;  // removed, and a pass has been enqueued since (its particles are dead keys)
   wcsph_instance_desc desc{};
   int n = 0;
   int ncell[3] = {0, 0, 0};
@@ -171,6 +172,12 @@ static StepArgs make_args(SimImpl& S) {
   return a;
 }
 
+// A pass was enqueued (captured passes are always launched right after): every removed instance's particles are dead after it.
+static void mark_drained(SimImpl& S) {
+  for (auto& I : S.inst)
+    if (I.used && !I.active) I.drained = true;
+}
+
 constexpr int kBlock = 256;
 static inline int nblk(long long n) { return (int)std::max<long long>(1, (n + kBlock - 1) / kBlock); }
 
@@ -235,6 +242,7 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
   }
   WCSPH_CUDA(cudaGetLastError());
   if (launches) *launches = L;
+  mark_drained(S);
   return 0;
 }
 
@@ -246,11 +254,14 @@ static int sync_compact(SimImpl& S) {
     S.n_host = n_alive;
     S.graph_dirty = true;
   }
-  // Slots whose particles are all gone can be reused.
+  // Slots of removed instances whose particles a pass has already turned into
+  // dead keys can be reused.
   for (auto& I : S.inst)
-    if (I.used && !I.active) I.used = false;
+    if (I.used && !I.active && I.drained) I.used = false;
   return 0;
 }
+
+
 
 static int set_all_phases(SimImpl& S, int active_phase) {
   for (size_t k = 0; k < S.inst.size(); ++k) S.h_phase[k] = S.inst[k].active ? active_phase : PH_IDLE;
@@ -440,6 +451,17 @@ int wcsph_sim_add_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, cons
   SimImpl& S = sim->impl;
   WCSPH_CUDA(cudaSetDevice(S.opt.device));
   if (int rc = sync_compact(S)) return rc;
+  bool draining = false;
+  for (auto& I : S.inst) draining |= I.used && !I.active;
+  if ((long long)S.n_host + desc->n > S.opt.max_particles && draining) {
+    // Removed instances still hold slots: run one pass with every instance
+    // idle so their particles become dead keys, then compact.
+    for (size_t q = 0; q < S.inst.size(); ++q) S.h_phase[q] = PH_IDLE;
+    if (int rc = upload_tables(S)) return rc;
+    if (int rc = enqueue_pass(S, make_args(S), false, false, nullptr)) return rc;
+    if (int rc = set_all_phases(S, PH_STEP)) return rc;
+    if (int rc = sync_compact(S)) return rc;
+  }
   if ((long long)S.n_host + desc->n > S.opt.max_particles) {
     set_error("wcsph_sim_add_instance: %d + %d particles exceed capacity %lld", S.n_host, desc->n,
               (long long)S.opt.max_particles);
@@ -518,6 +540,7 @@ int wcsph_sim_remove_instance(wcsph_sim* sim, int32_t slot) {
   }
   WCSPH_CUDA(cudaSetDevice(S.opt.device));
   S.inst[slot].active = false;  // particles are marked dead by the next binning
+  S.inst[slot].drained = false;
   S.h_phase[slot] = PH_IDLE;
   return rebuild_tables(S);
 }
@@ -554,6 +577,7 @@ int wcsph_sim_step(wcsph_sim* sim, int32_t nsteps) {
     S.graph_dirty = false;
   }
   for (int t = 0; t < nsteps; ++t) WCSPH_CUDA(cudaGraphLaunch(S.gexec, S.s));
+  mark_drained(S);
   return 0;
 }
 
