@@ -20,8 +20,12 @@
 //      per i in shared memory.
 //   4. Lane l finishes i = batch + l with the epilogue shared with the plain
 //      kernel (gravity, final kick, density floor, next-dt fold, state write).
-// Work is distributed dynamically: warps take cells from the list of
-// non-empty cells through a global counter (persistent grid).
+// Work distribution: a persistent grid; warp w takes the non-empty cells
+// w, w + W, w + 2W, ... of the cell list (W warps in the grid), whose order
+// follows the Morton sort, so neighbouring warps share L2-resident records.
+// Staging is latency-bound, so it is flattened: each lane locates the source
+// cell of its candidates by a binary search over the 27 range offsets and
+// keeps several independent loads in flight.
 #pragma once
 #include "f32x2.cuh"
 #include "sim_kernels.cuh"
@@ -30,6 +34,7 @@ namespace wcsph {
 
 constexpr int kTiledWarps = 4;
 constexpr int kTile = 512;                 // candidates staged per pass (multiple of 64)
+constexpr int kStageUnroll = 4;            // staging loads in flight per lane
 constexpr uint32_t kSlotMask = (1u << 27) - 1;
 constexpr int kMaxTiledParticles = 1 << 27;  // queue entries hold the slot in 27 bits
 
@@ -249,12 +254,14 @@ __global__ void __launch_bounds__(kTiledWarps * 32) k_pair_tiled(StepArgs a) {
   const int nrun = *a.run_count;
   const unsigned lt = lanemask_lt();
   unsigned long long pairs = 0;
-  for (;;) {
-    int c = 0;
-    if (lane == 0) c = atomicAdd(PASS == PASS_HYDRO ? a.work_counter : a.work_counter2, 1);
-    c = __shfl_sync(full, c, 0);
-    if (c >= nrun) break;
-    const int lin = a.run_list[c];
+  // Static round-robin over the non-empty cells (no contended counter); the
+  // next cell's index is loaded one iteration ahead.
+  const int stride = gridDim.x * kTiledWarps;
+  int c = blockIdx.x * kTiledWarps + warp;
+  int lin_next = c < nrun ? a.run_list[c] : 0;
+  for (; c < nrun; c += stride) {
+    const int lin = lin_next;
+    if (c + stride < nrun) lin_next = a.run_list[c + stride];
     const int s = a.cell_start[lin], e = a.cell_end[lin];
     const uint32_t f0 = a.alt.flags[s];
     const int inst = f0 & kInstMask;
@@ -292,7 +299,7 @@ __global__ void __launch_bounds__(kTiledWarps * 32) k_pair_tiled(StepArgs a) {
     }
     const int T = __shfl_sync(full, incl, 31);
     const int excl = incl - nb_cnt;
-    const unsigned nonempty = __ballot_sync(full, nb_cnt > 0);
+    const int own = __shfl_sync(full, excl, 13);  // tile offset of the cell's own particles
     const float H2 = P.H2;
     float dt_cand = 0.f;
     bool dt_valid = false;
@@ -304,21 +311,39 @@ __global__ void __launch_bounds__(kTiledWarps * 32) k_pair_tiled(StepArgs a) {
         const int tn = min(kTile, T - t0);
         const int tn64 = (tn + 63) & ~63;
         __syncwarp();
-        for (unsigned m = nonempty; m; m &= m - 1) {
-          const int k = __ffs(m) - 1;
-          const int ck = __shfl_sync(full, nb_cnt, k);
-          const int sk = __shfl_sync(full, nb_start, k);
-          const int ek = __shfl_sync(full, excl, k);
-          const float sx = __shfl_sync(full, shx, k), sy = __shfl_sync(full, shy, k), sz = __shfl_sync(full, shz, k);
-          const uint32_t ck27 = __shfl_sync(full, code, k) << 27;
-          const int lo_ = max(ek, t0), hi_ = min(ek + ck, t0 + tn);
-          for (int u = lo_ + lane; u < hi_; u += 32) {
-            const int g = sk + (u - ek);
-            const float4 J = __ldg(&a.jA[g]);
-            tx[u - t0] = __fadd_rn(J.x, sx);
-            ty[u - t0] = __fadd_rn(J.y, sy);
-            tz[u - t0] = __fadd_rn(J.z, sz);
-            te[u - t0] = (uint32_t)g | ck27;
+        // Flattened staging: candidate u comes from the last neighbour cell k
+        // with excl_k <= u (binary search over lanes 0..26); kStageUnroll
+        // independent loads per lane are in flight before any store.
+        for (int ub = t0; ub < t0 + tn; ub += 32 * kStageUnroll) {
+          float4 J[kStageUnroll];
+          int gk[kStageUnroll], kk[kStageUnroll];
+#pragma unroll
+          for (int r = 0; r < kStageUnroll; ++r) {
+            const int u = ub + 32 * r + lane;
+            int k = 0;
+#pragma unroll
+            for (int step = 16; step; step >>= 1) {
+              const int cand = k + step;
+              const int ec = __shfl_sync(full, excl, cand < 27 ? cand : 26);
+              if (cand < 27 && ec <= u) k = cand;
+            }
+            const int sk = __shfl_sync(full, nb_start, k), ek = __shfl_sync(full, excl, k);
+            kk[r] = k;
+            gk[r] = sk + (u - ek);
+            if (u < t0 + tn) J[r] = __ldg(&a.jA[gk[r]]);
+          }
+#pragma unroll
+          for (int r = 0; r < kStageUnroll; ++r) {
+            const int u = ub + 32 * r + lane;
+            const int k = kk[r];
+            const float sx = __shfl_sync(full, shx, k), sy = __shfl_sync(full, shy, k), sz = __shfl_sync(full, shz, k);
+            const uint32_t ck27 = __shfl_sync(full, code, k) << 27;
+            if (u < t0 + tn) {
+              tx[u - t0] = __fadd_rn(J[r].x, sx);
+              ty[u - t0] = __fadd_rn(J[r].y, sy);
+              tz[u - t0] = __fadd_rn(J[r].z, sz);
+              te[u - t0] = (uint32_t)gk[r] | ck27;
+            }
           }
         }
         for (int u = tn + lane; u < tn64; u += 32) {  // pad to a multiple of 64: never in support
@@ -332,8 +357,12 @@ __global__ void __launch_bounds__(kTiledWarps * 32) k_pair_tiled(StepArgs a) {
           const int ia = ib + ii;
           const bool has_b = ii + 1 < nbat;
           const int ibb = has_b ? ia + 1 : ia;
-          const float4 IA = __ldg(&a.jA[ia]);
-          const float4 IB = __ldg(&a.jA[ibb]);
+          // i positions from the tile when the own cell (lane 13) is staged in this pass
+          const int oa = own + (ia - s) - t0, ob = own + (ibb - s) - t0;
+          const float4 IA = (oa >= 0 && oa < tn) ? make_float4(tx[oa], ty[oa], tz[oa], __ldg(&a.jA[ia].w))
+                                                 : __ldg(&a.jA[ia]);
+          const float4 IB = (ob >= 0 && ob < tn) ? make_float4(tx[ob], ty[ob], tz[ob], __ldg(&a.jA[ibb].w))
+                                                 : __ldg(&a.jA[ibb]);
           const f2 XA = dup(IA.x), YA = dup(IA.y), ZA = dup(IA.z);
           const f2 XB = dup(IB.x), YB = dup(IB.y), ZB = dup(IB.z);
           int na = 0, nb = 0;

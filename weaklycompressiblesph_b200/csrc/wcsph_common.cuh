@@ -6,7 +6,7 @@
 #include <cstdio>
 #include <string>
 
-#include "../../include/wcsph.h"
+#include "wcsph.h"
 
 namespace wcsph {
 
