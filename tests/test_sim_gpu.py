@@ -13,12 +13,18 @@ from weaklycompressiblesph_b200.sim import Solver
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-5
-PRECISIONS = [N.PREC_FP32, N.PREC_TILED]
+PRECISIONS = [N.PREC_FP32, N.PREC_TILED, N.PREC_HALF2]
 
 
-@pytest.fixture(params=PRECISIONS, ids=["fp32", "tiled"])
+@pytest.fixture(params=PRECISIONS, ids=["fp32", "tiled", "half2"])
 def prec(request):
     return request.param
+
+
+def force_tol(prec):
+    """FP32 pair arithmetic: 1e-5 relative L2 vs FP64.  The half2 kernel
+    gradient carries ~5e-4 relative error per pair: 3e-3."""
+    return 3e-3 if prec == N.PREC_HALF2 else TOL
 
 
 def f32(a):
@@ -62,9 +68,9 @@ def test_hydro_forces(prec, native, oracle_lib, which):
         k = s.add(case, density_mode=N.DENSITY_CONTINUITY)
         pr = s.probe(k)
         acc, dv, dt, cnt, _ = oracle_forces(oracle_lib, case, case.pos, case.vel, case.dens)
-        assert rel_l2(pr["acc"], acc) < TOL
-        assert rel_l2(pr["div_v"], dv) < TOL
-        np.testing.assert_allclose(pr["dt"], dt, rtol=TOL)
+        assert rel_l2(pr["acc"], acc) < force_tol(prec)
+        assert rel_l2(pr["div_v"], dv) < force_tol(prec)
+        np.testing.assert_allclose(pr["dt"], dt, rtol=force_tol(prec))
 
 
 @pytest.mark.parametrize("shepard", [0, 1])
@@ -90,8 +96,8 @@ def test_initial_pass_matches_oracle(prec, native, oracle_lib):
     o["vel"][:] = f32(case.vel)
     o["dens"][:] = f32(case.dens)
     oracle_lib.state_initial(case.n, o, cfg)
-    assert rel_l2(st["acc"], o["acc"]) < TOL
-    assert rel_l2(st["div_v"], o["div_v"]) < TOL
+    assert rel_l2(st["acc"], o["acc"]) < force_tol(prec)
+    assert rel_l2(st["div_v"], o["div_v"]) < force_tol(prec)
     np.testing.assert_allclose(st["dens"], o["dens"], rtol=TOL)
 
 
@@ -119,9 +125,10 @@ def test_trajectory_vs_fp64(prec, native, oracle_lib, mode):
     assert status["steps"] == nsteps
     assert status["time"] == pytest.approx(t, rel=1e-5)
     disp = o["pos"] - f32(case.pos)
-    assert rel_l2(st["pos"] - f32(case.pos), disp) < 1e-3
-    assert rel_l2(st["vel"], o["vel"]) < 1e-3
-    np.testing.assert_allclose(st["dens"], o["dens"], rtol=1e-5)
+    traj = 1e-2 if prec == N.PREC_HALF2 else 1e-3
+    assert rel_l2(st["pos"] - f32(case.pos), disp) < traj
+    assert rel_l2(st["vel"], o["vel"]) < traj
+    np.testing.assert_allclose(st["dens"], o["dens"], rtol=1e-4 if prec == N.PREC_HALF2 else 1e-5)
 
 
 def test_momentum_conservation_periodic(prec, native):

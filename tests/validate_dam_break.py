@@ -1,0 +1,98 @@
+"""Config-2 validation: the dam break at dx = 0.005 (1,024,000 fluid + 571,308
+wall particles), FP32 (tiled) vs half2-gradient paths.
+
+    python tests/validate_dam_break.py [--steps 5000] [--every 500] [--dx 0.005]
+
+At every checkpoint the GPU's own FP32 state is read back and one force pass
+is checked against the FP64 oracle on that state: relative L2 of the
+acceleration, drho/dt = -rho div v, and div v.  The surge front (largest x of
+a fluid particle) is recorded against physical time for both paths and the
+half2 front is compared with the FP32 front.  Prints one JSON line.
+Not collected by pytest (long); run on a GPU box.
+"""
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+import oracle  # noqa: E402
+from weaklycompressiblesph_b200 import _native as N  # noqa: E402
+from weaklycompressiblesph_b200 import cases  # noqa: E402
+from weaklycompressiblesph_b200.sim import Solver  # noqa: E402
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def check(case, s, k):
+    """GPU force pass vs FP64 oracle on the GPU's current state."""
+    st = s.read(k)
+    pr = s.probe(k)
+    cfg = oracle.config_from_case(case)
+    p4 = oracle.pos4(st["pos"])
+    v4 = oracle.pos4(st["vel"])
+    d = st["dens"].astype(np.float64)
+    pres, snds = oracle.eos(d, case.phys.gamma, case.phys.rho0, case.phys.c0)
+    acc, dv, _ = oracle.hydro(p4, v4, st["dens"], pres.astype(np.float32), snds.astype(np.float32), cfg)
+    cnt, _ = oracle.neighbors(p4, cfg)
+    return {"acc": rel(pr["acc"], acc), "drho_dt": rel(-pr["dens"] * pr["div_v"], -d * dv), "div_v": rel(pr["div_v"], dv),
+            "neighbors_exact": bool(np.array_equal(pr["nbr"], cnt))}
+
+
+def run(case, precision, steps, every):
+    front = []
+    checks = []
+    with Solver(case.n + 1024, precision=precision) as s:
+        k = s.add(case)
+        fluid = case.type == N.HYDRO
+        t0 = time.perf_counter()
+        done = 0
+        while True:
+            st = s.status(k)
+            pos = s.read(k)["pos"]
+            front.append((st["time"], float(pos[fluid, 0].max())))
+            if done % every == 0 or done == steps:
+                c = check(case, s, k)
+                c["step"] = done
+                checks.append(c)
+            if done >= steps:
+                break
+            n = min(100, steps - done)
+            s.step(n)
+            done += n
+        wall = time.perf_counter() - t0
+    return {"front": front, "checks": checks, "wall_s": wall}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--every", type=int, default=1000)
+    ap.add_argument("--dx", type=float, default=0.005)
+    args = ap.parse_args()
+    case = cases.dam_break(dx=args.dx)
+    out = {"case": case.name, "particles": case.n, "steps": args.steps}
+    res = {}
+    for name, prec in (("fp32_tiled", N.PREC_TILED), ("half2", N.PREC_HALF2)):
+        res[name] = run(case, prec, args.steps, args.every)
+        out[name] = {"checks": res[name]["checks"], "sim_time_end": res[name]["front"][-1][0],
+                     "front_end": res[name]["front"][-1][1]}
+    f32 = np.array(res["fp32_tiled"]["front"])
+    h16 = np.array(res["half2"]["front"])
+    # compare fronts at common physical times (interpolate half2 onto fp32 times)
+    hi = np.interp(f32[:, 0], h16[:, 0], h16[:, 1])
+    col = 0.4  # initial column length
+    out["surge_front"] = {"max_abs_diff_m": float(np.abs(hi - f32[:, 1]).max()),
+                          "max_rel_diff_vs_travel": float(np.abs(hi - f32[:, 1]).max() / max(f32[:, 1].max() - col, 1e-9)),
+                          "fp32_samples": [(round(t, 5), round(x, 5)) for t, x in f32[:: max(1, len(f32) // 10)]]}
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -220,8 +220,7 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
     } else if (S.opt.precision == WCSPH_PREC_TILED) {
       if (int rc = launch_pair_tiled<PASS_HYDRO>(a, n, S.s)) return rc;
     } else {
-      set_error("precision %d is not built in this library", S.opt.precision);
-      return WCSPH_E_INVALID;
+      if (int rc = launch_pair_tiled<PASS_HYDRO, true>(a, n, S.s)) return rc;
     }
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[3], S.s));

@@ -27,6 +27,8 @@
 // cell of its candidates by a binary search over the 27 range offsets and
 // keeps several independent loads in flight.
 #pragma once
+#include <cuda_fp16.h>
+
 #include "f32x2.cuh"
 #include "sim_kernels.cuh"
 
@@ -93,6 +95,10 @@ __device__ __forceinline__ void entry_shift(const InstParams& P, uint32_t code, 
 // Pair terms of i_a (low half) and i_b (high half) over their queues; adds
 // the warp totals into res[0] (i_a) and res[1] (i_b): ax, ay, az, sum g drdv,
 // v_sig, count.  Lanes past a queue's end contribute exactly zero.
+// H16: the kernel gradient (|dr|^2, 1/|dr|, s, F(s), F/|dr|) is evaluated in
+// packed half2 on displacements in units of the support 2h; everything else
+// stays FP32 (WCSPH_PREC_HALF2).
+template <bool H16>
 __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParams& P, int ia, int ib, bool has_b,
                                               const float4& IA, const float4& IBp, const uint32_t* qa, int na,
                                               const uint32_t* qb, int nb, float (*res)[6], int lane) {
@@ -132,11 +138,29 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
     const f2 R2raw = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
     const f2 R2 = pk(va ? lo(R2raw) : H2, vb ? hi(R2raw) : H2);  // finite stand-in for idle halves
     const f2 W = pk(va ? 1.0f : 0.0f, vb ? 1.0f : 0.0f);
-    const f2 RINV = rsqrt2(R2);
-    const f2 S = mul2(mul2(R2, RINV), IH);
-    const f2 A = max0_2(sub2(ONE, S)), B = max0_2(sub2(HALF, S));
-    const f2 F = fma2(TWELVE, mul2(B, B), mul2(MTHREE, mul2(A, A)));  // 12 (1/2-s)+^2 - 3 (1-s)+^2
-    const f2 G = mul2(mul2(F, KG), mul2(RINV, W));                     // gradW = G * dr
+    f2 G;  // gradW = G * dr
+    if (H16) {
+      const float iH = P.inv_H;
+      // q = dr / 2h; idle halves get a harmless |q| = 1/2
+      const __half2 qx = __floats2half2_rn(va ? lo(DX) * iH : 0.5f, vb ? hi(DX) * iH : 0.5f);
+      const __half2 qy = __floats2half2_rn(va ? lo(DY) * iH : 0.0f, vb ? hi(DY) * iH : 0.0f);
+      const __half2 qz = __floats2half2_rn(va ? lo(DZ) * iH : 0.0f, vb ? hi(DZ) * iH : 0.0f);
+      const __half2 r2h = __hmax2(__hfma2(qz, qz, __hfma2(qy, qy, __hmul2(qx, qx))), __float2half2_rn(1.0e-4f));
+      const __half2 rih = h2rsqrt(r2h);
+      const __half2 sh = __hmul2(r2h, rih);  // s = |dr| / 2h
+      const __half2 ah = __hmax2(__hsub2(__float2half2_rn(1.0f), sh), __float2half2_rn(0.0f));
+      const __half2 bh = __hmax2(__hsub2(__float2half2_rn(0.5f), sh), __float2half2_rn(0.0f));
+      const __half2 Fh = __hfma2(__float2half2_rn(12.0f), __hmul2(bh, bh),
+                                 __hmul2(__float2half2_rn(-3.0f), __hmul2(ah, ah)));
+      const float2 gq = __half22float2(__hmul2(Fh, rih));  // F(s) / |q|
+      G = mul2(pk(gq.x, gq.y), mul2(dup(P.Kg * iH), W));    // g = F Kg / |dr| = (F/|q|) Kg / 2h
+    } else {
+      const f2 RINV = rsqrt2(R2);
+      const f2 S = mul2(mul2(R2, RINV), IH);
+      const f2 A = max0_2(sub2(ONE, S)), B = max0_2(sub2(HALF, S));
+      const f2 F = fma2(TWELVE, mul2(B, B), mul2(MTHREE, mul2(A, A)));  // 12 (1/2-s)+^2 - 3 (1-s)+^2
+      G = mul2(mul2(F, KG), mul2(RINV, W));
+    }
     const f2 DVX = sub2(VX, pk(JBa.x, JBb.x)), DVY = sub2(VY, pk(JBa.y, JBb.y)), DVZ = sub2(VZ, pk(JBa.z, JBb.z));
     const f2 DRDV = fma2(DZ, DVZ, fma2(DY, DVY, mul2(DX, DVX)));
     const f2 RDEN = rcp2(add2(R2, EH2));
@@ -238,7 +262,7 @@ __device__ __forceinline__ void append2(uint32_t* q, int& n, bool he, bool ho, u
 
 enum PairPass { PASS_HYDRO = 0, PASS_DENSITY = 1 };
 
-template <int PASS>
+template <int PASS, bool H16>
 __global__ void __launch_bounds__(kTiledWarps * 32) k_pair_tiled(StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TiledSmem& S = *reinterpret_cast<TiledSmem*>(smem_raw);
@@ -380,7 +404,7 @@ __global__ void __launch_bounds__(kTiledWarps * 32) k_pair_tiled(StepArgs a) {
             append2(qb, nb, has_b && rb0 > 0.0f && rb0 < H2, has_b && rb1 > 0.0f && rb1 < H2, E.x, E.y, lt);
           }
           __syncwarp();
-          if (PASS == PASS_HYDRO) hydro_queues2(a, P, ia, ibb, has_b, IA, IB, qa, na, qb, nb, &res[ii], lane);
+          if (PASS == PASS_HYDRO) hydro_queues2<H16>(a, P, ia, ibb, has_b, IA, IB, qa, na, qb, nb, &res[ii], lane);
           else density_queues2(a, P, ia, has_b, IA, IB, qa, na, qb, nb, &res[ii], lane);
           __syncwarp();
         }
@@ -413,7 +437,7 @@ struct TiledLaunch {
   int blocks = 0;
 };
 
-template <int PASS>
+template <int PASS, bool H16 = false>
 inline int launch_pair_tiled(const StepArgs& a, int n, cudaStream_t s) {
   if (n > kMaxTiledParticles) {
     set_error("the tiled path holds at most %d particles per solver (got %d)", kMaxTiledParticles, n);
@@ -425,14 +449,14 @@ inline int launch_pair_tiled(const StepArgs& a, int n, cudaStream_t s) {
   TiledLaunch& T = L[dev & 15];
   if (T.device != dev) {
     const int bytes = (int)sizeof(TiledSmem);
-    WCSPH_CUDA(cudaFuncSetAttribute(k_pair_tiled<PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    WCSPH_CUDA(cudaFuncSetAttribute(k_pair_tiled<PASS, H16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     int per_sm = 0, sms = 0;
-    WCSPH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_tiled<PASS>, kTiledWarps * 32, bytes));
+    WCSPH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_tiled<PASS, H16>, kTiledWarps * 32, bytes));
     WCSPH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     T.blocks = std::max(1, per_sm) * sms;
     T.device = dev;
   }
-  k_pair_tiled<PASS><<<T.blocks, kTiledWarps * 32, sizeof(TiledSmem), s>>>(a);
+  k_pair_tiled<PASS, H16><<<T.blocks, kTiledWarps * 32, sizeof(TiledSmem), s>>>(a);
   WCSPH_CUDA(cudaGetLastError());
   return 0;
 }
