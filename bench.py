@@ -210,6 +210,7 @@ def run_device(case, prec_name, steps, warmup, device, clocks=False):
         ph = s.profile_steps(prof_steps)
         res["phase_ms"] = (ph / prof_steps).tolist()
         res["status"] = s.status(k)
+        res["tuning"] = s.tuning()
     return res
 
 
@@ -416,6 +417,7 @@ def main():
                      "model": f"{bpp} B per true pair (j-record) / hydro kernel time", "peak_kind": peak_kind},
         "cpu_baseline": cpu,
         "e2e": e2e,
+        "autotune": dev.get("tuning"),
         "ensemble": ens,
         "serving": srv,
         "gpu_launches": dev["kernels_per_step"] * args.steps,

@@ -196,6 +196,10 @@ typedef struct wcsph_sim_options {
   int64_t max_cells;           /* capacity of the cell table over all instances */
   int32_t max_instances;
   int32_t use_graph;           /* capture each step in a CUDA graph (1) or launch eagerly (0) */
+  int32_t autotune;            /* 1: time the kernel variants on the live instance set (probe
+                                  passes, state untouched) and keep the fastest, re-tuned when the
+                                  particle count crosses a power of two; 0: fixed defaults */
+  int32_t reserved_;
 } wcsph_sim_options;
 
 typedef struct wcsph_sim wcsph_sim;
@@ -246,6 +250,11 @@ int wcsph_sim_conservation(wcsph_sim* sim, int32_t slot, double* out6);
 int64_t wcsph_sim_last_pairs(wcsph_sim* sim);
 /* Number of kernel launches per step issued by the solver (for accounting). */
 int32_t wcsph_sim_kernels_per_step(wcsph_sim* sim);
+/* The autotuner's current choice: out[0] tile shape of the tiled pair kernels
+ * (0: 4 warps x 512 candidates, 1: 2 x 512, 2: 2 x 1024), out[1] density
+ * kernel (0 per-thread, 1 tiled), out[2] log2 particle bucket it was tuned
+ * for (-1: defaults, not tuned). */
+int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out3);
 /* The solver's CUDA stream (a cudaStream_t), so callers can record events on it. */
 void* wcsph_sim_stream(wcsph_sim* sim);
 /* Run nsteps steps launched one by one (no graph) with CUDA events around each

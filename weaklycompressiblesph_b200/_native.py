@@ -52,7 +52,8 @@ class InstanceDesc(C.Structure):
 
 class SimOptions(C.Structure):
     _fields_ = [("device", C.c_int32), ("precision", C.c_int32), ("max_particles", C.c_int64),
-                ("max_cells", C.c_int64), ("max_instances", C.c_int32), ("use_graph", C.c_int32)]
+                ("max_cells", C.c_int64), ("max_instances", C.c_int32), ("use_graph", C.c_int32),
+                ("autotune", C.c_int32), ("reserved_", C.c_int32)]
 
 
 class WcsphError(RuntimeError):
@@ -99,6 +100,7 @@ _SIGS = {
     "wcsph_sim_last_pairs": (C.c_int64, [P]),
     "wcsph_sim_kernels_per_step": (C.c_int32, [P]),
     "wcsph_sim_stream": (C.c_void_p, [P]),
+    "wcsph_sim_tuning": (C.c_int, [P, I32P]),
     "wcsph_sim_profile_steps": (C.c_int, [P, C.c_int32, F64P]),
 }
 

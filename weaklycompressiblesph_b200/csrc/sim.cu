@@ -66,6 +66,8 @@ struct SimImpl {
   long long total_cells = 0;
   bool any_density = false;
   bool density_tiled = false;  // density pass kernel: per-thread (default) or tiled, chosen by the autotuner
+  int tile_shape = 0;          // tiled pair-kernel shape, chosen by the autotuner
+  int tuned_bucket = -1;       // log2 particle bucket of the last tuning
   cudaGraphExec_t gexec = nullptr;
   bool graph_dirty = true;
   int kernels_per_step = 0;
@@ -209,7 +211,7 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
       if (!S.density_tiled) {
         k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(a);
       } else {
-        if (int rc = launch_pair_tiled<PASS_DENSITY>(a, n, S.s)) return rc;
+        if (int rc = launch_pair_tiled<PASS_DENSITY>(a, n, S.s, S.tile_shape)) return rc;
       }
       k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
       L += 2;
@@ -218,9 +220,9 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
     if (S.opt.precision == WCSPH_PREC_FP32) {
       k_hydro_plain<true><<<nblk(n), kBlock, 0, S.s>>>(a);
     } else if (S.opt.precision == WCSPH_PREC_TILED) {
-      if (int rc = launch_pair_tiled<PASS_HYDRO>(a, n, S.s)) return rc;
+      if (int rc = launch_pair_tiled<PASS_HYDRO>(a, n, S.s, S.tile_shape)) return rc;
     } else {
-      if (int rc = launch_pair_tiled<PASS_HYDRO, true>(a, n, S.s)) return rc;
+      if (int rc = launch_pair_tiled<PASS_HYDRO, true>(a, n, S.s, S.tile_shape)) return rc;
     }
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[3], S.s));
@@ -232,8 +234,7 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
       if (!S.density_tiled) {
         k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(b);
       } else {
-        WCSPH_CUDA(cudaMemsetAsync(S.d_counters + 2, 0, sizeof(int), S.s));
-        if (int rc = launch_pair_tiled<PASS_DENSITY>(b, n, S.s)) return rc;
+        if (int rc = launch_pair_tiled<PASS_DENSITY>(b, n, S.s, S.tile_shape)) return rc;
       }
       k_apply_init_filter<<<nblk(n), kBlock, 0, S.s>>>(b);
       L += 2;
@@ -261,6 +262,61 @@ static int sync_compact(SimImpl& S) {
 }
 
 
+
+static int set_all_phases(SimImpl& S, int active_phase);
+
+// Milliseconds of `reps` back-to-back launches of fn on the solver stream.
+template <typename F>
+static int time_launches(SimImpl& S, int reps, F&& fn, float* ms) {
+  if (int rc = fn()) return rc;  // warm-up
+  WCSPH_CUDA(cudaEventRecord(S.ev0, S.s));
+  for (int r = 0; r < reps; ++r)
+    if (int rc = fn()) return rc;
+  WCSPH_CUDA(cudaEventRecord(S.ev1, S.s));
+  WCSPH_CUDA(cudaEventSynchronize(S.ev1));
+  WCSPH_CUDA(cudaEventElapsedTime(ms, S.ev0, S.ev1));
+  return 0;
+}
+
+// Autotuner: on the live instance set, time every tile shape of the tiled
+// hydro kernel and the per-thread vs tiled density kernel with probe passes
+// (forces go to the diagnostic arrays, the state is untouched), keep the
+// fastest.  Re-tuned only when the particle count crosses a power of two.
+static int autotune(SimImpl& S) {
+  if (!S.opt.autotune || S.opt.precision == WCSPH_PREC_FP32 || S.n_host <= 0) return 0;
+  int bucket = 0;
+  while ((1LL << bucket) < S.n_host) ++bucket;
+  if (bucket == S.tuned_bucket) return 0;
+  for (size_t q = 0; q < S.inst.size(); ++q) S.h_phase[q] = S.inst[q].active ? PH_PROBE : PH_IDLE;
+  if (int rc = upload_tables(S)) return rc;
+  StepArgs a = make_args(S);
+  a.probe_density = 1;
+  // one probe pass bins and sorts; repeated pair-kernel launches are then idempotent
+  if (int rc = enqueue_pass(S, a, false, false, nullptr)) return rc;
+  const int n = S.n_host;
+  const bool h16 = S.opt.precision == WCSPH_PREC_HALF2;
+  float best = 1e30f, ms = 0.f;
+  int best_shape = 0;
+  for (int v = 0; v < kTileShapes; ++v) {
+    int rc = time_launches(S, 3, [&]() {
+      return h16 ? launch_pair_tiled<PASS_HYDRO, true>(a, n, S.s, v) : launch_pair_tiled<PASS_HYDRO>(a, n, S.s, v);
+    }, &ms);
+    if (rc) return rc;
+    if (ms < best) best = ms, best_shape = v;
+  }
+  S.tile_shape = best_shape;
+  float ms_plain = 0.f, ms_tiled = 0.f;
+  if (int rc = time_launches(S, 3, [&]() {
+        k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(a);
+        return cuda_fail_if(cudaGetLastError());
+      }, &ms_plain)) return rc;
+  if (int rc = time_launches(S, 3, [&]() { return launch_pair_tiled<PASS_DENSITY>(a, n, S.s, S.tile_shape); },
+                             &ms_tiled)) return rc;
+  S.density_tiled = ms_tiled < ms_plain;
+  S.tuned_bucket = bucket;
+  S.graph_dirty = true;
+  return set_all_phases(S, PH_STEP);
+}
 
 static int set_all_phases(SimImpl& S, int active_phase) {
   for (size_t k = 0; k < S.inst.size(); ++k) S.h_phase[k] = S.inst[k].active ? active_phase : PH_IDLE;
@@ -559,6 +615,8 @@ int wcsph_sim_step(wcsph_sim* sim, int32_t nsteps) {
     return 0;
   }
   if (S.graph_dirty || !S.gexec) {
+    if (int rc = autotune(S)) return rc;
+    a = make_args(S);
     if (S.gexec) {
       cudaGraphExecDestroy(S.gexec);
       S.gexec = nullptr;
@@ -771,6 +829,14 @@ int64_t wcsph_sim_last_pairs(wcsph_sim* sim) {
 int32_t wcsph_sim_kernels_per_step(wcsph_sim* sim) { return sim ? sim->impl.kernels_per_step : -1; }
 
 void* wcsph_sim_stream(wcsph_sim* sim) { return sim ? (void*)sim->impl.s : nullptr; }
+
+int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out3) {
+  if (!sim || !out3) return WCSPH_E_INVALID;
+  out3[0] = sim->impl.tile_shape;
+  out3[1] = sim->impl.density_tiled ? 1 : 0;
+  out3[2] = sim->impl.tuned_bucket;
+  return 0;
+}
 
 int wcsph_sim_profile_steps(wcsph_sim* sim, int32_t nsteps, double* ms4) {
   if (!sim || !ms4 || nsteps < 0) return WCSPH_E_INVALID;

@@ -34,17 +34,18 @@
 
 namespace wcsph {
 
-constexpr int kTiledWarps = 4;
-constexpr int kTile = 512;                 // candidates staged per pass (multiple of 64)
 constexpr int kStageUnroll = 4;            // staging loads in flight per lane
 constexpr uint32_t kSlotMask = (1u << 27) - 1;
 constexpr int kMaxTiledParticles = 1 << 27;  // queue entries hold the slot in 27 bits
 
+// Shared memory of a block of WARPS warps with TILE-candidate tiles
+// (TILE a multiple of 64).
+template <int WARPS, int TILE>
 struct TiledSmem {
-  float x[kTiledWarps][kTile], y[kTiledWarps][kTile], z[kTiledWarps][kTile];  // staged candidates
-  uint32_t e[kTiledWarps][kTile];            // slot | image code << 27
-  uint32_t q[kTiledWarps][2][kTile];         // per-i compacted queues of entries
-  float res[kTiledWarps][32][6];             // per-i accumulators of the current batch
+  float x[WARPS][TILE], y[WARPS][TILE], z[WARPS][TILE];  // staged candidates
+  uint32_t e[WARPS][TILE];                   // slot | image code << 27
+  uint32_t q[WARPS][2][TILE];                // per-i compacted queues of entries
+  float res[WARPS][32][6];                   // per-i accumulators of the current batch
 };
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -262,10 +263,12 @@ __device__ __forceinline__ void append2(uint32_t* q, int& n, bool he, bool ho, u
 
 enum PairPass { PASS_HYDRO = 0, PASS_DENSITY = 1 };
 
-template <int PASS, bool H16>
-__global__ void __launch_bounds__(kTiledWarps * 32) k_pair_tiled(StepArgs a) {
+template <int PASS, bool H16, int WARPS, int TILE>
+__global__ void __launch_bounds__(WARPS * 32) k_pair_tiled(StepArgs a) {
+  constexpr int kTiledWarps = WARPS;
+  constexpr int kTile = TILE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  TiledSmem& S = *reinterpret_cast<TiledSmem*>(smem_raw);
+  TiledSmem<WARPS, TILE>& S = *reinterpret_cast<TiledSmem<WARPS, TILE>*>(smem_raw);
   const unsigned full = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* tx = S.x[warp];
@@ -437,28 +440,45 @@ struct TiledLaunch {
   int blocks = 0;
 };
 
-template <int PASS, bool H16 = false>
-inline int launch_pair_tiled(const StepArgs& a, int n, cudaStream_t s) {
-  if (n > kMaxTiledParticles) {
-    set_error("the tiled path holds at most %d particles per solver (got %d)", kMaxTiledParticles, n);
-    return WCSPH_E_CAPACITY;
-  }
+template <int PASS, bool H16, int WARPS, int TILE>
+inline int launch_pair_tiled_v(const StepArgs& a, cudaStream_t s) {
   static TiledLaunch L[16];
   int dev = 0;
   WCSPH_CUDA(cudaGetDevice(&dev));
   TiledLaunch& T = L[dev & 15];
+  auto kern = k_pair_tiled<PASS, H16, WARPS, TILE>;
+  const int bytes = (int)sizeof(TiledSmem<WARPS, TILE>);
   if (T.device != dev) {
-    const int bytes = (int)sizeof(TiledSmem);
-    WCSPH_CUDA(cudaFuncSetAttribute(k_pair_tiled<PASS, H16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    WCSPH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     int per_sm = 0, sms = 0;
-    WCSPH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_tiled<PASS, H16>, kTiledWarps * 32, bytes));
+    WCSPH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, bytes));
     WCSPH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     T.blocks = std::max(1, per_sm) * sms;
     T.device = dev;
   }
-  k_pair_tiled<PASS, H16><<<T.blocks, kTiledWarps * 32, sizeof(TiledSmem), s>>>(a);
+  kern<<<T.blocks, WARPS * 32, bytes, s>>>(a);
   WCSPH_CUDA(cudaGetLastError());
   return 0;
+}
+
+// Tile shapes the autotuner chooses among: (warps per block, candidates per tile).
+constexpr int kTileShapes = 3;
+inline const char* tile_shape_name(int v) {
+  static const char* names[kTileShapes] = {"4 warps x 512", "2 warps x 512", "2 warps x 1024"};
+  return (v >= 0 && v < kTileShapes) ? names[v] : "?";
+}
+
+template <int PASS, bool H16 = false>
+inline int launch_pair_tiled(const StepArgs& a, int n, cudaStream_t s, int shape = 0) {
+  if (n > kMaxTiledParticles) {
+    set_error("the tiled path holds at most %d particles per solver (got %d)", kMaxTiledParticles, n);
+    return WCSPH_E_CAPACITY;
+  }
+  switch (shape) {
+    case 1: return launch_pair_tiled_v<PASS, H16, 2, 512>(a, s);
+    case 2: return launch_pair_tiled_v<PASS, H16, 2, 1024>(a, s);
+    default: return launch_pair_tiled_v<PASS, H16, 4, 512>(a, s);
+  }
 }
 
 }  // namespace wcsph

@@ -14,6 +14,8 @@ namespace wcsph {
 void set_error(const char* fmt, ...);
 int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
 
+inline int cuda_fail_if(cudaError_t e) { return e == cudaSuccess ? 0 : cuda_fail(e, "kernel launch", __FILE__, __LINE__); }
+
 #define WCSPH_CUDA(call)                                                 \
   do {                                                                   \
     cudaError_t e_ = (call);                                             \
@@ -130,19 +132,25 @@ __device__ __forceinline__ bool neighbor_cell(const InstParams& P, int k, int q,
   return true;
 }
 
-// Tait EoS (EoS.h:75-90).  x = rho/rho0.
+// Tait EoS (EoS.h:75-90): P = max(B ((rho/rho0)^gamma - 1), 0),
+// c = sqrt(max(B gamma/rho0 (rho/rho0)^(gamma-1), 1e-16)).
+// (rho/rho0)^gamma - 1 is evaluated on d = (rho - rho0)/rho0 without the
+// cancellation of x^gamma - 1 near rho0 (weakly compressible: |d| ~ 1e-3):
+// for gamma = 7 the binomial expansion d (7 + d (21 + d (35 + ...))) in Horner
+// form, otherwise expm1(gamma log1p(d)).
 __device__ __forceinline__ void tait(const InstParams& P, float rho, float& pres, float& snds) {
-  const float x = rho * P.inv_rho0;
-  float xg, xg1;
+  const float d = (rho - P.rho0) * P.inv_rho0;
+  float xgm1, xg1;
   if (P.gamma == 7.0f) {
-    const float x2 = x * x, x3 = x2 * x;
+    xgm1 = d * (7.0f + d * (21.0f + d * (35.0f + d * (35.0f + d * (21.0f + d * (7.0f + d))))));
+    const float x = 1.0f + d, x2 = x * x, x3 = x2 * x;
     xg1 = x3 * x3;
-    xg = xg1 * x;
   } else {
-    xg = powf(x, P.gamma);
-    xg1 = powf(x, P.gamma - 1.0f);
+    const float l = log1pf(d);
+    xgm1 = expm1f(P.gamma * l);
+    xg1 = expf((P.gamma - 1.0f) * l);
   }
-  pres = fmaxf(P.B * (xg - 1.0f), 0.0f);
+  pres = fmaxf(P.B * xgm1, 0.0f);
   snds = sqrtf(fmaxf(P.cs2_coef * xg1, 1.0e-16f));
 }
 

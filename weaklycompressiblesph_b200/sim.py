@@ -25,7 +25,7 @@ def _f32(a, shape):
 
 class Solver:
     def __init__(self, max_particles, precision=N.PREC_FP32, max_cells=None, max_instances=64, device=0,
-                 use_graph=True):
+                 use_graph=True, autotune=True):
         o = N.SimOptions()
         o.device = device
         o.precision = precision
@@ -33,6 +33,7 @@ class Solver:
         o.max_cells = int(max_cells if max_cells is not None else max(1 << 20, 2 * max_particles))
         o.max_instances = int(max_instances)
         o.use_graph = 1 if use_graph else 0
+        o.autotune = 1 if autotune else 0
         self.opt = o
         h = C.c_void_p()
         N.call("wcsph_sim_create", C.byref(o), C.byref(h))
@@ -42,7 +43,7 @@ class Solver:
     @staticmethod
     def device_bytes(max_particles, max_cells=None, max_instances=64):
         o = N.SimOptions(0, 0, int(max_particles), int(max_cells or max(1 << 20, 2 * max_particles)),
-                         int(max_instances), 1)
+                         int(max_instances), 1, 0, 0)
         return int(N.lib().wcsph_sim_device_bytes(C.byref(o)))
 
     def close(self):
@@ -134,6 +135,12 @@ class Solver:
 
     def kernels_per_step(self):
         return int(N.lib().wcsph_sim_kernels_per_step(self._h))
+
+    def tuning(self):
+        """Autotuner decision: tile shape, density kernel (0 per-thread, 1 tiled), tuned bucket."""
+        out = np.zeros(3, np.int32)
+        N.call("wcsph_sim_tuning", self._h, N.ptr(out, C.c_int32))
+        return dict(tile_shape=int(out[0]), density_tiled=bool(out[1]), bucket=int(out[2]))
 
     def stream(self):
         """The solver's cudaStream_t as an integer handle."""
