@@ -250,10 +250,11 @@ int wcsph_sim_conservation(wcsph_sim* sim, int32_t slot, double* out6);
 int64_t wcsph_sim_last_pairs(wcsph_sim* sim);
 /* Number of kernel launches per step issued by the solver (for accounting). */
 int32_t wcsph_sim_kernels_per_step(wcsph_sim* sim);
-/* The autotuner's current choice: out[0] tile shape of the tiled pair kernels
- * (0: 4 warps x 512 candidates, 1: 2 x 512, 2: 2 x 1024), out[1] density
- * kernel (0 per-thread, 1 tiled), out[2] log2 particle bucket it was tuned
- * for (-1: defaults, not tuned). */
+/* The autotuner's current choice: out[0] block shape of the tiled hydro
+ * kernel (0: 4 warps, 1: 2 warps, 2: 8 warps per block, 512-candidate tiles;
+ * the shapes share their arithmetic, so results do not depend on the choice),
+ * out[1] density kernel (always 0: per-thread), out[2] log2 particle bucket it
+ * was tuned for (-1: defaults, not tuned). */
 int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out3);
 /* The solver's CUDA stream (a cudaStream_t), so callers can record events on it. */
 void* wcsph_sim_stream(wcsph_sim* sim);

@@ -65,7 +65,6 @@ struct SimImpl {
   int key_bits = 1;
   long long total_cells = 0;
   bool any_density = false;
-  bool density_tiled = false;  // density pass kernel: per-thread (default) or tiled, chosen by the autotuner
   int tile_shape = 0;          // tiled pair-kernel shape, chosen by the autotuner
   int tuned_bucket = -1;       // log2 particle bucket of the last tuning
   cudaGraphExec_t gexec = nullptr;
@@ -208,11 +207,7 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));
     if (density) {
-      if (!S.density_tiled) {
-        k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(a);
-      } else {
-        if (int rc = launch_pair_tiled<PASS_DENSITY>(a, n, S.s, S.tile_shape)) return rc;
-      }
+      k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(a);
       k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
       L += 2;
     }
@@ -220,9 +215,9 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
     if (S.opt.precision == WCSPH_PREC_FP32) {
       k_hydro_plain<true><<<nblk(n), kBlock, 0, S.s>>>(a);
     } else if (S.opt.precision == WCSPH_PREC_TILED) {
-      if (int rc = launch_pair_tiled<PASS_HYDRO>(a, n, S.s, S.tile_shape)) return rc;
+      if (int rc = launch_hydro_tiled<false>(a, n, S.s, S.tile_shape)) return rc;
     } else {
-      if (int rc = launch_pair_tiled<PASS_HYDRO, true>(a, n, S.s, S.tile_shape)) return rc;
+      if (int rc = launch_hydro_tiled<true>(a, n, S.s, S.tile_shape)) return rc;
     }
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[3], S.s));
@@ -231,11 +226,7 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
     if (init_filter) {
       StepArgs b = a;
       b.init_filter = 1;
-      if (!S.density_tiled) {
-        k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(b);
-      } else {
-        if (int rc = launch_pair_tiled<PASS_DENSITY>(b, n, S.s, S.tile_shape)) return rc;
-      }
+      k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(b);
       k_apply_init_filter<<<nblk(n), kBlock, 0, S.s>>>(b);
       L += 2;
     }
@@ -278,10 +269,12 @@ static int time_launches(SimImpl& S, int reps, F&& fn, float* ms) {
   return 0;
 }
 
-// Autotuner: on the live instance set, time every tile shape of the tiled
-// hydro kernel and the per-thread vs tiled density kernel with probe passes
-// (forces go to the diagnostic arrays, the state is untouched), keep the
-// fastest.  Re-tuned only when the particle count crosses a power of two.
+// Autotuner: on the live instance set, time every block shape of the tiled
+// hydro kernel with probe passes (forces go to the diagnostic arrays, the
+// state is untouched) and keep the fastest.  The candidates share their
+// arithmetic exactly, so the choice never changes a result (an instance is
+// bit-identical alone and in a mix).  Re-tuned only when the particle count
+// crosses a power of two.
 static int autotune(SimImpl& S) {
   if (!S.opt.autotune || S.opt.precision == WCSPH_PREC_FP32 || S.n_host <= 0) return 0;
   int bucket = 0;
@@ -299,20 +292,12 @@ static int autotune(SimImpl& S) {
   int best_shape = 0;
   for (int v = 0; v < kTileShapes; ++v) {
     int rc = time_launches(S, 3, [&]() {
-      return h16 ? launch_pair_tiled<PASS_HYDRO, true>(a, n, S.s, v) : launch_pair_tiled<PASS_HYDRO>(a, n, S.s, v);
+      return h16 ? launch_hydro_tiled<true>(a, n, S.s, v) : launch_hydro_tiled<false>(a, n, S.s, v);
     }, &ms);
     if (rc) return rc;
     if (ms < best) best = ms, best_shape = v;
   }
   S.tile_shape = best_shape;
-  float ms_plain = 0.f, ms_tiled = 0.f;
-  if (int rc = time_launches(S, 3, [&]() {
-        k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(a);
-        return cuda_fail_if(cudaGetLastError());
-      }, &ms_plain)) return rc;
-  if (int rc = time_launches(S, 3, [&]() { return launch_pair_tiled<PASS_DENSITY>(a, n, S.s, S.tile_shape); },
-                             &ms_tiled)) return rc;
-  S.density_tiled = ms_tiled < ms_plain;
   S.tuned_bucket = bucket;
   S.graph_dirty = true;
   return set_all_phases(S, PH_STEP);
@@ -833,7 +818,7 @@ void* wcsph_sim_stream(wcsph_sim* sim) { return sim ? (void*)sim->impl.s : nullp
 int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out3) {
   if (!sim || !out3) return WCSPH_E_INVALID;
   out3[0] = sim->impl.tile_shape;
-  out3[1] = sim->impl.density_tiled ? 1 : 0;
+  out3[1] = 0;  // the density pass always uses the per-thread kernel
   out3[2] = sim->impl.tuned_bucket;
   return 0;
 }

@@ -1,4 +1,4 @@
-// Tiled pair kernels (WCSPH_PREC_TILED): one warp per non-empty cell.
+// Tiled hydro kernel (WCSPH_PREC_TILED, WCSPH_PREC_HALF2): one warp per non-empty cell.
 //
 //   1. The 27 neighbour cells of the warp's cell are flattened into one
 //      candidate list and staged into the warp's shared-memory tile as
@@ -202,56 +202,6 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
   }
 }
 
-// Density sums of i_a / i_b over their queues: sum w and sum w / rho_j
-// (w = (1-s)+^3 - 4 (1/2-s)+^3, the cubic spline without its normalisation),
-// added into res[.][0], res[.][1]; count into res[.][5].
-__device__ __forceinline__ void density_queues2(const StepArgs& a, const InstParams& P, int ia, bool has_b,
-                                                const float4& IA, const float4& IBp, const uint32_t* qa, int na,
-                                                const uint32_t* qb, int nb, float (*res)[6], int lane) {
-  const f2 X = pk(IA.x, IBp.x), Y = pk(IA.y, IBp.y), Z = pk(IA.z, IBp.z);
-  const float H2 = P.H2;
-  const f2 IH = dup(P.inv_H), ONE = dup(1.0f), HALF = dup(0.5f), MFOUR = dup(-4.0f);
-  const bool per = P.periodic;
-  const int nbq = has_b ? nb : 0;
-  const int n = max(na, nbq);
-  f2 SW = 0ull, SO = 0ull;
-  for (int k = lane; k < n; k += 32) {
-    const bool va = k < na, vb = k < nbq;
-    const uint32_t self = (uint32_t)ia | (13u << 27);
-    const uint32_t ea = va ? qa[k] : self, eb = vb ? qb[k] : self;
-    const int ga = ea & kSlotMask, gb = eb & kSlotMask;
-    const float4 Ja = __ldg(&a.jA[ga]), Jb = __ldg(&a.jA[gb]);
-    const f2 RJ = pk(__ldg(&a.jB[ga].w), __ldg(&a.jB[gb].w));
-    float jxa = Ja.x, jya = Ja.y, jza = Ja.z, jxb = Jb.x, jyb = Jb.y, jzb = Jb.z;
-    if (per) {
-      float sx, sy, sz;
-      entry_shift(P, ea >> 27, sx, sy, sz);
-      jxa = __fadd_rn(jxa, sx), jya = __fadd_rn(jya, sy), jza = __fadd_rn(jza, sz);
-      entry_shift(P, eb >> 27, sx, sy, sz);
-      jxb = __fadd_rn(jxb, sx), jyb = __fadd_rn(jyb, sy), jzb = __fadd_rn(jzb, sz);
-    }
-    const f2 DX = sub2(X, pk(jxa, jxb)), DY = sub2(Y, pk(jya, jyb)), DZ = sub2(Z, pk(jza, jzb));
-    const f2 R2raw = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
-    const f2 R2 = pk(va ? lo(R2raw) : H2, vb ? hi(R2raw) : H2);
-    const f2 S = mul2(mul2(R2, rsqrt2(R2)), IH);
-    const f2 A = max0_2(sub2(ONE, S)), B = max0_2(sub2(HALF, S));
-    const f2 Wf = mul2(fma2(MFOUR, mul2(B, mul2(B, B)), mul2(A, mul2(A, A))), pk(va ? 1.0f : 0.0f, vb ? 1.0f : 0.0f));
-    SW = add2(SW, Wf);
-    SO = fma2(Wf, rcp2(RJ), SO);
-  }
-  const float v8[8] = {lo(SW), lo(SO), 0.f, 0.f, hi(SW), hi(SO), 0.f, 0.f};
-  const float y = butterfly8(v8, lane);
-  if ((lane & 3) == 0) {
-    const int slot = lane >> 2;
-    if (slot < 2) res[0][slot] += y;
-    else if (slot >= 4 && slot < 6 && has_b) res[1][slot - 4] += y;
-  }
-  if (lane == 0) {
-    res[0][5] += (float)na;
-    if (has_b) res[1][5] += (float)nb;
-  }
-}
-
 // Append the in-support candidates (even/odd halves of the lane's pair) to a queue.
 __device__ __forceinline__ void append2(uint32_t* q, int& n, bool he, bool ho, uint32_t ee, uint32_t eo, unsigned lt) {
   const unsigned me = __ballot_sync(0xffffffffu, he), mo = __ballot_sync(0xffffffffu, ho);
@@ -261,10 +211,8 @@ __device__ __forceinline__ void append2(uint32_t* q, int& n, bool he, bool ho, u
   n += __popc(me) + __popc(mo);
 }
 
-enum PairPass { PASS_HYDRO = 0, PASS_DENSITY = 1 };
-
-template <int PASS, bool H16, int WARPS, int TILE>
-__global__ void __launch_bounds__(WARPS * 32) k_pair_tiled(StepArgs a) {
+template <bool H16, int WARPS, int TILE>
+__global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
   constexpr int kTiledWarps = WARPS;
   constexpr int kTile = TILE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -294,12 +242,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_pair_tiled(StepArgs a) {
     const int inst = f0 & kInstMask;
     const InstParams& P = a.params[inst];
     const int ph = a.phase[inst];
-    const int dkind = PASS == PASS_DENSITY ? density_kind(a, P, a.dyn[inst], ph) : 0;
-    if (PASS == PASS_HYDRO && !wants_force(P, a.dyn[inst], ph)) {
+    if (!wants_force(P, a.dyn[inst], ph)) {
       for (int p = s + lane; p < e; p += 32) copy_state(a, p);
       continue;
     }
-    if (PASS == PASS_DENSITY && !dkind) continue;
     const int nx = P.ncell[0], ny = P.ncell[1];
     const int local = lin - P.cell_base;
     const int cx = local % nx, cy = (local / nx) % ny, cz = local / (nx * ny);
@@ -407,8 +353,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_pair_tiled(StepArgs a) {
             append2(qb, nb, has_b && rb0 > 0.0f && rb0 < H2, has_b && rb1 > 0.0f && rb1 < H2, E.x, E.y, lt);
           }
           __syncwarp();
-          if (PASS == PASS_HYDRO) hydro_queues2<H16>(a, P, ia, ibb, has_b, IA, IB, qa, na, qb, nb, &res[ii], lane);
-          else density_queues2(a, P, ia, has_b, IA, IB, qa, na, qb, nb, &res[ii], lane);
+          hydro_queues2<H16>(a, P, ia, ibb, has_b, IA, IB, qa, na, qb, nb, &res[ii], lane);
           __syncwarp();
         }
       }
@@ -416,23 +361,16 @@ __global__ void __launch_bounds__(WARPS * 32) k_pair_tiled(StepArgs a) {
       if (lane < nbat) {
         const int p = ib + lane;
         const float* r = res[lane];
-        if (PASS == PASS_HYDRO) {
-          pairs += (unsigned long long)r[5];
-          finish_hydro(a, p, P, inst, ph, a.alt.flags[p], r[0], r[1], r[2], r[3], r[4], (unsigned)r[5], dt_cand,
-                       dt_valid);
-        } else {  // self term w(0) = 1/2 (force.h:16-20 lists contain i)
-          const float sum = 0.5f + r[0];
-          a.rho_new[p] = dkind == 2 ? sum / (0.5f / a.jB[p].w + r[1]) : P.mass * P.Kw * sum;
-        }
+        pairs += (unsigned long long)r[5];
+        finish_hydro(a, p, P, inst, ph, a.alt.flags[p], r[0], r[1], r[2], r[3], r[4], (unsigned)r[5], dt_cand,
+                     dt_valid);
       }
     }
-    if (PASS == PASS_HYDRO) dt_min(a.dyn, inst, dt_cand, dt_valid);
+    dt_min(a.dyn, inst, dt_cand, dt_valid);
   }
-  if (PASS == PASS_HYDRO) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(full, pairs, o);
-    if (lane == 0 && pairs) atomicAdd(a.pair_count, pairs);
-  }
+  for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(full, pairs, o);
+  if (lane == 0 && pairs) atomicAdd(a.pair_count, pairs);
 }
 
 struct TiledLaunch {
@@ -440,13 +378,13 @@ struct TiledLaunch {
   int blocks = 0;
 };
 
-template <int PASS, bool H16, int WARPS, int TILE>
+template <bool H16, int WARPS, int TILE>
 inline int launch_pair_tiled_v(const StepArgs& a, cudaStream_t s) {
   static TiledLaunch L[16];
   int dev = 0;
   WCSPH_CUDA(cudaGetDevice(&dev));
   TiledLaunch& T = L[dev & 15];
-  auto kern = k_pair_tiled<PASS, H16, WARPS, TILE>;
+  auto kern = k_hydro_tiled<H16, WARPS, TILE>;
   const int bytes = (int)sizeof(TiledSmem<WARPS, TILE>);
   if (T.device != dev) {
     WCSPH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
@@ -461,23 +399,21 @@ inline int launch_pair_tiled_v(const StepArgs& a, cudaStream_t s) {
   return 0;
 }
 
-// Tile shapes the autotuner chooses among: (warps per block, candidates per tile).
+// Block shapes the autotuner chooses among (warps per block, at a fixed
+// 512-candidate tile).  They change only how cells map to blocks, never the
+// order of any sum, so results are bit-identical whichever is chosen.
 constexpr int kTileShapes = 3;
-inline const char* tile_shape_name(int v) {
-  static const char* names[kTileShapes] = {"4 warps x 512", "2 warps x 512", "2 warps x 1024"};
-  return (v >= 0 && v < kTileShapes) ? names[v] : "?";
-}
 
-template <int PASS, bool H16 = false>
-inline int launch_pair_tiled(const StepArgs& a, int n, cudaStream_t s, int shape = 0) {
+template <bool H16>
+inline int launch_hydro_tiled(const StepArgs& a, int n, cudaStream_t s, int shape = 0) {
   if (n > kMaxTiledParticles) {
     set_error("the tiled path holds at most %d particles per solver (got %d)", kMaxTiledParticles, n);
     return WCSPH_E_CAPACITY;
   }
   switch (shape) {
-    case 1: return launch_pair_tiled_v<PASS, H16, 2, 512>(a, s);
-    case 2: return launch_pair_tiled_v<PASS, H16, 2, 1024>(a, s);
-    default: return launch_pair_tiled_v<PASS, H16, 4, 512>(a, s);
+    case 1: return launch_pair_tiled_v<H16, 2, 512>(a, s);
+    case 2: return launch_pair_tiled_v<H16, 8, 512>(a, s);
+    default: return launch_pair_tiled_v<H16, 4, 512>(a, s);
   }
 }
 
