@@ -215,6 +215,22 @@ int64_t wcsph_sim_device_bytes(const wcsph_sim_options* opt);
  * (main.cpp:69-78) before returning.  *slot receives the instance handle. */
 int wcsph_sim_add_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, const float* pos3, const float* vel3,
                            const float* dens, const int32_t* type, int32_t* slot);
+/* Restore an instance from a restart file's state (io.h:60-84 reads the
+ * reference's binary dumps): positions, velocities, densities, types, the
+ * last force pass's acc3 and div_v, the physical time, step count and the dt
+ * of the next step.  No force pass is run, so stepping continues exactly where
+ * the saved run stopped.  alive (may be NULL) drops particles with alive[i] = 0;
+ * they keep their original index in reads.  order (may be NULL) is the
+ * sequence in which the particles are stored on the device, a permutation of
+ * 0..n-1 (wcsph_sim_read_order's perm followed by the dead particles): the
+ * binning sort is stable, so with the saved order the neighbour sums run in
+ * the same sequence and the continuation is bit-identical. */
+int wcsph_sim_restore_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, const float* pos3, const float* vel3,
+                               const float* dens, const int32_t* type, const float* acc3, const float* div_v,
+                               const int32_t* alive, const int32_t* order, double time, int64_t steps,
+                               float dt_next, int32_t* slot);
+/* dt the instance's next step will use (its CFL minimum from the last force pass). */
+int wcsph_sim_next_dt(wcsph_sim* sim, int32_t slot, float* dt_next);
 /* Remove an instance; its particles and cells are reclaimed at the next step. */
 int wcsph_sim_remove_instance(wcsph_sim* sim, int32_t slot);
 

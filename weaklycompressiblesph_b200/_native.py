@@ -89,6 +89,9 @@ _SIGS = {
     "wcsph_sim_destroy": (C.c_int, [P]),
     "wcsph_sim_device_bytes": (C.c_int64, [C.POINTER(SimOptions)]),
     "wcsph_sim_add_instance": (C.c_int, [P, C.POINTER(InstanceDesc), F32P, F32P, F32P, I32P, I32P]),
+    "wcsph_sim_restore_instance": (C.c_int, [P, C.POINTER(InstanceDesc), F32P, F32P, F32P, I32P, F32P, F32P, I32P,
+                                              I32P, C.c_double, C.c_int64, C.c_float, I32P]),
+    "wcsph_sim_next_dt": (C.c_int, [P, C.c_int32, F32P]),
     "wcsph_sim_remove_instance": (C.c_int, [P, C.c_int32]),
     "wcsph_sim_step": (C.c_int, [P, C.c_int32]),
     "wcsph_sim_synchronize": (C.c_int, [P]),

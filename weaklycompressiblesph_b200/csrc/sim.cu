@@ -482,14 +482,16 @@ int wcsph_sim_destroy(wcsph_sim* sim) {
   return 0;
 }
 
-int wcsph_sim_add_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, const float* pos3, const float* vel3,
-                           const float* dens, const int32_t* type, int32_t* slot) {
-  if (!sim || !desc || !pos3 || !vel3 || !dens || !type) {
-    set_error("wcsph_sim_add_instance: null argument");
-    return WCSPH_E_INVALID;
-  }
-  SimImpl& S = sim->impl;
-  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+}  // extern "C"
+
+namespace wcsph {
+// Append an instance's particles at [n_host, n_host + n) and register it.
+// With init_pass the initial force pass (main.cpp:69-78) runs for it alone;
+// otherwise acc3/div_v and *dyn are taken as saved state (restart).
+static int append_instance(SimImpl& S, const wcsph_instance_desc* desc, const float* pos3, const float* vel3,
+                           const float* dens, const int32_t* type, const float* acc3, const float* div_v,
+                           const int32_t* alive, const int32_t* order, const InstDyn* saved, bool init_pass,
+                           int32_t* slot) {
   if (int rc = sync_compact(S)) return rc;
   bool draining = false;
   for (auto& I : S.inst) draining |= I.used && !I.active;
@@ -503,7 +505,7 @@ int wcsph_sim_add_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, cons
     if (int rc = sync_compact(S)) return rc;
   }
   if ((long long)S.n_host + desc->n > S.opt.max_particles) {
-    set_error("wcsph_sim_add_instance: %d + %d particles exceed capacity %lld", S.n_host, desc->n,
+    set_error("adding an instance: %d + %d particles exceed capacity %lld", S.n_host, desc->n,
               (long long)S.opt.max_particles);
     return WCSPH_E_CAPACITY;
   }
@@ -515,7 +517,7 @@ int wcsph_sim_add_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, cons
     }
   if (k < 0) {
     if ((int)S.inst.size() >= S.opt.max_instances) {
-      set_error("wcsph_sim_add_instance: all %d instance slots are in use", S.opt.max_instances);
+      set_error("adding an instance: all %d instance slots are in use", S.opt.max_instances);
       return WCSPH_E_CAPACITY;
     }
     k = (int)S.inst.size();
@@ -527,13 +529,13 @@ int wcsph_sim_add_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, cons
   InstParams P;
   if (int rc = fill_params(*desc, I, P)) return rc;
   I.used = I.active = true;
-  HostInst saved = S.inst[k];
-  InstParams saved_p = S.h_params[k];
+  HostInst prev = S.inst[k];
+  InstParams prev_p = S.h_params[k];
   S.inst[k] = I;
   S.h_params[k] = P;
   if (int rc = rebuild_tables(S)) {
-    S.inst[k] = saved;
-    S.h_params[k] = saved_p;
+    S.inst[k] = prev;
+    S.h_params[k] = prev_p;
     rebuild_tables(S);
     return rc;
   }
@@ -542,11 +544,13 @@ int wcsph_sim_add_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, cons
   std::vector<float4> pos(n), vel(n), acc(n, make_float4(0, 0, 0, 0));
   std::vector<int> pid(n);
   std::vector<uint32_t> flags(n);
-  for (int i = 0; i < n; ++i) {
-    pos[i] = make_float4(pos3[3 * i], pos3[3 * i + 1], pos3[3 * i + 2], dens[i]);
-    vel[i] = make_float4(vel3[3 * i], vel3[3 * i + 1], vel3[3 * i + 2], 0.f);
-    pid[i] = i;
-    flags[i] = (uint32_t)k | (type[i] == WCSPH_FREEZE ? kFreezeBit : 0u);
+  for (int q = 0; q < n; ++q) {
+    const int i = order ? order[q] : q;  // storage position q holds particle i
+    pos[q] = make_float4(pos3[3 * i], pos3[3 * i + 1], pos3[3 * i + 2], dens[i]);
+    vel[q] = make_float4(vel3[3 * i], vel3[3 * i + 1], vel3[3 * i + 2], 0.f);
+    if (acc3) acc[q] = make_float4(acc3[3 * i], acc3[3 * i + 1], acc3[3 * i + 2], div_v ? div_v[i] : 0.f);
+    pid[q] = i;
+    flags[q] = (uint32_t)k | (type[i] == WCSPH_FREEZE ? kFreezeBit : 0u) | (alive && !alive[i] ? kDeadBit : 0u);
   }
   WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.pos + base, pos.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, S.s));
   WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.vel + base, vel.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, S.s));
@@ -555,8 +559,22 @@ int wcsph_sim_add_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, cons
   WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.flags + base, flags.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, S.s));
   InstDyn dyn{};
   dyn.dt_next_bits = 0x7f800000u;
+  if (saved) dyn = *saved;
   WCSPH_CUDA(cudaMemcpyAsync(S.d_dyn + k, &dyn, sizeof(InstDyn), cudaMemcpyHostToDevice, S.s));
   S.n_host = base + n;
+  if (!init_pass) {
+    // One pass with every instance idle bins the restored particles (their
+    // keys come from the saved positions, so a saved sorted order stays as
+    // it is) and sets the instance's range; no state changes.
+    for (size_t q = 0; q < S.inst.size(); ++q) S.h_phase[q] = PH_IDLE;
+    if (int rc = upload_tables(S)) return rc;
+    if (int rc = enqueue_pass(S, make_args(S), false, false, nullptr)) return rc;
+    if (int rc = set_all_phases(S, PH_STEP)) return rc;
+    WCSPH_CUDA(cudaStreamSynchronize(S.s));
+    S.graph_dirty = true;
+    if (slot) *slot = k;
+    return 0;
+  }
   // Initial force pass for this instance only (main.cpp:69-78).
   for (size_t q = 0; q < S.inst.size(); ++q) S.h_phase[q] = PH_IDLE;
   S.h_phase[k] = PH_INIT;
@@ -568,6 +586,65 @@ int wcsph_sim_add_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, cons
   WCSPH_CUDA(cudaStreamSynchronize(S.s));
   S.graph_dirty = true;
   if (slot) *slot = k;
+  return 0;
+}
+
+}  // namespace wcsph
+
+extern "C" {
+
+int wcsph_sim_add_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, const float* pos3, const float* vel3,
+                           const float* dens, const int32_t* type, int32_t* slot) {
+  if (!sim || !desc || !pos3 || !vel3 || !dens || !type) {
+    set_error("wcsph_sim_add_instance: null argument");
+    return WCSPH_E_INVALID;
+  }
+  WCSPH_CUDA(cudaSetDevice(sim->impl.opt.device));
+  return append_instance(sim->impl, desc, pos3, vel3, dens, type, nullptr, nullptr, nullptr, nullptr, nullptr, true,
+                         slot);
+}
+
+int wcsph_sim_restore_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, const float* pos3, const float* vel3,
+                               const float* dens, const int32_t* type, const float* acc3, const float* div_v,
+                               const int32_t* alive, const int32_t* order, double time, int64_t steps,
+                               float dt_next, int32_t* slot) {
+  if (!sim || !desc || !pos3 || !vel3 || !dens || !type || !acc3 || !div_v || !(dt_next > 0.f) || time < 0.0 ||
+      steps < 0 || desc->n <= 0) {
+    set_error("wcsph_sim_restore_instance: null argument, empty instance, non-positive dt_next or negative time");
+    return WCSPH_E_INVALID;
+  }
+  if (order) {
+    std::vector<char> seen(desc->n, 0);
+    for (int q = 0; q < desc->n; ++q) {
+      if (order[q] < 0 || order[q] >= desc->n || seen[order[q]]) {
+        set_error("wcsph_sim_restore_instance: order is not a permutation of 0..%d (entry %d)", desc->n - 1, q);
+        return WCSPH_E_INVALID;
+      }
+      seen[order[q]] = 1;
+    }
+  }
+  WCSPH_CUDA(cudaSetDevice(sim->impl.opt.device));
+  InstDyn dyn{};
+  dyn.time = time;
+  dyn.steps = steps;
+  memcpy(&dyn.dt_next_bits, &dt_next, sizeof(float));
+  dyn.finished = (desc->t_end > 0.0 && time >= desc->t_end) ? 1 : 0;
+  dyn.range_lo = 0x7fffffff;
+  return append_instance(sim->impl, desc, pos3, vel3, dens, type, acc3, div_v, alive, order, &dyn, false, slot);
+}
+
+int wcsph_sim_next_dt(wcsph_sim* sim, int32_t slot, float* dt_next) {
+  if (!sim || !dt_next) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  if (slot < 0 || slot >= (int)S.inst.size() || !S.inst[slot].used) {
+    set_error("wcsph_sim_next_dt: slot %d is not in use", slot);
+    return WCSPH_E_INVALID;
+  }
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  InstDyn d;
+  WCSPH_CUDA(cudaMemcpy(&d, S.d_dyn + slot, sizeof(InstDyn), cudaMemcpyDeviceToHost));
+  memcpy(dt_next, &d.dt_next_bits, sizeof(float));
   return 0;
 }
 

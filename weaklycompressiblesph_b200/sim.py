@@ -8,6 +8,7 @@ the device for every instance at once).
 from __future__ import annotations
 
 import ctypes as C
+from types import SimpleNamespace
 
 import numpy as np
 
@@ -75,6 +76,34 @@ class Solver:
                N.ptr(dens, C.c_float), N.ptr(typ, C.c_int32), C.byref(slot))
         self.slots[slot.value] = case
         return slot.value
+
+    def restore(self, case, state, desc=None) -> int:
+        """Add an instance from saved state (a dict with pos, vel, dens, acc,
+        div_v, time, steps, dt_next and optionally alive, order, type; see
+        snapshot.py) without a force pass, so that it continues exactly where
+        the saved run stopped.  case may be None when desc and state["type"]
+        are given."""
+        d = desc if desc is not None else case.desc()
+        n = int(d.n)
+        typ = state.get("type", None if case is None else case.type)
+        f = lambda a, shape: np.ascontiguousarray(np.asarray(a, np.float32).reshape(shape))
+        i32 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.int32)
+        typ, alive, order = i32(typ), i32(state.get("alive")), i32(state.get("order"))
+        if typ is None or len(typ) != n:
+            raise ValueError("restore: particle types of length desc.n are required")
+        slot = C.c_int32()
+        N.call("wcsph_sim_restore_instance", self._h, C.byref(d), N.ptr(f(state["pos"], (n, 3)), C.c_float),
+               N.ptr(f(state["vel"], (n, 3)), C.c_float), N.ptr(f(state["dens"], (n,)), C.c_float),
+               N.ptr(typ, C.c_int32), N.ptr(f(state["acc"], (n, 3)), C.c_float),
+               N.ptr(f(state["div_v"], (n,)), C.c_float), N.ptr(alive, C.c_int32), N.ptr(order, C.c_int32),
+               float(state["time"]), int(state["steps"]), float(state["dt_next"]), C.byref(slot))
+        self.slots[slot.value] = case if case is not None else SimpleNamespace(n=n, type=typ)
+        return slot.value
+
+    def next_dt(self, slot):
+        v = C.c_float()
+        N.call("wcsph_sim_next_dt", self._h, slot, C.byref(v))
+        return v.value
 
     def remove(self, slot):
         N.call("wcsph_sim_remove_instance", self._h, slot)
