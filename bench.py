@@ -312,14 +312,14 @@ def measure_ensemble(device, steps=None):
 
 def measure_serving(device):
     """Config 5 sample: Poisson(20/s) dam-break requests, fluid counts
-    log-uniform in [2e4, 2e5] (config: up to 2e6), each run to t = 0.02 s
+    log-uniform in [2e4, 2e5] (config: up to 2e6), each run to t = 0.1 s
     (config: 1.0 s), admitted by a 150 GB HBM budget; p50/p99
     time-to-completion and aggregate particle-steps/s, vs the same requests
     one at a time on the plain FP32 path."""
     from weaklycompressiblesph_b200 import _native as N
     from weaklycompressiblesph_b200 import cases
     from weaklycompressiblesph_b200.serving import Server, run_alone
-    reqs = cases.serving_requests(count=16, rate=20.0, seed=7, n_min=2e4, n_max=2e5, t_end=0.02)
+    reqs = cases.serving_requests(count=16, rate=20.0, seed=7, n_min=2e4, n_max=2e5, t_end=0.1)
     total = sum(c.n for _, c in reqs)
     with Server(budget_bytes=150e9, max_particles=total + 1024, device=device, read_results=False) as srv:
         out = srv.run(reqs)
@@ -333,7 +333,7 @@ def measure_serving(device):
             "wall_s": out["wall_s"], "particle_steps_per_s": out["particle_steps_per_s"],
             "serial_plain_particle_steps_per_s": ps / el,
             "speedup_vs_serial_plain": out["particle_steps_per_s"] / (ps / el),
-            "sample": "16 requests, counts log-uniform [2e4, 2e5], t_end 0.02 s, Poisson 20/s, budget 150 GB "
+            "sample": "16 requests, counts log-uniform [2e4, 2e5], t_end 0.1 s, Poisson 20/s, budget 150 GB "
                       "(config: counts to 2e6, t_end 1.0 s)"}
 
 

@@ -48,7 +48,7 @@ struct SimImpl {
   int* d_phase = nullptr;
   int* d_n_alive = nullptr;
   int* run_list = nullptr;
-  int* d_counters = nullptr;  // [0] run_count, [1] work_counter
+  int* d_counters = nullptr;  // [0] run_count
   unsigned long long* d_pairs = nullptr;
   double* d_cons = nullptr;
   float4* diag_acc = nullptr;
@@ -164,8 +164,6 @@ static StepArgs make_args(SimImpl& S) {
   a.pair_count = S.d_pairs;
   a.run_list = S.run_list;
   a.run_count = S.d_counters;
-  a.work_counter = S.d_counters + 1;
-  a.work_counter2 = S.d_counters + 2;
   a.diag_acc = S.diag_acc;
   a.diag_dt = S.diag_dt;
   a.diag_nbr = S.diag_nbr;
@@ -202,7 +200,7 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
       WCSPH_CUDA(cudaMemsetAsync(S.cell_start, 0, sizeof(int) * S.total_cells, S.s));
       WCSPH_CUDA(cudaMemsetAsync(S.cell_end, 0, sizeof(int) * S.total_cells, S.s));
     }
-    WCSPH_CUDA(cudaMemsetAsync(S.d_counters, 0, 3 * sizeof(int), S.s));
+    WCSPH_CUDA(cudaMemsetAsync(S.d_counters, 0, sizeof(int), S.s));
     k_permute<<<nblk(n), kBlock, 0, S.s>>>(a);
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));

@@ -37,8 +37,6 @@ struct StepArgs {
   unsigned long long* pair_count;
   int* run_list;          // linear index of every non-empty cell (unordered)
   int* run_count;         // number of entries in run_list
-  int* work_counter;      // cells taken so far by the persistent tiled hydro kernel
-  int* work_counter2;     // the same for the tiled density kernel
   int init_filter;        // initial-pass Shepard filter launch (main.cpp:75)
   int probe_density;      // density pass of a probe launch: 0 none, 1 summation, 2 Shepard
   // diagnostics (probe phase)
