@@ -231,6 +231,52 @@ int wcsph_sim_restore_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, 
                                float dt_next, int32_t* slot);
 /* dt the instance's next step will use (its CFL minimum from the last force pass). */
 int wcsph_sim_next_dt(wcsph_sim* sim, int32_t slot, float* dt_next);
+/* Overwrite it (e.g. with the minimum over the slabs of one simulation). */
+int wcsph_sim_set_next_dt(wcsph_sim* sim, int32_t slot, float dt_next);
+/* The initial force pass of an instance (main.cpp:69-78) on its current
+ * particles: run by wcsph_sim_add_instance itself, and by a slab rank once
+ * its first ghost layer is in place. */
+int wcsph_sim_force_pass(wcsph_sim* sim, int32_t slot);
+
+/* ---- slab decomposition: one simulation over several solvers ------------
+ * Replaces FDPS's domain decomposition and particle exchange
+ * (main.cpp:61-62,109-110).  Each rank owns the particles with x in
+ * [x_lo, x_hi) as one instance and holds ghost copies of its neighbours'
+ * particles within a layer of width wcsph_slab_layer_width() beyond each
+ * face.  Per step, on every rank:
+ *   wcsph_sim_step(sim, 1);
+ *   wcsph_sim_slab_pack(...)   -> records [emigrants L, ghosts L, emigrants R, ghosts R]
+ *   (transport: send the L part left and the R part right, receive both)
+ *   wcsph_sim_slab_unpack(...) once per received part
+ *   dt = min over ranks of wcsph_sim_next_dt(); wcsph_sim_set_next_dt(dt)
+ * Records are WCSPH_SLAB_RECORD_BYTES each: float4 (x, y, z, rho),
+ * float4 (vx, vy, vz, 0), float4 (ax, ay, az, div v), int32 id,
+ * int32 type, 8 bytes padding.  The x axis must not be periodic. */
+#define WCSPH_SLAB_RECORD_BYTES 64
+typedef struct wcsph_slab {
+  float x_lo, x_hi;            /* owned range [x_lo, x_hi); a side without a neighbour extends to the grid */
+  float margin;                /* largest drift of a particle in one step that the ghost layer covers (> 0) */
+  int32_t has_left, has_right; /* a neighbouring slab exists on that side */
+} wcsph_slab;
+
+/* Ghost-layer width W = 2 (2h) (1 + 1e-4) + 2 margin, in FP32. */
+float wcsph_slab_layer_width(double h, float margin);
+/* Add a slab instance: desc describes the whole simulation (desc->n is the
+ * size of the id space, grid bounds are the whole domain's); the count
+ * particles given (ids[k] in [0, desc->n)) are the ones the slab owns.  No
+ * force pass runs: exchange a first ghost layer, then wcsph_sim_force_pass. */
+int wcsph_sim_add_slab(wcsph_sim* sim, const wcsph_instance_desc* desc, const wcsph_slab* slab, int32_t count,
+                       const int32_t* ids, const float* pos3, const float* vel3, const float* dens,
+                       const int32_t* type, int32_t* slot);
+/* Classify, pack into the device buffer send (capacity records) and retire
+ * the previous ghost layer.  counts[4] = emigrants left, ghosts left,
+ * emigrants right, ghosts right; the records are in that order.  Returns
+ * WCSPH_E_STATE when a particle drifted farther than the margin in a step and
+ * WCSPH_E_CAPACITY when the records do not fit (nothing changed then). */
+int wcsph_sim_slab_pack(wcsph_sim* sim, int32_t slot, void* send, int64_t capacity, int32_t counts[4]);
+/* Append n_owned + n_ghost records from the device buffer recv: the first
+ * n_owned become owned particles (a neighbour's emigrants), the rest ghosts. */
+int wcsph_sim_slab_unpack(wcsph_sim* sim, int32_t slot, const void* recv, int32_t n_owned, int32_t n_ghost);
 /* Remove an instance; its particles and cells are reclaimed at the next step. */
 int wcsph_sim_remove_instance(wcsph_sim* sim, int32_t slot);
 

@@ -56,6 +56,14 @@ class SimOptions(C.Structure):
                 ("autotune", C.c_int32), ("reserved_", C.c_int32)]
 
 
+class Slab(C.Structure):
+    _fields_ = [("x_lo", C.c_float), ("x_hi", C.c_float), ("margin", C.c_float),
+                ("has_left", C.c_int32), ("has_right", C.c_int32)]
+
+
+SLAB_RECORD_BYTES = 64
+
+
 class WcsphError(RuntimeError):
     def __init__(self, fn, code, msg):
         super().__init__(f"{fn} failed: {STATUS_NAMES.get(code, code)}: {msg}")
@@ -92,6 +100,13 @@ _SIGS = {
     "wcsph_sim_restore_instance": (C.c_int, [P, C.POINTER(InstanceDesc), F32P, F32P, F32P, I32P, F32P, F32P, I32P,
                                               I32P, C.c_double, C.c_int64, C.c_float, I32P]),
     "wcsph_sim_next_dt": (C.c_int, [P, C.c_int32, F32P]),
+    "wcsph_sim_set_next_dt": (C.c_int, [P, C.c_int32, C.c_float]),
+    "wcsph_sim_force_pass": (C.c_int, [P, C.c_int32]),
+    "wcsph_slab_layer_width": (C.c_float, [C.c_double, C.c_float]),
+    "wcsph_sim_add_slab": (C.c_int, [P, C.POINTER(InstanceDesc), C.POINTER(Slab), C.c_int32, I32P, F32P, F32P, F32P,
+                                      I32P, I32P]),
+    "wcsph_sim_slab_pack": (C.c_int, [P, C.c_int32, P, C.c_int64, I32P]),
+    "wcsph_sim_slab_unpack": (C.c_int, [P, C.c_int32, P, C.c_int32, C.c_int32]),
     "wcsph_sim_remove_instance": (C.c_int, [P, C.c_int32]),
     "wcsph_sim_step": (C.c_int, [P, C.c_int32]),
     "wcsph_sim_synchronize": (C.c_int, [P]),

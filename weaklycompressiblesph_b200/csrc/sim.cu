@@ -13,6 +13,7 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -20,11 +21,14 @@
 #include "sim_kernels.cuh"
 #include "sim_aux.cuh"
 #include "sim_tiled.cuh"
+#include "sim_slab.cuh"
 
 namespace wcsph {
 
 struct HostInst {
   bool used = false;     // slot holds an instance (active or draining)
+  bool slab = false;     // one slab of a decomposed simulation (wcsph_sim_add_slab)
+  SlabGeom geom{};
   bool active = false;   // stepping
   bool drained = false;  // removed, and a pass has been enqueued since (its particles are dead keys)
   wcsph_instance_desc desc{};
@@ -62,6 +66,7 @@ struct SimImpl {
   std::vector<InstParams> h_params;
   std::vector<int> h_phase;
   int n_host = 0;
+  bool appended = false;       // particles were appended after the last pass (its live count is stale)
   int key_bits = 1;
   long long total_cells = 0;
   bool any_density = false;
@@ -232,11 +237,13 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
   WCSPH_CUDA(cudaGetLastError());
   if (launches) *launches = L;
   mark_drained(S);
+  S.appended = false;
   return 0;
 }
 
 static int sync_compact(SimImpl& S) {
   WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  if (S.appended) return 0;  // no pass has counted the appended particles yet
   int n_alive = 0;
   WCSPH_CUDA(cudaMemcpy(&n_alive, S.d_n_alive, sizeof(int), cudaMemcpyDeviceToHost));
   if (n_alive != S.n_host) {
@@ -460,6 +467,7 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
   if (rc) return fail(WCSPH_E_NOMEM);
   if (cudaMemsetAsync(S.d_dyn, 0, (size_t)opt->max_instances * sizeof(InstDyn), S.s) != cudaSuccess ||
       cudaMemsetAsync(S.d_n_alive, 0, sizeof(int), S.s) != cudaSuccess ||
+      cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s) != cudaSuccess ||
       cudaEventCreate(&S.ev0) != cudaSuccess || cudaEventCreate(&S.ev1) != cudaSuccess)
     return fail(WCSPH_E_CUDA);
   *out = sim;
@@ -483,17 +491,49 @@ int wcsph_sim_destroy(wcsph_sim* sim) {
 }  // extern "C"
 
 namespace wcsph {
-// Append an instance's particles at [n_host, n_host + n) and register it.
-// With init_pass the initial force pass (main.cpp:69-78) runs for it alone;
-// otherwise acc3/div_v and *dyn are taken as saved state (restart).
-static int append_instance(SimImpl& S, const wcsph_instance_desc* desc, const float* pos3, const float* vel3,
-                           const float* dens, const int32_t* type, const float* acc3, const float* div_v,
-                           const int32_t* alive, const int32_t* order, const InstDyn* saved, bool init_pass,
-                           int32_t* slot) {
+
+// The initial force pass (main.cpp:69-78) of instance k alone.
+static int init_force_pass(SimImpl& S, int k) {
+  const wcsph_instance_desc& d = S.inst[k].desc;
+  for (size_t q = 0; q < S.inst.size(); ++q) S.h_phase[q] = PH_IDLE;
+  S.h_phase[k] = PH_INIT;
+  if (int rc = upload_tables(S)) return rc;
+  StepArgs a = make_args(S);
+  WCSPH_CUDA(cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s));  // last_pairs: this pass
+  if (int rc = enqueue_pass(S, a, d.density_mode == WCSPH_DENSITY_SUMMATION, d.density_mode == WCSPH_DENSITY_SHEPARD,
+                            nullptr))
+    return rc;
+  if (int rc = set_all_phases(S, PH_STEP)) return rc;
+  WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  S.graph_dirty = true;
+  return 0;
+}
+
+// What an appended instance brings.  Particle q of the storage sequence is
+// particle ids[q] with its data at index q (slab), or particle order[q] with
+// its data at index order[q] (restart), or particle q (default).
+struct AppendSpec {
+  const wcsph_instance_desc* desc = nullptr;
+  int count = 0;
+  const int32_t* ids = nullptr;
+  const int32_t* order = nullptr;
+  const float *pos3 = nullptr, *vel3 = nullptr, *dens = nullptr, *acc3 = nullptr, *div_v = nullptr;
+  const int32_t *type = nullptr, *alive = nullptr;
+  const InstDyn* saved = nullptr;  // restart state, else a fresh instance
+  enum After { INIT_PASS, BIN_PASS, NO_PASS } after = INIT_PASS;
+  const wcsph_slab* slab = nullptr;
+};
+
+// Append an instance's particles at [n_host, n_host + count) and register it,
+// then run its initial force pass, or one pass with every instance idle that
+// only bins (restart), or nothing (slab: the ghost layer comes first).
+static int append_instance(SimImpl& S, const AppendSpec& A, int32_t* slot) {
+  const wcsph_instance_desc* desc = A.desc;
+  const int n = A.count;
   if (int rc = sync_compact(S)) return rc;
   bool draining = false;
   for (auto& I : S.inst) draining |= I.used && !I.active;
-  if ((long long)S.n_host + desc->n > S.opt.max_particles && draining) {
+  if ((long long)S.n_host + n > S.opt.max_particles && draining) {
     // Removed instances still hold slots: run one pass with every instance
     // idle so their particles become dead keys, then compact.
     for (size_t q = 0; q < S.inst.size(); ++q) S.h_phase[q] = PH_IDLE;
@@ -502,8 +542,8 @@ static int append_instance(SimImpl& S, const wcsph_instance_desc* desc, const fl
     if (int rc = set_all_phases(S, PH_STEP)) return rc;
     if (int rc = sync_compact(S)) return rc;
   }
-  if ((long long)S.n_host + desc->n > S.opt.max_particles) {
-    set_error("adding an instance: %d + %d particles exceed capacity %lld", S.n_host, desc->n,
+  if ((long long)S.n_host + n > S.opt.max_particles) {
+    set_error("adding an instance: %d + %d particles exceed capacity %lld", S.n_host, n,
               (long long)S.opt.max_particles);
     return WCSPH_E_CAPACITY;
   }
@@ -525,7 +565,22 @@ static int append_instance(SimImpl& S, const wcsph_instance_desc* desc, const fl
   }
   HostInst I;
   InstParams P;
-  if (int rc = fill_params(*desc, I, P)) return rc;
+  wcsph_instance_desc d = *desc;
+  float W = 0.f;
+  if (A.slab) {
+    // The slab's grid covers its range and the ghost layers beyond its faces.
+    const wcsph_slab& sl = *A.slab;
+    W = wcsph_slab_layer_width(d.h, sl.margin);
+    if (sl.has_left) d.lo[0] = std::max(d.lo[0], sl.x_lo - W - sl.margin);
+    if (sl.has_right) d.hi[0] = std::min(d.hi[0], sl.x_hi + W + sl.margin);
+  }
+  if (int rc = fill_params(d, I, P)) return rc;
+  if (A.slab) {
+    const wcsph_slab& sl = *A.slab;
+    I.slab = true;
+    I.geom = SlabGeom{sl.x_lo, sl.x_hi, W, sl.has_left ? 1 : 0, sl.has_right ? 1 : 0};
+    P.slab_margin2 = sl.margin * sl.margin;
+  }
   I.used = I.active = true;
   HostInst prev = S.inst[k];
   InstParams prev_p = S.h_params[k];
@@ -537,30 +592,37 @@ static int append_instance(SimImpl& S, const wcsph_instance_desc* desc, const fl
     rebuild_tables(S);
     return rc;
   }
-  // Append the particles at [n_host, n_host + n).
-  const int n = desc->n, base = S.n_host;
+  const int base = S.n_host;
   std::vector<float4> pos(n), vel(n), acc(n, make_float4(0, 0, 0, 0));
   std::vector<int> pid(n);
   std::vector<uint32_t> flags(n);
   for (int q = 0; q < n; ++q) {
-    const int i = order ? order[q] : q;  // storage position q holds particle i
-    pos[q] = make_float4(pos3[3 * i], pos3[3 * i + 1], pos3[3 * i + 2], dens[i]);
-    vel[q] = make_float4(vel3[3 * i], vel3[3 * i + 1], vel3[3 * i + 2], 0.f);
-    if (acc3) acc[q] = make_float4(acc3[3 * i], acc3[3 * i + 1], acc3[3 * i + 2], div_v ? div_v[i] : 0.f);
-    pid[q] = i;
-    flags[q] = (uint32_t)k | (type[i] == WCSPH_FREEZE ? kFreezeBit : 0u) | (alive && !alive[i] ? kDeadBit : 0u);
+    const int id = A.ids ? A.ids[q] : (A.order ? A.order[q] : q);
+    const int i = A.ids ? q : id;  // index of the particle's data in the input arrays
+    pos[q] = make_float4(A.pos3[3 * i], A.pos3[3 * i + 1], A.pos3[3 * i + 2], A.dens[i]);
+    vel[q] = make_float4(A.vel3[3 * i], A.vel3[3 * i + 1], A.vel3[3 * i + 2], 0.f);
+    if (A.acc3)
+      acc[q] = make_float4(A.acc3[3 * i], A.acc3[3 * i + 1], A.acc3[3 * i + 2], A.div_v ? A.div_v[i] : 0.f);
+    pid[q] = id;
+    flags[q] = (uint32_t)k | (A.type[i] == WCSPH_FREEZE ? kFreezeBit : 0u) | (A.alive && !A.alive[i] ? kDeadBit : 0u);
   }
-  WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.pos + base, pos.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, S.s));
-  WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.vel + base, vel.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, S.s));
-  WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.acc + base, acc.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, S.s));
-  WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.pid + base, pid.data(), sizeof(int) * n, cudaMemcpyHostToDevice, S.s));
-  WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.flags + base, flags.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, S.s));
+  if (n > 0) {
+    WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.pos + base, pos.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, S.s));
+    WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.vel + base, vel.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, S.s));
+    WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.acc + base, acc.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, S.s));
+    WCSPH_CUDA(cudaMemcpyAsync(S.buf_main.pid + base, pid.data(), sizeof(int) * n, cudaMemcpyHostToDevice, S.s));
+    WCSPH_CUDA(
+        cudaMemcpyAsync(S.buf_main.flags + base, flags.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, S.s));
+  }
   InstDyn dyn{};
   dyn.dt_next_bits = 0x7f800000u;
-  if (saved) dyn = *saved;
+  if (A.saved) dyn = *A.saved;
   WCSPH_CUDA(cudaMemcpyAsync(S.d_dyn + k, &dyn, sizeof(InstDyn), cudaMemcpyHostToDevice, S.s));
   S.n_host = base + n;
-  if (!init_pass) {
+  S.appended = true;
+  if (slot) *slot = k;
+  if (A.after == AppendSpec::INIT_PASS) return init_force_pass(S, k);
+  if (A.after == AppendSpec::BIN_PASS) {
     // One pass with every instance idle bins the restored particles (their
     // keys come from the saved positions, so a saved sorted order stays as
     // it is) and sets the instance's range; no state changes.
@@ -568,22 +630,9 @@ static int append_instance(SimImpl& S, const wcsph_instance_desc* desc, const fl
     if (int rc = upload_tables(S)) return rc;
     if (int rc = enqueue_pass(S, make_args(S), false, false, nullptr)) return rc;
     if (int rc = set_all_phases(S, PH_STEP)) return rc;
-    WCSPH_CUDA(cudaStreamSynchronize(S.s));
-    S.graph_dirty = true;
-    if (slot) *slot = k;
-    return 0;
   }
-  // Initial force pass for this instance only (main.cpp:69-78).
-  for (size_t q = 0; q < S.inst.size(); ++q) S.h_phase[q] = PH_IDLE;
-  S.h_phase[k] = PH_INIT;
-  if (int rc = upload_tables(S)) return rc;
-  StepArgs a = make_args(S);
-  const bool dens_pass = desc->density_mode == WCSPH_DENSITY_SUMMATION;
-  if (int rc = enqueue_pass(S, a, dens_pass, desc->density_mode == WCSPH_DENSITY_SHEPARD, nullptr)) return rc;
-  if (int rc = set_all_phases(S, PH_STEP)) return rc;
   WCSPH_CUDA(cudaStreamSynchronize(S.s));
   S.graph_dirty = true;
-  if (slot) *slot = k;
   return 0;
 }
 
@@ -598,8 +647,11 @@ int wcsph_sim_add_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, cons
     return WCSPH_E_INVALID;
   }
   WCSPH_CUDA(cudaSetDevice(sim->impl.opt.device));
-  return append_instance(sim->impl, desc, pos3, vel3, dens, type, nullptr, nullptr, nullptr, nullptr, nullptr, true,
-                         slot);
+  AppendSpec A;
+  A.desc = desc;
+  A.count = desc->n;
+  A.pos3 = pos3, A.vel3 = vel3, A.dens = dens, A.type = type;
+  return append_instance(sim->impl, A, slot);
 }
 
 int wcsph_sim_restore_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, const float* pos3, const float* vel3,
@@ -628,7 +680,14 @@ int wcsph_sim_restore_instance(wcsph_sim* sim, const wcsph_instance_desc* desc, 
   memcpy(&dyn.dt_next_bits, &dt_next, sizeof(float));
   dyn.finished = (desc->t_end > 0.0 && time >= desc->t_end) ? 1 : 0;
   dyn.range_lo = 0x7fffffff;
-  return append_instance(sim->impl, desc, pos3, vel3, dens, type, acc3, div_v, alive, order, &dyn, false, slot);
+  AppendSpec A;
+  A.desc = desc;
+  A.count = desc->n;
+  A.order = order;
+  A.pos3 = pos3, A.vel3 = vel3, A.dens = dens, A.type = type, A.acc3 = acc3, A.div_v = div_v, A.alive = alive;
+  A.saved = &dyn;
+  A.after = AppendSpec::BIN_PASS;
+  return append_instance(sim->impl, A, slot);
 }
 
 int wcsph_sim_next_dt(wcsph_sim* sim, int32_t slot, float* dt_next) {
@@ -643,6 +702,153 @@ int wcsph_sim_next_dt(wcsph_sim* sim, int32_t slot, float* dt_next) {
   InstDyn d;
   WCSPH_CUDA(cudaMemcpy(&d, S.d_dyn + slot, sizeof(InstDyn), cudaMemcpyDeviceToHost));
   memcpy(dt_next, &d.dt_next_bits, sizeof(float));
+  return 0;
+}
+
+int wcsph_sim_set_next_dt(wcsph_sim* sim, int32_t slot, float dt_next) {
+  if (!sim || !(dt_next > 0.f)) {
+    set_error("wcsph_sim_set_next_dt: dt_next must be positive");
+    return WCSPH_E_INVALID;
+  }
+  SimImpl& S = sim->impl;
+  if (slot < 0 || slot >= (int)S.inst.size() || !S.inst[slot].active) {
+    set_error("wcsph_sim_set_next_dt: slot %d is not active", slot);
+    return WCSPH_E_INVALID;
+  }
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  unsigned bits;
+  memcpy(&bits, &dt_next, sizeof(bits));
+  static_assert(offsetof(InstDyn, dt_next_bits) % 4 == 0, "dt_next_bits alignment");
+  WCSPH_CUDA(cudaMemcpyAsync((char*)(S.d_dyn + slot) + offsetof(InstDyn, dt_next_bits), &bits, sizeof(bits),
+                             cudaMemcpyHostToDevice, S.s));
+  WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  return 0;
+}
+
+int wcsph_sim_force_pass(wcsph_sim* sim, int32_t slot) {
+  if (!sim) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  if (slot < 0 || slot >= (int)S.inst.size() || !S.inst[slot].active) {
+    set_error("wcsph_sim_force_pass: slot %d is not active", slot);
+    return WCSPH_E_INVALID;
+  }
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  return init_force_pass(S, slot);
+}
+
+float wcsph_slab_layer_width(double h, float margin) {
+  return (float)(2.0 * (2.0 * h) * 1.0001) + 2.0f * margin;
+}
+
+int wcsph_sim_add_slab(wcsph_sim* sim, const wcsph_instance_desc* desc, const wcsph_slab* slab, int32_t count,
+                       const int32_t* ids, const float* pos3, const float* vel3, const float* dens,
+                       const int32_t* type, int32_t* slot) {
+  if (!sim || !desc || !slab || count < 0 || (count > 0 && (!ids || !pos3 || !vel3 || !dens || !type))) {
+    set_error("wcsph_sim_add_slab: null argument or negative count");
+    return WCSPH_E_INVALID;
+  }
+  if (desc->periodic) {
+    set_error("wcsph_sim_add_slab: slabs along a periodic x axis are not supported");
+    return WCSPH_E_INVALID;
+  }
+  const float W = wcsph_slab_layer_width(desc->h, slab->margin);
+  const float lo = slab->has_left ? slab->x_lo : desc->lo[0], hi = slab->has_right ? slab->x_hi : desc->hi[0];
+  if (!(slab->margin > 0.f) || !(hi > lo) || ((slab->has_left || slab->has_right) && hi - lo < 2.0f * W)) {
+    set_error("wcsph_sim_add_slab: need margin > 0 and a slab at least twice the ghost layer (%g) wide", W);
+    return WCSPH_E_INVALID;
+  }
+  for (int q = 0; q < count; ++q)
+    if (ids[q] < 0 || ids[q] >= desc->n) {
+      set_error("wcsph_sim_add_slab: id %d at %d outside [0, %d)", ids[q], q, desc->n);
+      return WCSPH_E_INVALID;
+    }
+  WCSPH_CUDA(cudaSetDevice(sim->impl.opt.device));
+  AppendSpec A;
+  A.desc = desc;
+  A.count = count;
+  A.ids = ids;
+  A.pos3 = pos3, A.vel3 = vel3, A.dens = dens, A.type = type;
+  A.after = AppendSpec::NO_PASS;
+  A.slab = slab;
+  return append_instance(sim->impl, A, slot);
+}
+
+int wcsph_sim_slab_pack(wcsph_sim* sim, int32_t slot, void* send, int64_t capacity, int32_t counts[4]) {
+  if (!sim || !counts || capacity < 0 || (capacity > 0 && !send)) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  if (slot < 0 || slot >= (int)S.inst.size() || !S.inst[slot].active || !S.inst[slot].slab) {
+    set_error("wcsph_sim_slab_pack: slot %d is not an active slab", slot);
+    return WCSPH_E_INVALID;
+  }
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  if (int rc = sync_compact(S)) return rc;
+  InstDyn d;
+  WCSPH_CUDA(cudaMemcpy(&d, S.d_dyn + slot, sizeof(InstDyn), cudaMemcpyDeviceToHost));
+  if (d.errors & kErrDrift) {
+    set_error("wcsph_sim_slab_pack: a particle drifted farther than the slab margin (%g) in one step",
+              (double)std::sqrt(S.h_params[slot].slab_margin2));
+    return WCSPH_E_STATE;
+  }
+  const int n = S.n_host;
+  const SlabGeom G = S.inst[slot].geom;
+  int h_counts[4] = {0, 0, 0, 0};
+  if (n > 0) {
+    // class keys and indices in the step's sort buffers (free between passes)
+    WCSPH_CUDA(cudaMemsetAsync(S.d_counters, 0, 4 * sizeof(int), S.s));
+    k_slab_classify<<<nblk(n), kBlock, 0, S.s>>>(S.buf_main, n, slot, G, S.keys_in, S.vals_in, S.d_counters);
+    WCSPH_CUDA(cudaGetLastError());
+    size_t need = 0;
+    WCSPH_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, need, S.keys_in, S.keys_out, S.vals_in, S.vals_out, n, 0,
+                                               kSlabClassBits, S.s));
+    if (need > S.cub_bytes) {
+      set_error("wcsph_sim_slab_pack: sort scratch %zu B exceeds %zu B", need, S.cub_bytes);
+      return WCSPH_E_CAPACITY;
+    }
+    size_t bytes = S.cub_bytes;
+    WCSPH_CUDA(cub::DeviceRadixSort::SortPairs(S.cub_tmp, bytes, S.keys_in, S.keys_out, S.vals_in, S.vals_out, n, 0,
+                                               kSlabClassBits, S.s));
+    WCSPH_CUDA(cudaMemcpyAsync(h_counts, S.d_counters, sizeof(h_counts), cudaMemcpyDeviceToHost, S.s));
+    WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  }
+  const long long total = (long long)h_counts[0] + h_counts[1] + h_counts[2] + h_counts[3];
+  if (total > capacity) {
+    set_error("wcsph_sim_slab_pack: %lld records exceed the send buffer (%lld)", total, (long long)capacity);
+    return WCSPH_E_CAPACITY;
+  }
+  if (total > 0) {
+    k_slab_pack<<<nblk(total), kBlock, 0, S.s>>>(S.buf_main, S.vals_out, (int)total, (SlabRecord*)send);
+    WCSPH_CUDA(cudaGetLastError());
+  }
+  if (n > 0) {
+    k_slab_commit<<<nblk(n), kBlock, 0, S.s>>>(S.buf_main, n, slot, G);
+    WCSPH_CUDA(cudaGetLastError());
+  }
+  WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  for (int c = 0; c < 4; ++c) counts[c] = h_counts[c];
+  return 0;
+}
+
+int wcsph_sim_slab_unpack(wcsph_sim* sim, int32_t slot, const void* recv, int32_t n_owned, int32_t n_ghost) {
+  if (!sim || n_owned < 0 || n_ghost < 0 || (n_owned + n_ghost > 0 && !recv)) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  if (slot < 0 || slot >= (int)S.inst.size() || !S.inst[slot].active || !S.inst[slot].slab) {
+    set_error("wcsph_sim_slab_unpack: slot %d is not an active slab", slot);
+    return WCSPH_E_INVALID;
+  }
+  const long long m = (long long)n_owned + n_ghost;
+  if (S.n_host + m > S.opt.max_particles) {
+    set_error("wcsph_sim_slab_unpack: %d + %lld particles exceed capacity %lld", S.n_host, m,
+              (long long)S.opt.max_particles);
+    return WCSPH_E_CAPACITY;
+  }
+  if (m == 0) return 0;
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  k_slab_unpack<<<nblk(m), kBlock, 0, S.s>>>(S.buf_main, S.n_host, (int)m, n_owned, slot, (const SlabRecord*)recv);
+  WCSPH_CUDA(cudaGetLastError());
+  WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  S.n_host += (int)m;
+  S.appended = true;
+  S.graph_dirty = true;
   return 0;
 }
 
@@ -782,7 +988,7 @@ int wcsph_sim_read_instance(wcsph_sim* sim, int32_t slot, float* pos3, float* ve
   if (alive)
     for (int i = 0; i < n; ++i) alive[i] = 0;
   for (size_t q = 0; q < pid.size(); ++q) {
-    if ((int)(flags[q] & kInstMask) != slot) continue;
+    if ((int)(flags[q] & kInstMask) != slot || (flags[q] & kGhostBit)) continue;  // ghosts: their owner reports them
     const int i = pid[q];
     if (i < 0 || i >= n) continue;
     if (pos3) pos3[3 * i] = pos[q].x, pos3[3 * i + 1] = pos[q].y, pos3[3 * i + 2] = pos[q].z;

@@ -12,6 +12,7 @@ __global__ void k_conservation(SimArrays A, const InstDyn* dyn, const InstParams
   const double m = params[slot].mass, g = params[slot].g;
   double s[6] = {0, 0, 0, 0, 0, 0};
   for (int p = lo + blockIdx.x * blockDim.x + threadIdx.x; p < hi; p += gridDim.x * blockDim.x) {
+    if (A.flags[p] & kGhostBit) continue;  // a slab's ghost copies belong to their owner's sums
     const float4 v = A.vel[p];
     const float4 a = A.acc[p];
     s[0] += m;

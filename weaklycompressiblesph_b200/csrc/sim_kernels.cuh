@@ -102,6 +102,8 @@ __global__ void k_kick_bin(StepArgs a) {
         x.x += dt * vh.x;
         x.y += dt * vh.y;
         x.z += dt * vh.z;
+        if (P.slab_margin2 > 0.0f && dt * dt * (vh.x * vh.x + vh.y * vh.y + vh.z * vh.z) > P.slab_margin2)
+          atomicOr(&a.dyn[inst].errors, kErrDrift);  // the ghost layer no longer covers this drift
         v = make_float4(v.x + dt * acc.x, v.y + dt * acc.y, v.z + dt * acc.z, 0.f);
         if (P.periodic) {
           float* c = &x.x;
@@ -324,10 +326,12 @@ __device__ __forceinline__ void finish_hydro(const StepArgs& a, int p, const Ins
   } else {
     az -= P.g;
     if (!(f & kFreezeBit)) {
-      const float amag = sqrtf(ax * ax + ay * ay + az * az);
-      const float c = fminf(fminf(dt_i, 0.25f * sqrtf(h / amag)), P.dt_nu);
-      dt_cand = dt_valid ? fminf(dt_cand, c) : c;
-      dt_valid = true;
+      if (!(f & kGhostBit)) {  // ghosts: their owner folds their dt
+        const float amag = sqrtf(ax * ax + ay * ay + az * az);
+        const float c = fminf(fminf(dt_i, 0.25f * sqrtf(h / amag)), P.dt_nu);
+        dt_cand = dt_valid ? fminf(dt_cand, c) : c;
+        dt_valid = true;
+      }
       if (ph == PH_STEP) {
         const float hdt = 0.5f * a.dyn[inst].dt_cur;
         const float4 vh = a.alt.vh[p];
@@ -403,6 +407,7 @@ __global__ void __launch_bounds__(256) k_hydro_plain(StepArgs a) {
         dsum += g * drdv;
       });
       finish_hydro(a, p, P, inst, ph, f, ax, ay, az, dsum, vsig, cnt, dt_cand, dt_valid);
+      if (f & kGhostBit) cnt = 0;  // pairs are counted for owned particles only
     } else {
       copy_state(a, p);
     }

@@ -361,9 +361,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
       if (lane < nbat) {
         const int p = ib + lane;
         const float* r = res[lane];
-        pairs += (unsigned long long)r[5];
-        finish_hydro(a, p, P, inst, ph, a.alt.flags[p], r[0], r[1], r[2], r[3], r[4], (unsigned)r[5], dt_cand,
-                     dt_valid);
+        const uint32_t fp = a.alt.flags[p];
+        if (!(fp & kGhostBit)) pairs += (unsigned long long)r[5];  // owned particles only
+        finish_hydro(a, p, P, inst, ph, fp, r[0], r[1], r[2], r[3], r[4], (unsigned)r[5], dt_cand, dt_valid);
       }
     }
     dt_min(a.dyn, inst, dt_cand, dt_valid);

@@ -90,6 +90,7 @@ struct InstParams {
   float rho0, inv_rho0, B, gamma, cs2_coef /* B*gamma/rho0 */, rho_floor, g;
   float dt_nu;            // 0.125 h^2 / nu (or +inf)
   float kill_lo[3], kill_hi[3];
+  float slab_margin2;     // slab instances: squared largest drift a step may make (0: not a slab)
   double t_end;
 };
 
@@ -103,15 +104,21 @@ struct InstDyn {
   int phase;             // 0 idle, 1 step, 2 initial force pass, 3 probe
   int range_lo, range_hi;// [first, last+1) sorted slot of this instance after binning
   int n_alive;
-  int pad_;
+  unsigned errors;       // kErrDrift: a slab particle drifted past the ghost-layer margin
 };
+
+constexpr unsigned kErrDrift = 1u;
 
 enum Phase { PH_IDLE = 0, PH_STEP = 1, PH_INIT = 2, PH_PROBE = 3 };
 
-// Particle flags word: bits 0-15 instance slot, bit 16 FREEZE, bit 17 dead.
+// Particle flags word: bits 0-15 instance slot, bit 16 FREEZE, bit 17 dead,
+// bit 18 ghost (a copy of a particle another slab owns: a neighbour in the
+// pair sums, kicked and drifted like its owner's copy, never reported, never
+// in the dt minimum or the pair count).
 constexpr uint32_t kInstMask = 0xffffu;
 constexpr uint32_t kFreezeBit = 1u << 16;
 constexpr uint32_t kDeadBit = 1u << 17;
+constexpr uint32_t kGhostBit = 1u << 18;
 constexpr uint32_t kDeadKey = 0xffffffffu;
 
 // Neighbour cell q (may be out of range by one) on axis k: wrapped index and

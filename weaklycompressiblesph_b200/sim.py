@@ -105,6 +105,39 @@ class Solver:
         N.call("wcsph_sim_next_dt", self._h, slot, C.byref(v))
         return v.value
 
+    def set_next_dt(self, slot, dt):
+        N.call("wcsph_sim_set_next_dt", self._h, slot, float(dt))
+
+    def force_pass(self, slot):
+        N.call("wcsph_sim_force_pass", self._h, slot)
+
+    # -- slab decomposition (see slab.py) ------------------------------------
+    def add_slab(self, case: Case, slab: N.Slab, ids, density_mode=None, t_end=None) -> int:
+        """Add the particles `ids` of `case` as the slab `slab` of a decomposed
+        simulation; no force pass runs (see wcsph_sim_add_slab)."""
+        d = case.desc(density_mode=density_mode, t_end=t_end)
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        pos = _f32(case.pos[ids], (-1, 3))
+        vel = _f32(case.vel[ids], (-1, 3))
+        dens = _f32(case.dens[ids], (-1,))
+        typ = np.ascontiguousarray(case.type[ids], dtype=np.int32)
+        slot = C.c_int32()
+        N.call("wcsph_sim_add_slab", self._h, C.byref(d), C.byref(slab), len(ids), N.ptr(ids, C.c_int32),
+               N.ptr(pos, C.c_float), N.ptr(vel, C.c_float), N.ptr(dens, C.c_float), N.ptr(typ, C.c_int32),
+               C.byref(slot))
+        self.slots[slot.value] = case
+        return slot.value
+
+    def slab_pack(self, slot, send_ptr, capacity):
+        """Pack into the device buffer at send_ptr (capacity records); returns
+        [emigrants left, ghosts left, emigrants right, ghosts right]."""
+        counts = (C.c_int32 * 4)()
+        N.call("wcsph_sim_slab_pack", self._h, slot, C.c_void_p(send_ptr), int(capacity), counts)
+        return [int(c) for c in counts]
+
+    def slab_unpack(self, slot, recv_ptr, n_owned, n_ghost):
+        N.call("wcsph_sim_slab_unpack", self._h, slot, C.c_void_p(recv_ptr), int(n_owned), int(n_ghost))
+
     def remove(self, slot):
         N.call("wcsph_sim_remove_instance", self._h, slot)
         self.slots.pop(slot, None)
