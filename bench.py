@@ -13,7 +13,9 @@ in-support pairs (0 < r^2 < (2h)^2) per second over the timed steps.
 (wcsph_hydro_dispatch / wcsph_hydro_retrieve) from host walk records, copies
 included.  `--impl reference` times the reference's own CPU functor
 (STD::CalcHydroForce, built by oracle/) on the same walks, on all host cores.
-Multi-GPU: independent replicas (the dam break is not sharded), weak scaling.
+Multi-GPU: independent replicas by default (weak scaling); `--decomp slab`
+cuts the one dam break into x-slabs, one per rank, with ghost-layer and
+particle exchange over NCCL after every step (strong scaling).
 """
 from __future__ import annotations
 
@@ -45,6 +47,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dam1m", choices=["dam1m", "dam16k", "periodic8m"])
     ap.add_argument("--precision", default="best", choices=["best", "fp32", "tiled", "half2"])
+    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
+                    help="N>1: independent replicas (weak scaling) or one dam break cut into x-slabs (strong)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison run")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble and serving samples")
@@ -133,7 +137,10 @@ def dist_setup(args):
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        # host scalars (barrier, max over ranks) over gloo; the slab mode's
+        # exchange buffers (device memory) over NCCL
+        backend = "cpu:gloo,cuda:nccl" if getattr(args, "decomp", "replicas") == "slab" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         pg = dist
     return world, rank, local, pg
 
@@ -211,6 +218,40 @@ def run_device(case, prec_name, steps, warmup, device, clocks=False):
         res["phase_ms"] = (ph / prof_steps).tolist()
         res["status"] = s.status(k)
         res["tuning"] = s.tuning()
+    return res
+
+
+def run_slab(case, prec_name, steps, warmup, rank, world, device, pg, clocks=False):
+    """One dam break cut into `world` x-slabs, this rank's slab on its GPU;
+    every step is followed by the ghost-layer and particle exchange and the
+    dt minimum over the ranks.  Timed with CUDA events on the solver stream
+    (the exchange synchronises it, so the interval spans all of it)."""
+    from weaklycompressiblesph_b200 import slab
+    slabs = slab.plan(case, world)
+    dom = slab.SlabDomain(case, slabs, rank, precision=precision_code(prec_name), device=device)
+    try:
+        drv = slab.DistRank(dom, rank, world) if world > 1 else slab.LocalGroup([dom])
+        drv.start()
+        drv.step(warmup)
+        barrier(pg)
+        pairs = dom.last_pairs()
+        sampler = ClockSampler(device) if clocks else None
+        if sampler:
+            sampler.__enter__()
+        ms = cuda_events_ms(dom.solver.stream(), lambda: drv.step(steps))
+        if sampler:
+            sampler.__exit__()
+        res = {"ms_per_step": ms / steps, "pairs_per_step": 0.5 * (pairs + dom.last_pairs()),
+               "kernels_per_step": dom.solver.kernels_per_step() + 3,  # + classify, pack, commit (+ unpacks)
+               "status": dom.status(), "tuning": None, "owned": int(dom.read()["alive"].sum())}
+        if sampler:
+            res["clocks"] = sampler.summary()
+        barrier(pg)
+        # per-phase kernel times of the slab's own passes (after the timed region; no exchange)
+        prof_steps = max(3, min(20, steps // 5))
+        res["phase_ms"] = (dom.solver.profile_steps(prof_steps) / prof_steps).tolist()
+    finally:
+        dom.close()
     return res
 
 
@@ -356,7 +397,12 @@ def main():
     prec = args.precision if args.precision != "best" else best_precision()
     case = make_case(args.workload)
     barrier(pg)
-    dev = run_device(case, prec, args.steps, args.warmup, local, clocks=(rank == 0))
+    slab_mode = args.decomp == "slab"
+    if slab_mode:
+        args.no_plain = args.no_e2e = args.no_ensemble = True
+        dev = run_slab(case, prec, args.steps, args.warmup, rank, world, local, pg, clocks=(rank == 0))
+    else:
+        dev = run_device(case, prec, args.steps, args.warmup, local, clocks=(rank == 0))
     ms = max_over_ranks(pg, dev["ms_per_step"])
     pairs_all = sum_over_ranks(pg, dev["pairs_per_step"])
     value = pairs_all / (ms * 1e-3)
@@ -394,17 +440,20 @@ def main():
         srv = measure_serving(local)
     if rank != 0:
         barrier(pg)
+        finish(pg)
         return 0
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong" if slab_mode else "weak",
         "vs_baseline": None, "dtype": "f32" if prec != "half2" else "f16x2-pair/f32-accumulate",
         "data": "synthetic (seeded lattice IC, no dataset)",
         "config": {"workload": {"dam1m": "3-D dam break dx=0.005 (1,024,000 fluid + 571,308 wall particles)",
                                 "dam16k": "3-D dam break dx=0.02 (16,000 fluid + 38,508 wall particles)",
                                 "periodic8m": "periodic jittered lattice 200^3 dx=0.01"}[args.workload],
                    "n_particles": case.n, "precision": prec, "h_over_dx": case.phys.h_over_dx,
-                   "density_mode": case.phys.density_mode, "parallelism": f"replicas x{world}",
+                   "density_mode": case.phys.density_mode,
+                   "parallelism": f"slab x{world}" if slab_mode else f"replicas x{world}",
                    "l2": "working set > L2 (126 MB): particle state and records "
                          f"{case.n * 200 / 1e6:.0f} MB, no flush needed"},
         "steps_per_s": steps_per_s * 1.0,
@@ -424,10 +473,18 @@ def main():
         "clocks": dev.get("clocks"),
         "sim_time_s": dev["status"]["time"],
     }
+    if slab_mode:
+        line["e2e_note"] = "e2e, cpu_baseline, plain FP32, ensemble and serving are measured in the default mode"
     print(json.dumps(line))
     sys.stdout.flush()
     barrier(pg)
+    finish(pg)
     return 0
+
+
+def finish(pg):
+    if pg is not None:
+        pg.destroy_process_group()
 
 
 def main_reference(args):
