@@ -25,6 +25,7 @@
 #include <mutex>
 #include <vector>
 
+#include "f32x2.cuh"
 #include "wcsph_common.cuh"
 
 namespace wcsph {
@@ -68,77 +69,262 @@ __device__ __forceinline__ float grad_factor(float r, float h) {  // g(r,h) with
   return spline_F(r * iH) * K / r;
 }
 
+// Hydro pair sum over FDPS walks (force.h:38-57; GPU variant kernel.cu:241-280
+// when VSIG/GRAD select it).  A walk's j-list is a superset of every one of
+// its i's neighbours (a few per cent of the (i, j) combinations are in
+// support), so the pass is split in two, per pair of i-particles and
+// 1024-record tile of the j-list:
+//   scan  — the tile is staged as structure-of-arrays (padded to a multiple
+//           of 64 with far-away sentinels); each lane tests two adjacent
+//           candidates against both i with packed f32x2 arithmetic and a
+//           squared-radius bound that covers every pair of the tile (2 max h),
+//           and the in-bound candidates are ballot-compacted into one queue
+//           of tile indices per i.  The GPU variant's v_sig (max of -mu over
+//           the whole walk, kernel.cu:263) is taken here over every j with
+//           r^2 > 0, with the rounding of the pair terms;
+//   pairs — lanes take consecutive queue entries (dense, no predicate
+//           divergence) and evaluate the exact support test and pair terms.
+// Partial sums are combined per warp with a butterfly reduce-scatter and kept
+// per i in shared memory.  A block of kWQWarps warps shares the staged tile;
+// warp w always takes the same i-pairs, so every sum runs in a fixed order.
+constexpr int kWQWarps = 4;
+constexpr int kWQTile = 1024;   // j-records per staged tile (queue entries are 16-bit tile indices)
+constexpr int kWQBatch = 128;   // i-particles accumulated per pass over the j-list
+
+// Dynamic shared memory of a walk block: staged j as SoA (x, y, z, h and, for
+// the GPU-variant v_sig, vx, vy, vz, rho), per-i queues, per-i accumulators
+// (ax, ay, az, -sum m g dr.dv, v_sig), the tile's largest h.
+template <int VSIG>
+struct WalkQLayout {
+  static constexpr int nsoa = VSIG ? 8 : 4;
+  static constexpr size_t soa = 0;
+  static constexpr size_t q = soa + sizeof(float) * nsoa * kWQTile;
+  static constexpr size_t res = q + sizeof(uint16_t) * kWQWarps * 2 * kWQTile;
+  static constexpr size_t hmax = res + sizeof(float) * kWQBatch * 5;
+  static constexpr size_t bytes = hmax + 16;
+};
+
+__device__ __forceinline__ float wq_butterfly8(const float v[8], int lane) {
+  const unsigned full = 0xffffffffu;
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+  float w[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float send = b4 ? v[k] : v[k + 4];
+    const float keep = b4 ? v[k + 4] : v[k];
+    w[k] = keep + __shfl_xor_sync(full, send, 16);
+  }
+  float x[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const float send = b3 ? w[k] : w[k + 2];
+    const float keep = b3 ? w[k + 2] : w[k];
+    x[k] = keep + __shfl_xor_sync(full, send, 8);
+  }
+  const float send = b2 ? x[0] : x[1];
+  float y = (b2 ? x[1] : x[0]) + __shfl_xor_sync(full, send, 4);
+  y += __shfl_xor_sync(full, y, 2);
+  y += __shfl_xor_sync(full, y, 1);
+  return y;  // warp total of slot (lane >> 2) & 7
+}
+
+// Pair terms of i (records a, b, c) with j (A, B, C): adds to
+// acc = (ax, ay, az, -sum m g dr.dv) as force.h:42-54 / kernel.cu:251-273
+// evaluate them (FP32).
+template <int GRAD>
+__device__ __forceinline__ void walk_pair(const float4& a, const float4& b, const float4& c, const float4& A,
+                                          const float4& B, const float4& C, const WalkPair& pp, float acc[4]) {
+  const float dx = a.x - A.x, dy = a.y - A.y, dz = a.z - A.z;
+  const float r2 = dist2(dx, dy, dz);
+  const float hi = a.w, hj = A.w;
+  const float dvx = b.x - B.x, dvy = b.y - B.y, dvz = b.z - B.z;
+  const float drdv = __fmaf_rn(dz, dvz, __fmaf_rn(dy, dvy, __fmul_rn(dx, dvx)));
+  const float den = r2 + pp.eps * hi * hj;
+  const float mu = drdv < 0.0f ? 0.5f * (hi + hj) * drdv / den : 0.0f;
+  const float r = sqrtf(r2);
+  float g;
+  if (GRAD == WCSPH_GRAD_SYM) {
+    g = 0.0f;
+    if (r < 2.0f * hi) g += grad_factor(r, hi);
+    if (r < 2.0f * hj) g += grad_factor(r, hj);
+    g *= 0.5f;
+  } else {
+    const float hb = 0.5f * (hi + hj);
+    g = (r < 2.0f * hb) ? grad_factor(r, hb) : 0.0f;
+  }
+  if (g == 0.0f) return;  // outside the support every term is zero
+  const float rho_sum = b.w + B.w;
+  const float av = (-pp.alpha * 0.5f * (c.y + C.y) * mu + pp.beta * mu * mu) * 2.0f / rho_sum;
+  const float pterm = c.x + C.x + av;
+  const float visc = 2.0f * (c.z + C.z) * (g * r2) / rho_sum / den;
+  const float m = C.w;
+  acc[0] += m * (visc * dvx - pterm * g * dx);
+  acc[1] += m * (visc * dvy - pterm * g * dy);
+  acc[2] += m * (visc * dvz - pterm * g * dz);
+  acc[3] -= m * g * drdv;
+}
+
+// max(vs, -mu) over one more j (r2 > 0, drdv as walk_pair rounds it).  The
+// running maximum is screened with a fast approximate quotient (relative
+// error far below 1e-6); the exact quotient of walk_pair is taken only where
+// it can raise the maximum, so the result is the maximum of the exact values.
+__device__ __forceinline__ float walk_vsig(float vs, float hi, float hj, float r2, float drdv, float eps) {
+  if (!(drdv < 0.0f) || !(r2 > 0.0f)) return vs;
+  const float num = 0.5f * (hi + hj) * drdv;
+  const float den = r2 + eps * hi * hj;
+  if (__fdividef(-num, den) < vs * 0.999999f) return vs;
+  return fmaxf(vs, -(num / den));
+}
+
+__device__ __forceinline__ void wq_append2(uint16_t* q, int& n, bool he, bool ho, int u, unsigned lt) {
+  const unsigned me = __ballot_sync(0xffffffffu, he), mo = __ballot_sync(0xffffffffu, ho);
+  const int p = n + __popc(me & lt) + __popc(mo & lt);
+  if (he) q[p] = (uint16_t)u;
+  if (ho) q[p + (he ? 1 : 0)] = (uint16_t)(u + 1);
+  n += __popc(me) + __popc(mo);
+}
+
 template <int VSIG, int GRAD>
-__global__ void __launch_bounds__(kWalkThreads) k_walk_hydro(const float4* __restrict__ iA, const float4* __restrict__ iB,
-                                                            const float4* __restrict__ iC, const float4* __restrict__ jA,
-                                                            const float4* __restrict__ jB, const float4* __restrict__ jC,
-                                                            const int* __restrict__ ni_displ,
-                                                            const int* __restrict__ nj_displ, int walk0, WalkPair pp,
-                                                            float4* __restrict__ out4, float* __restrict__ out_dt) {
-  __shared__ float4 sA[kWalkTile], sB[kWalkTile], sC[kWalkTile];
+__global__ void __launch_bounds__(kWQWarps * 32) k_walk_hydro(const float4* __restrict__ iA, const float4* __restrict__ iB,
+                                                              const float4* __restrict__ iC, const float4* __restrict__ jA,
+                                                              const float4* __restrict__ jB, const float4* __restrict__ jC,
+                                                              const int* __restrict__ ni_displ,
+                                                              const int* __restrict__ nj_displ, int walk0, WalkPair pp,
+                                                              float4* __restrict__ out4, float* __restrict__ out_dt) {
+  using Lay = WalkQLayout<VSIG>;
+  extern __shared__ __align__(16) unsigned char wq_smem[];
+  float* tx = reinterpret_cast<float*>(wq_smem + Lay::soa);
+  float* ty = tx + kWQTile;
+  float* tz = ty + kWQTile;
+  float* th = tz + kWQTile;
+  float* tvx = th + kWQTile;  // VSIG only
+  float* tvy = tvx + kWQTile;
+  float* tvz = tvy + kWQTile;
+  float* trho = tvz + kWQTile;
+  uint16_t(*sq)[2][kWQTile] = reinterpret_cast<uint16_t(*)[2][kWQTile]>(wq_smem + Lay::q);
+  float(*res)[5] = reinterpret_cast<float(*)[5]>(wq_smem + Lay::res);
+  unsigned* s_hmax = reinterpret_cast<unsigned*>(wq_smem + Lay::hmax);
+  const unsigned full = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned lt;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
   const int w = walk0 + blockIdx.x;
   const int i0 = ni_displ[w], i1 = ni_displ[w + 1];
   const int j0 = nj_displ[w], j1 = nj_displ[w + 1];
-  for (int ib = i0; ib < i1; ib += kWalkThreads) {
-    const int i = ib + threadIdx.x;
-    const bool valid = i < i1;
-    float4 a = make_float4(0.f, 0.f, 0.f, 1.f), b = make_float4(0.f, 0.f, 0.f, 1.f), c = make_float4(0.f, 1.f, 0.f, 0.f);
-    if (valid) {
-      a = iA[i];
-      b = iB[i];
-      c = iC[i];
-    }
-    float ax = 0.f, ay = 0.f, az = 0.f, dv_acc = 0.f, vsig = 0.f;
-    for (int jb = j0; jb < j1; jb += kWalkTile) {
-      const int nt = min(kWalkTile, j1 - jb);
+  uint16_t* qa = sq[warp][0];
+  uint16_t* qb = sq[warp][1];
+  for (int ib = i0; ib < i1; ib += kWQBatch) {
+    const int nb = min(kWQBatch, i1 - ib);
+    for (int t = threadIdx.x; t < kWQBatch * 5; t += blockDim.x) (&res[0][0])[t] = 0.0f;
+    // largest h of the batch's i (h > 0: its bits order like the values)
+    float hm = 0.0f;
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) hm = fmaxf(hm, iA[ib + t].w);
+    for (int jb = j0; jb < j1; jb += kWQTile) {
+      const int nt = min(kWQTile, j1 - jb), nt64 = (nt + 63) & ~63;
+      __syncthreads();  // the previous tile's readers are done; res zeroed
+      if (threadIdx.x == 0) s_hmax[0] = 0u;
       __syncthreads();
-      for (int k = threadIdx.x; k < nt; k += kWalkThreads) {
-        sA[k] = jA[jb + k];
-        sB[k] = jB[jb + k];
-        sC[k] = jC[jb + k];
-      }
-      __syncthreads();
-      if (!valid) continue;
-      for (int k = 0; k < nt; ++k) {
-        const float4 A = sA[k];
-        const float dx = a.x - A.x, dy = a.y - A.y, dz = a.z - A.z;
-        const float r2 = dist2(dx, dy, dz);
-        if (!(r2 > 0.0f)) continue;  // force.h:42
-        const float4 B = sB[k];
-        const float hi = a.w, hj = A.w;
-        const float dvx = b.x - B.x, dvy = b.y - B.y, dvz = b.z - B.z;
-        const float drdv = dx * dvx + dy * dvy + dz * dvz;
-        const float den = r2 + pp.eps * hi * hj;
-        const float mu = drdv < 0.0f ? 0.5f * (hi + hj) * drdv / den : 0.0f;
-        vsig = VSIG ? fmaxf(vsig, -mu) : fmaxf(vsig, mu);
-        const float r = sqrtf(r2);
-        float g;
-        if (GRAD == WCSPH_GRAD_SYM) {
-          g = 0.0f;
-          if (r < 2.0f * hi) g += grad_factor(r, hi);
-          if (r < 2.0f * hj) g += grad_factor(r, hj);
-          g *= 0.5f;
-        } else {
-          const float hb = 0.5f * (hi + hj);
-          g = (r < 2.0f * hb) ? grad_factor(r, hb) : 0.0f;
+      float hj_max = hm;
+      for (int k = threadIdx.x; k < nt64; k += blockDim.x) {
+        if (k < nt) {
+          const float4 J = jA[jb + k];
+          tx[k] = J.x, ty[k] = J.y, tz[k] = J.z, th[k] = J.w;
+          hj_max = fmaxf(hj_max, J.w);
+          if (VSIG) {
+            const float4 V = jB[jb + k];
+            tvx[k] = V.x, tvy[k] = V.y, tvz[k] = V.z, trho[k] = V.w;
+          }
+        } else {  // padding: never within any bound, never approaching
+          tx[k] = 1.0e30f, ty[k] = 1.0e30f, tz[k] = 1.0e30f, th[k] = 0.0f;
+          if (VSIG) tvx[k] = tvy[k] = tvz[k] = trho[k] = 0.0f;
         }
-        if (g == 0.0f) continue;  // outside the support every term below is zero
-        const float4 C = sC[k];
-        const float rho_sum = b.w + B.w;
-        const float av = (-pp.alpha * 0.5f * (c.y + C.y) * mu + pp.beta * mu * mu) * 2.0f / rho_sum;
-        const float pterm = c.x + C.x + av;
-        const float visc = 2.0f * (c.z + C.z) * (g * r2) / rho_sum / den;
-        const float m = C.w;
-        ax += m * (visc * dvx - pterm * g * dx);
-        ay += m * (visc * dvy - pterm * g * dy);
-        az += m * (visc * dvz - pterm * g * dz);
-        dv_acc -= m * g * drdv;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) hj_max = fmaxf(hj_max, __shfl_xor_sync(full, hj_max, o));
+      if (lane == 0) atomicMax(s_hmax, __float_as_uint(hj_max));
+      __syncthreads();
+      // every pair of the tile lies within 2 max h (both variants), with margin
+      const float Rb = 2.0f * __uint_as_float(s_hmax[0]);
+      const float B2 = Rb * Rb * 1.0001f;
+      for (int ip = 2 * warp; ip < nb; ip += 2 * kWQWarps) {
+        const int ia = ib + ip;
+        const bool has_b = ip + 1 < nb;
+        const int ibb = has_b ? ia + 1 : ia;
+        const float4 Aa = iA[ia], Ab = iA[ibb];
+        const float4 Ba = iB[ia], Bb = iB[ibb];
+        const f2 XA = dup(Aa.x), YA = dup(Aa.y), ZA = dup(Aa.z);
+        const f2 XB = dup(Ab.x), YB = dup(Ab.y), ZB = dup(Ab.z);
+        int na = 0, nq = 0;
+        float vsa = 0.0f, vsb = 0.0f;
+        for (int tb = 2 * lane; tb < nt64; tb += 64) {
+          const f2 CX = *reinterpret_cast<const f2*>(&tx[tb]);
+          const f2 CY = *reinterpret_cast<const f2*>(&ty[tb]);
+          const f2 CZ = *reinterpret_cast<const f2*>(&tz[tb]);
+          const f2 DXA = sub2(XA, CX), DYA = sub2(YA, CY), DZA = sub2(ZA, CZ);
+          const f2 DXB = sub2(XB, CX), DYB = sub2(YB, CY), DZB = sub2(ZB, CZ);
+          const f2 RA = fma2(DZA, DZA, fma2(DYA, DYA, mul2(DXA, DXA)));  // == dist2 per half
+          const f2 RB = fma2(DZB, DZB, fma2(DYB, DYB, mul2(DXB, DXB)));
+          const float ra0 = lo(RA), ra1 = hi(RA), rb0 = lo(RB), rb1 = hi(RB);
+          wq_append2(qa, na, ra0 > 0.0f && ra0 < B2, ra1 > 0.0f && ra1 < B2, tb, lt);
+          wq_append2(qb, nq, has_b && rb0 > 0.0f && rb0 < B2, has_b && rb1 > 0.0f && rb1 < B2, tb, lt);
+          if (VSIG) {
+            const f2 CVX = *reinterpret_cast<const f2*>(&tvx[tb]);
+            const f2 CVY = *reinterpret_cast<const f2*>(&tvy[tb]);
+            const f2 CVZ = *reinterpret_cast<const f2*>(&tvz[tb]);
+            const f2 DA = fma2(DZA, sub2(dup(Ba.z), CVZ), fma2(DYA, sub2(dup(Ba.y), CVY), mul2(DXA, sub2(dup(Ba.x), CVX))));
+            const f2 DB = fma2(DZB, sub2(dup(Bb.z), CVZ), fma2(DYB, sub2(dup(Bb.y), CVY), mul2(DXB, sub2(dup(Bb.x), CVX))));
+            const float h0 = th[tb], h1 = th[tb + 1];
+            const bool real0 = tb < nt, real1 = tb + 1 < nt;
+            if (real0) vsa = walk_vsig(vsa, Aa.w, h0, ra0, lo(DA), pp.eps);
+            if (real1) vsa = walk_vsig(vsa, Aa.w, h1, ra1, hi(DA), pp.eps);
+            if (has_b && real0) vsb = walk_vsig(vsb, Ab.w, h0, rb0, lo(DB), pp.eps);
+            if (has_b && real1) vsb = walk_vsig(vsb, Ab.w, h1, rb1, hi(DB), pp.eps);
+          }
+        }
+        __syncwarp();
+        const float4 Ca = iC[ia], Cb = iC[ibb];
+        float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        const int n = max(na, nq);
+        for (int k = lane; k < n; k += 32) {
+          if (k < na) {
+            const int u = qa[k];
+            const float4 J = make_float4(tx[u], ty[u], tz[u], th[u]);
+            const float4 V = VSIG ? make_float4(tvx[u], tvy[u], tvz[u], trho[u]) : jB[jb + u];
+            walk_pair<GRAD>(Aa, Ba, Ca, J, V, jC[jb + u], pp, acc);
+          }
+          if (k < nq) {
+            const int u = qb[k];
+            const float4 J = make_float4(tx[u], ty[u], tz[u], th[u]);
+            const float4 V = VSIG ? make_float4(tvx[u], tvy[u], tvz[u], trho[u]) : jB[jb + u];
+            walk_pair<GRAD>(Ab, Bb, Cb, J, V, jC[jb + u], pp, acc + 4);
+          }
+        }
+        const float y = wq_butterfly8(acc, lane);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          vsa = fmaxf(vsa, __shfl_xor_sync(full, vsa, o));
+          vsb = fmaxf(vsb, __shfl_xor_sync(full, vsb, o));
+        }
+        if ((lane & 3) == 0) {
+          const int slot = lane >> 2;
+          if (slot < 4) res[ip][slot] += y;
+          else if (has_b) res[ip + 1][slot - 4] += y;
+        }
+        if (lane == 0) {
+          res[ip][4] = fmaxf(res[ip][4], vsa);
+          if (has_b) res[ip + 1][4] = fmaxf(res[ip + 1][4], vsb);
+        }
+        __syncwarp();
       }
     }
-    if (valid) {
-      out4[i] = make_float4(ax, ay, az, dv_acc / b.w);
-      out_dt[i] = pp.c_cfl * a.w / (c.y + vsig);  // force.h:56 / kernel.cu:279
+    __syncthreads();
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+      const int i = ib + t;
+      const float* r = res[t];
+      out4[i] = make_float4(r[0], r[1], r[2], r[3] / iB[i].w);
+      out_dt[i] = pp.c_cfl * iA[i].w / (iC[i].y + r[4]);  // force.h:56 / kernel.cu:279
     }
+    __syncthreads();
   }
 }
 
@@ -520,8 +706,10 @@ static int dispatch_common(int kind, int32_t tag, int32_t n_walk, const void* co
       float* out_dt = (float*)(out4 + NI);
       auto kern = pp.vsig_mode ? (pp.grad_mode ? k_walk_hydro<1, 1> : k_walk_hydro<1, 0>)
                                : (pp.grad_mode ? k_walk_hydro<0, 1> : k_walk_hydro<0, 0>);
-      kern<<<w1 - w0, kWalkThreads, 0, T.stream>>>(diA, diA + NI, diA + 2 * NI, djA, djA + NJ, djA + 2 * NJ, d_ni,
-                                                   d_nj, w0, pp, out4, out_dt);
+      const int smem = (int)(pp.vsig_mode ? WalkQLayout<1>::bytes : WalkQLayout<0>::bytes);
+      WCSPH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      kern<<<w1 - w0, kWQWarps * 32, smem, T.stream>>>(diA, diA + NI, diA + 2 * NI, djA, djA + NJ, djA + 2 * NJ, d_ni,
+                                                      d_nj, w0, pp, out4, out_dt);
       WCSPH_CUDA(cudaGetLastError());
       if (a1 > a0) {
         WCSPH_CUDA(cudaMemcpyAsync((float4*)T.h_out.p + a0, out4 + a0, sizeof(float4) * (a1 - a0),
