@@ -85,11 +85,15 @@ __device__ __forceinline__ float grad_factor(float r, float h) {  // g(r,h) with
 //   pairs — lanes take consecutive queue entries (dense, no predicate
 //           divergence) and evaluate the exact support test and pair terms.
 // Partial sums are combined per warp with a butterfly reduce-scatter and kept
-// per i in shared memory.  A block of kWQWarps warps shares the staged tile;
-// warp w always takes the same i-pairs, so every sum runs in a fixed order.
+// per i in shared memory.  A block of kWQWarps warps takes kWQChunk i of one
+// walk and shares the staged tile; warp w always takes the same i-pairs, so
+// every sum runs in a fixed order.  The blocks come from a host-built work
+// list of (walk, first i) ordered by decreasing n_i n_j: a tree walk can
+// collect j-lists tens of times the median (a group whose Morton run spans
+// distant regions), and those blocks start first instead of ending last.
 constexpr int kWQWarps = 4;
 constexpr int kWQTile = 1024;   // j-records per staged tile (queue entries are 16-bit tile indices)
-constexpr int kWQBatch = 128;   // i-particles accumulated per pass over the j-list
+constexpr int kWQChunk = 32;    // i-particles per block: a walk is split into blocks of this many i
 
 // Dynamic shared memory of a walk block: staged j as SoA (x, y, z, h and, for
 // the GPU-variant v_sig, vx, vy, vz, rho), per-i queues, per-i accumulators
@@ -100,7 +104,7 @@ struct WalkQLayout {
   static constexpr size_t soa = 0;
   static constexpr size_t q = soa + sizeof(float) * nsoa * kWQTile;
   static constexpr size_t res = q + sizeof(uint16_t) * kWQWarps * 2 * kWQTile;
-  static constexpr size_t hmax = res + sizeof(float) * kWQBatch * 5;
+  static constexpr size_t hmax = res + sizeof(float) * kWQChunk * 5;
   static constexpr size_t bytes = hmax + 16;
 };
 
@@ -189,7 +193,8 @@ __global__ void __launch_bounds__(kWQWarps * 32) k_walk_hydro(const float4* __re
                                                               const float4* __restrict__ iC, const float4* __restrict__ jA,
                                                               const float4* __restrict__ jB, const float4* __restrict__ jC,
                                                               const int* __restrict__ ni_displ,
-                                                              const int* __restrict__ nj_displ, int walk0, WalkPair pp,
+                                                              const int* __restrict__ nj_displ,
+                                                              const int2* __restrict__ items, WalkPair pp,
                                                               float4* __restrict__ out4, float* __restrict__ out_dt) {
   using Lay = WalkQLayout<VSIG>;
   extern __shared__ __align__(16) unsigned char wq_smem[];
@@ -208,14 +213,16 @@ __global__ void __launch_bounds__(kWQWarps * 32) k_walk_hydro(const float4* __re
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned lt;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
-  const int w = walk0 + blockIdx.x;
-  const int i0 = ni_displ[w], i1 = ni_displ[w + 1];
+  const int2 item = items[blockIdx.x];  // (walk, first i of this block)
+  const int w = item.x;
+  const int i1 = ni_displ[w + 1];
   const int j0 = nj_displ[w], j1 = nj_displ[w + 1];
   uint16_t* qa = sq[warp][0];
   uint16_t* qb = sq[warp][1];
-  for (int ib = i0; ib < i1; ib += kWQBatch) {
-    const int nb = min(kWQBatch, i1 - ib);
-    for (int t = threadIdx.x; t < kWQBatch * 5; t += blockDim.x) (&res[0][0])[t] = 0.0f;
+  {
+    const int ib = item.y;
+    const int nb = min(kWQChunk, i1 - ib);
+    for (int t = threadIdx.x; t < kWQChunk * 5; t += blockDim.x) (&res[0][0])[t] = 0.0f;
     // largest h of the batch's i (h > 0: its bits order like the values)
     float hm = 0.0f;
     for (int t = threadIdx.x; t < nb; t += blockDim.x) hm = fmaxf(hm, iA[ib + t].w);
@@ -595,11 +602,16 @@ static int dispatch_common(int kind, int32_t tag, int32_t n_walk, const void* co
   const size_t o_rec = kind == K_HYDRO ? sizeof(float4) + sizeof(float) : sizeof(float);
   if (int rc = ensure_pinned(T.h_i, i_rec * (NI + 1))) return rc;
   if (int rc = ensure_pinned(T.h_j, j_rec * (NJ + 1))) return rc;
-  if (int rc = ensure_pinned(T.h_off, sizeof(int) * 2 * (n_walk + 1))) return rc;
+  // Work list of the hydro kernel: (walk, first i) per block of kWQChunk i.
+  long long n_items = 0;
+  if (kind == K_HYDRO)
+    for (int w = 0; w < n_walk; ++w) n_items += (n_epi[w] + kWQChunk - 1) / kWQChunk;
+  const size_t off_bytes = sizeof(int) * 2 * (n_walk + 1) + sizeof(int2) * (size_t)n_items;
+  if (int rc = ensure_pinned(T.h_off, off_bytes)) return rc;
   if (int rc = ensure_pinned(T.h_out, o_rec * (NI + 1))) return rc;
   if (int rc = ensure_dev(T.d_i, i_rec * (NI + 1))) return rc;
   if (int rc = ensure_dev(T.d_j, j_rec * (NJ + 1))) return rc;
-  if (int rc = ensure_dev(T.d_off, sizeof(int) * 2 * (n_walk + 1))) return rc;
+  if (int rc = ensure_dev(T.d_off, off_bytes)) return rc;
   if (int rc = ensure_dev(T.d_out, o_rec * (NI + 1))) return rc;
 
   int* h_ni = (int*)T.h_off.p;
@@ -610,7 +622,31 @@ static int dispatch_common(int kind, int32_t tag, int32_t n_walk, const void* co
   }
   int* d_ni = (int*)T.d_off.p;
   int* d_nj = d_ni + (n_walk + 1);
-  WCSPH_CUDA(cudaMemcpyAsync(d_ni, h_ni, sizeof(int) * 2 * (n_walk + 1), cudaMemcpyHostToDevice, T.stream));
+  const int chunks = n_walk < kChunks * 64 ? 1 : kChunks;
+  // Per dispatch chunk, its blocks in decreasing order of work n_i n_j (ties
+  // by position, so the list is reproducible; the order never changes a result).
+  int2* h_items = reinterpret_cast<int2*>(h_nj + (n_walk + 1));
+  std::vector<long long> item_off(chunks + 1, 0);
+  if (kind == K_HYDRO) {
+    std::vector<std::pair<long long, long long>> key;  // (-work, position)
+    long long pos = 0;
+    for (int ch = 0; ch < chunks; ++ch) {
+      const int w0 = (int)((long long)n_walk * ch / chunks), w1 = (int)((long long)n_walk * (ch + 1) / chunks);
+      key.clear();
+      std::vector<int2> its;
+      for (int w = w0; w < w1; ++w)
+        for (int i = 0; i < n_epi[w]; i += kWQChunk) {
+          const long long work = (long long)std::min(kWQChunk, n_epi[w] - i) * std::max(1, n_epj[w]);
+          key.emplace_back(-work, (long long)its.size());
+          its.push_back(make_int2(w, (int)(ni_d[w] + i)));
+        }
+      std::sort(key.begin(), key.end());
+      for (const auto& k : key) h_items[pos++] = its[k.second];
+      item_off[ch + 1] = pos;
+    }
+  }
+  WCSPH_CUDA(cudaMemcpyAsync(d_ni, h_ni, off_bytes, cudaMemcpyHostToDevice, T.stream));
+  const int2* d_items = reinterpret_cast<const int2*>(d_nj + (n_walk + 1));
 
   // SoA sub-arrays inside the staging buffers.
   float4* hiA = (float4*)T.h_i.p;
@@ -623,7 +659,6 @@ static int dispatch_common(int kind, int32_t tag, int32_t n_walk, const void* co
   float4* diA = (float4*)T.d_i.p;
   float4* djA = (float4*)T.d_j.p;
 
-  const int chunks = n_walk < kChunks * 64 ? 1 : kChunks;
   for (int ch = 0; ch < chunks; ++ch) {
     const int w0 = (int)((long long)n_walk * ch / chunks), w1 = (int)((long long)n_walk * (ch + 1) / chunks);
     if (w0 == w1) continue;
@@ -708,9 +743,13 @@ static int dispatch_common(int kind, int32_t tag, int32_t n_walk, const void* co
                                : (pp.grad_mode ? k_walk_hydro<0, 1> : k_walk_hydro<0, 0>);
       const int smem = (int)(pp.vsig_mode ? WalkQLayout<1>::bytes : WalkQLayout<0>::bytes);
       WCSPH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-      kern<<<w1 - w0, kWQWarps * 32, smem, T.stream>>>(diA, diA + NI, diA + 2 * NI, djA, djA + NJ, djA + 2 * NJ, d_ni,
-                                                      d_nj, w0, pp, out4, out_dt);
-      WCSPH_CUDA(cudaGetLastError());
+      const long long nblk = item_off[ch + 1] - item_off[ch];
+      if (nblk > 0) {
+        kern<<<(unsigned)nblk, kWQWarps * 32, smem, T.stream>>>(diA, diA + NI, diA + 2 * NI, djA, djA + NJ,
+                                                                djA + 2 * NJ, d_ni, d_nj, d_items + item_off[ch], pp,
+                                                                out4, out_dt);
+        WCSPH_CUDA(cudaGetLastError());
+      }
       if (a1 > a0) {
         WCSPH_CUDA(cudaMemcpyAsync((float4*)T.h_out.p + a0, out4 + a0, sizeof(float4) * (a1 - a0),
                                    cudaMemcpyDeviceToHost, T.stream));
