@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
                     help="N>1: independent replicas (weak scaling) or one dam break cut into x-slabs (strong)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-only", action="store_true",
+                    help="time only the FDPS drop-in pass (dispatch + retrieve from host records), --steps passes")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison run")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble and serving samples")
     ap.add_argument("--ensemble-steps", type=int, default=60)
@@ -287,14 +289,25 @@ def run_e2e(case, steps, warmup, device):
 
     for _ in range(warmup):
         one_pass()
+    split = [0.0, 0.0]  # dispatch (pack + enqueue), retrieve (wait + unpack)
+
+    def timed_pass():
+        for pi, pj, po, ni, nj, nw in batches:
+            t0 = time.perf_counter()
+            N.check("dispatch", L.wcsph_hydro_dispatch(0, nw, pi, N.ptr(ni, C.c_int32), pj, N.ptr(nj, C.c_int32)))
+            t1 = time.perf_counter()
+            N.check("retrieve", L.wcsph_hydro_retrieve(0, nw, N.ptr(ni, C.c_int32), po))
+            split[0] += t1 - t0
+            split[1] += time.perf_counter() - t1
+
     t0 = time.perf_counter()
     for _ in range(steps):
-        one_pass()
+        timed_pass()
     dt = (time.perf_counter() - t0) / steps
     h2d = len(epi) * 48 + len(epj) * 48 + 8 * (w.n_walk + len(batches))
     d2h = len(epi) * 20
     return dict(s_per_pass=dt, h2d=h2d, d2h=d2h, n_walk=w.n_walk, evaluated=w.n_evaluated, walks=w, epi=epi,
-                epj=epj)
+                epj=epj, dispatch_ms=1e3 * split[0] / steps, retrieve_ms=1e3 * split[1] / steps)
 
 
 def cpu_reference(case, walks, epi, epj, seconds, pairs_total):
@@ -396,6 +409,17 @@ def main():
     B.build()
     prec = args.precision if args.precision != "best" else best_precision()
     case = make_case(args.workload)
+    if args.e2e_only:
+        if rank == 0:
+            e = run_e2e(case, args.steps, args.warmup, local)
+            print(json.dumps({"e2e_only": True, "workload": args.workload, "passes": args.steps,
+                              "warmup": args.warmup, "ms_per_pass": 1e3 * e["s_per_pass"],
+                              "dispatch_ms": e["dispatch_ms"], "retrieve_ms": e["retrieve_ms"],
+                              "walks": e["n_walk"], "pair_evaluations_per_pass": e["evaluated"],
+                              "h2d_bytes_per_pass": e["h2d"], "d2h_bytes_per_pass": e["d2h"]}))
+        barrier(pg)
+        finish(pg)
+        return 0
     barrier(pg)
     slab_mode = args.decomp == "slab"
     if slab_mode:
