@@ -199,6 +199,15 @@ typedef struct wcsph_sim_options {
   int32_t autotune;            /* 1: time the kernel variants on the live instance set (probe
                                   passes, state untouched) and keep the fastest, re-tuned when the
                                   particle count crosses a power of two; 0: fixed defaults */
+  int32_t list_interval;       /* 0: search neighbours every step (exact order of the reference
+                                  loop).  K > 0 (tiled and half2 precisions): neighbour lists of
+                                  radius 2h + list_skin h, rebuilt at least every K steps and
+                                  whenever a density pass is due, the instance set changes, or
+                                  the measured drift nears half the skin; the steps between
+                                  read the lists and test 0 < r^2 < (2h)^2 on current positions,
+                                  so the pairs summed are the same as with a fresh search (the
+                                  summation order differs) */
+  float list_skin;             /* skin in units of h (0: 0.2) */
   int32_t reserved_;
 } wcsph_sim_options;
 
@@ -318,6 +327,11 @@ int32_t wcsph_sim_kernels_per_step(wcsph_sim* sim);
  * out[1] density kernel (always 0: per-thread), out[2] log2 particle bucket it
  * was tuned for (-1: defaults, not tuned). */
 int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out3);
+/* Neighbour-list counters (list_interval > 0): out[0] list builds, out[1]
+ * steps that read the lists, out[2] builds whose lists overflowed (the next
+ * step builds again), out[3] largest list built so far, out[4] kernel
+ * launches of a build step, out[5] kernel launches of a list step. */
+int wcsph_sim_list_stats(wcsph_sim* sim, int64_t* out6);
 /* The solver's CUDA stream (a cudaStream_t), so callers can record events on it. */
 void* wcsph_sim_stream(wcsph_sim* sim);
 /* Run nsteps steps launched one by one (no graph) with CUDA events around each

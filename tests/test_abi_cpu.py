@@ -52,7 +52,7 @@ def test_configure_rejects_bad_params(native):
 
 def test_struct_sizes_match_header(native):
     assert C.sizeof(N.InstanceDesc) == 176
-    assert C.sizeof(N.SimOptions) == 40
+    assert C.sizeof(N.SimOptions) == 48
     assert C.sizeof(N.PairParams) == 40
     assert C.sizeof(N.FdpsLayout) == 30 * 4
 

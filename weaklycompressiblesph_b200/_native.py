@@ -53,7 +53,8 @@ class InstanceDesc(C.Structure):
 class SimOptions(C.Structure):
     _fields_ = [("device", C.c_int32), ("precision", C.c_int32), ("max_particles", C.c_int64),
                 ("max_cells", C.c_int64), ("max_instances", C.c_int32), ("use_graph", C.c_int32),
-                ("autotune", C.c_int32), ("reserved_", C.c_int32)]
+                ("autotune", C.c_int32), ("list_interval", C.c_int32), ("list_skin", C.c_float),
+                ("reserved_", C.c_int32)]
 
 
 class Slab(C.Structure):
@@ -118,6 +119,7 @@ _SIGS = {
     "wcsph_sim_last_pairs": (C.c_int64, [P]),
     "wcsph_sim_kernels_per_step": (C.c_int32, [P]),
     "wcsph_sim_stream": (C.c_void_p, [P]),
+    "wcsph_sim_list_stats": (C.c_int, [P, C.POINTER(C.c_int64)]),
     "wcsph_sim_tuning": (C.c_int, [P, I32P]),
     "wcsph_sim_profile_steps": (C.c_int, [P, C.c_int32, F64P]),
 }

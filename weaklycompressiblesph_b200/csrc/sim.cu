@@ -22,6 +22,7 @@
 #include "sim_aux.cuh"
 #include "sim_tiled.cuh"
 #include "sim_slab.cuh"
+#include "sim_list.cuh"
 
 namespace wcsph {
 
@@ -29,6 +30,7 @@ struct HostInst {
   bool used = false;     // slot holds an instance (active or draining)
   bool slab = false;     // one slab of a decomposed simulation (wcsph_sim_add_slab)
   SlabGeom geom{};
+  long long host_steps = 0;  // steps launched since the instance's step count was known (list schedule)
   bool active = false;   // stepping
   bool drained = false;  // removed, and a pass has been enqueued since (its particles are dead keys)
   wcsph_instance_desc desc{};
@@ -76,7 +78,24 @@ struct SimImpl {
   bool graph_dirty = true;
   int kernels_per_step = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // neighbour lists (opt.list_interval > 0)
+  uint32_t* list = nullptr;
+  int* list_cnt = nullptr;
+  float4* x0 = nullptr;
+  unsigned* d_lflags = nullptr;       // see StepArgs::list_flags
+  unsigned* h_lflags = nullptr;       // pinned copy, written at the end of every list-mode step
+  cudaGraphExec_t gexec_reuse = nullptr;
+  cudaEvent_t step_ev[2] = {nullptr, nullptr};
+  bool lists_valid = false;
+  int since_build = 0;
+  int kernels_reuse = 0;
+  long long steps_launched = 0, last_build = -1;
+  long long n_builds = 0, n_reuse = 0, n_overflow = 0;
+  float last_disp = 0.f, last_drift = 0.f;  // from the latest completed step, in units of the skin
 };
+
+constexpr int kListMax = 256;  // entries per particle list (2h + skin holds ~80-140 at h = 1.3 dx)
+static float list_skin(const wcsph_sim_options& o) { return o.list_skin > 0.f ? o.list_skin : 0.2f; }
 
 static int alloc(SimImpl& S, void** p, size_t bytes) {
   WCSPH_CUDA(cudaMalloc(p, bytes ? bytes : 16));
@@ -100,7 +119,8 @@ static size_t per_particle_bytes() {
 }
 
 static int64_t device_bytes(const wcsph_sim_options& o) {
-  return (int64_t)per_particle_bytes() * o.max_particles + 2 * sizeof(int) * o.max_cells +
+  const int64_t list_bytes = o.list_interval > 0 ? (int64_t)(kListMax * 4 + 4 + 16) * o.max_particles : 0;
+  return (int64_t)per_particle_bytes() * o.max_particles + list_bytes + 2 * sizeof(int) * o.max_cells +
          (sizeof(InstParams) + sizeof(InstDyn) + sizeof(int)) * (int64_t)o.max_instances + (int64_t)cub_sort_bytes(o.max_particles) +
          (1 << 20);
 }
@@ -173,6 +193,12 @@ static StepArgs make_args(SimImpl& S) {
   a.diag_dt = S.diag_dt;
   a.diag_nbr = S.diag_nbr;
   a.diag_rho = S.diag_rho;
+  if (S.opt.list_interval > 0) {
+    a.list = S.list;
+    a.list_cnt = S.list_cnt;
+    a.list_max = kListMax;
+    a.list_flags = S.d_lflags;
+  }
   return a;
 }
 
@@ -188,9 +214,11 @@ static inline int nblk(long long n) { return (int)std::max<long long>(1, (n + kB
 // Enqueue one pass of the pipeline.  init_filter adds the initial Shepard
 // filter after the hydro pass (main.cpp:75).  Returns the kernel-launch count.
 static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, int* launches,
-                        cudaEvent_t* ev = nullptr) {
+                        cudaEvent_t* ev = nullptr, bool build_lists = false) {
   int L = 0;
   const int n = S.n_host;
+  if (build_lists) a.x0 = S.x0;
+  else S.lists_valid = false;  // any other pass re-sorts or changes what the lists refer to
   if (ev) WCSPH_CUDA(cudaEventRecord(ev[0], S.s));
   k_step_begin<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
   ++L;
@@ -218,9 +246,13 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
     if (S.opt.precision == WCSPH_PREC_FP32) {
       k_hydro_plain<true><<<nblk(n), kBlock, 0, S.s>>>(a);
     } else if (S.opt.precision == WCSPH_PREC_TILED) {
-      if (int rc = launch_hydro_tiled<false>(a, n, S.s, S.tile_shape)) return rc;
+      if (int rc = build_lists ? launch_hydro_tiled<false, true>(a, n, S.s, S.tile_shape)
+                               : launch_hydro_tiled<false>(a, n, S.s, S.tile_shape))
+        return rc;
     } else {
-      if (int rc = launch_hydro_tiled<true>(a, n, S.s, S.tile_shape)) return rc;
+      if (int rc = build_lists ? launch_hydro_tiled<true, true>(a, n, S.s, S.tile_shape)
+                               : launch_hydro_tiled<true>(a, n, S.s, S.tile_shape))
+        return rc;
     }
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[3], S.s));
@@ -238,6 +270,35 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
   if (launches) *launches = L;
   mark_drained(S);
   S.appended = false;
+  return 0;
+}
+
+// A step that reads the neighbour lists (sim_list.cuh): no sort, no scan.
+static int enqueue_reuse(SimImpl& S, StepArgs a, int* launches, cudaEvent_t* ev = nullptr) {
+  const int n = S.n_host;
+  a.list_reuse = 1;
+  a.x0 = S.x0;  // read by k_refresh (the displacement since the build)
+  if (ev) WCSPH_CUDA(cudaEventRecord(ev[0], S.s));
+  k_step_begin<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
+  int L = 1;
+  if (n > 0) {
+    k_kick_bin<<<nblk(n), kBlock, 0, S.s>>>(a);
+    k_refresh<<<nblk(n), kBlock, 0, S.s>>>(a);
+    L += 2;
+    if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));
+    if (ev) WCSPH_CUDA(cudaEventRecord(ev[2], S.s));
+    if (S.opt.precision == WCSPH_PREC_HALF2) {
+      if (int rc = launch_hydro_list<true>(a, n, S.s)) return rc;
+    } else {
+      if (int rc = launch_hydro_list<false>(a, n, S.s)) return rc;
+    }
+    ++L;
+    if (ev) WCSPH_CUDA(cudaEventRecord(ev[3], S.s));
+    k_copy_dead<<<nblk(n), kBlock, 0, S.s>>>(a);
+    ++L;
+  }
+  WCSPH_CUDA(cudaGetLastError());
+  if (launches) *launches = L;
   return 0;
 }
 
@@ -394,6 +455,125 @@ static int fill_params(const wcsph_instance_desc& d, HostInst& I, InstParams& P)
   return 0;
 }
 
+// ------------------------------------------------------- neighbour lists
+// Density passes read the cell tables, so a step with one due is a build step.
+// The host keeps each instance's step count (finished instances over-count,
+// which can only add builds).
+static bool density_due(const SimImpl& S) {
+  for (const auto& I : S.inst) {
+    if (!I.active) continue;
+    if (I.desc.density_mode == WCSPH_DENSITY_SUMMATION) return true;
+    if (I.desc.density_mode == WCSPH_DENSITY_SHEPARD && I.desc.shepard_interval > 0 &&
+        I.host_steps % I.desc.shepard_interval == 0)
+      return true;
+  }
+  return false;
+}
+
+// Flags of the latest completed step.  Sticky errors are handled after
+// draining the stream, so that they are seen and cleared exactly once.
+static int read_list_flags(SimImpl& S) {
+  volatile unsigned* h = S.h_lflags;
+  if (h[2]) {
+    WCSPH_CUDA(cudaStreamSynchronize(S.s));
+    const unsigned e = h[2];
+    h[2] = 0u;
+    WCSPH_CUDA(cudaMemsetAsync(S.d_lflags + 2, 0, sizeof(unsigned), S.s));
+    WCSPH_CUDA(cudaStreamSynchronize(S.s));
+    S.lists_valid = false;
+    if (e & 2u) ++S.n_overflow;
+    if (e & 1u) {
+      set_error("wcsph_sim_step: a particle moved more than half the neighbour-list skin between list builds; "
+                "the step's pair sums may be incomplete (raise list_skin or lower list_interval)");
+      return WCSPH_E_STATE;
+    }
+  }
+  const unsigned u0 = h[0], u1 = h[1];
+  memcpy(&S.last_disp, &u0, sizeof(float));
+  memcpy(&S.last_drift, &u1, sizeof(float));
+  return 0;
+}
+
+// One step in list mode.  Build when the lists are stale, K steps old, a
+// density pass is due, or the displacement since the build plus 2.5 steps of
+// the latest drift would pass half the skin (the decision sees the step
+// before the one in flight).  At most two steps are in flight; a build is
+// waited for, since its lists may have overflowed.
+static int list_step(SimImpl& S, bool graph, cudaEvent_t* ev) {
+  const bool build = !S.lists_valid || S.since_build >= S.opt.list_interval || density_due(S) ||
+                     S.last_disp + 2.5f * S.last_drift > 0.5f;
+  if (graph) {
+    WCSPH_CUDA(cudaGraphLaunch(build ? S.gexec : S.gexec_reuse, S.s));
+  } else {
+    StepArgs a = make_args(S);
+    WCSPH_CUDA(cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s));
+    WCSPH_CUDA(cudaMemsetAsync(S.d_lflags, 0, 2 * sizeof(unsigned), S.s));
+    const int rc = build ? enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step, ev, true)
+                         : enqueue_reuse(S, a, &S.kernels_reuse, ev);
+    if (rc) return rc;
+    WCSPH_CUDA(cudaMemcpyAsync(S.h_lflags, S.d_lflags, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, S.s));
+  }
+  if (build) {
+    S.lists_valid = true;
+    S.since_build = 1;
+    S.last_disp = 0.f;
+    ++S.n_builds;
+  } else {
+    ++S.since_build;
+    ++S.n_reuse;
+  }
+  for (auto& I : S.inst)
+    if (I.active) ++I.host_steps;
+  const int par = (int)(S.steps_launched & 1);
+  WCSPH_CUDA(cudaEventRecord(S.step_ev[par], S.s));
+  ++S.steps_launched;
+  if (build) {
+    WCSPH_CUDA(cudaEventSynchronize(S.step_ev[par]));
+    return read_list_flags(S);
+  }
+  if (S.steps_launched >= 2) {
+    WCSPH_CUDA(cudaEventSynchronize(S.step_ev[par ^ 1]));
+    return read_list_flags(S);
+  }
+  return 0;
+}
+
+// Capture the build-step and list-step graphs.
+static int capture_list_graphs(SimImpl& S) {
+  StepArgs a = make_args(S);
+  for (int kind = 0; kind < 2; ++kind) {
+    cudaGraphExec_t& X = kind == 0 ? S.gexec : S.gexec_reuse;
+    if (X) {
+      cudaGraphExecDestroy(X);
+      X = nullptr;
+    }
+    cudaGraph_t g;
+    WCSPH_CUDA(cudaStreamBeginCapture(S.s, cudaStreamCaptureModeThreadLocal));
+    int rc = 0;
+    if (cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s) != cudaSuccess ||
+        cudaMemsetAsync(S.d_lflags, 0, 2 * sizeof(unsigned), S.s) != cudaSuccess)
+      rc = WCSPH_E_CUDA;
+    if (!rc)
+      rc = kind == 0 ? enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step, nullptr, true)
+                     : enqueue_reuse(S, a, &S.kernels_reuse);
+    if (!rc && cudaMemcpyAsync(S.h_lflags, S.d_lflags, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, S.s) !=
+                   cudaSuccess)
+      rc = WCSPH_E_CUDA;
+    cudaError_t e = cudaStreamEndCapture(S.s, &g);
+    if (rc) {
+      if (e == cudaSuccess) cudaGraphDestroy(g);
+      set_error("capturing the neighbour-list step graphs failed");
+      return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    e = cudaGraphInstantiate(&X, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+  }
+  S.graph_dirty = false;
+  return 0;
+}
+
 }  // namespace wcsph
 
 using namespace wcsph;
@@ -409,8 +589,12 @@ int64_t wcsph_sim_device_bytes(const wcsph_sim_options* opt) { return opt ? devi
 int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
   if (!opt || !out || opt->max_particles <= 0 || opt->max_particles > INT32_MAX - 1 || opt->max_cells <= 0 ||
       opt->max_cells > INT32_MAX || opt->max_instances <= 0 || opt->max_instances > (int)kInstMask ||
-      opt->precision < 0 || opt->precision > 2) {
+      opt->precision < 0 || opt->precision > 2 || opt->list_interval < 0 || !(opt->list_skin >= 0.f)) {
     set_error("wcsph_sim_create: invalid options");
+    return WCSPH_E_INVALID;
+  }
+  if (opt->list_interval > 0 && opt->precision == WCSPH_PREC_FP32) {
+    set_error("wcsph_sim_create: neighbour lists need the tiled or half2 precision");
     return WCSPH_E_INVALID;
   }
   int ndev = 0;
@@ -464,12 +648,29 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
   rc |= alloc(S, (void**)&S.d_cons, 8 * sizeof(double));
   S.cub_bytes = cub_sort_bytes((long long)N);
   rc |= alloc(S, &S.cub_tmp, S.cub_bytes);
-  if (rc) return fail(WCSPH_E_NOMEM);
+  if (opt->list_interval > 0) {
+    rc |= alloc(S, (void**)&S.list, N * kListMax * sizeof(uint32_t));
+    rc |= alloc(S, (void**)&S.list_cnt, N * sizeof(int));
+    rc |= alloc(S, (void**)&S.x0, N * sizeof(float4));
+    rc |= alloc(S, (void**)&S.d_lflags, 4 * sizeof(unsigned));
+    if (!rc && cudaHostAlloc((void**)&S.h_lflags, 4 * sizeof(unsigned), cudaHostAllocDefault) != cudaSuccess)
+      rc = 1;
+  }
+  if (rc) {
+    if (S.h_lflags) cudaFreeHost(S.h_lflags);
+    return fail(WCSPH_E_NOMEM);
+  }
   if (cudaMemsetAsync(S.d_dyn, 0, (size_t)opt->max_instances * sizeof(InstDyn), S.s) != cudaSuccess ||
       cudaMemsetAsync(S.d_n_alive, 0, sizeof(int), S.s) != cudaSuccess ||
       cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s) != cudaSuccess ||
-      cudaEventCreate(&S.ev0) != cudaSuccess || cudaEventCreate(&S.ev1) != cudaSuccess)
+      cudaEventCreate(&S.ev0) != cudaSuccess || cudaEventCreate(&S.ev1) != cudaSuccess ||
+      cudaEventCreateWithFlags(&S.step_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&S.step_ev[1], cudaEventDisableTiming) != cudaSuccess)
     return fail(WCSPH_E_CUDA);
+  if (S.d_lflags) {
+    memset(S.h_lflags, 0, 4 * sizeof(unsigned));
+    if (cudaMemsetAsync(S.d_lflags, 0, 4 * sizeof(unsigned), S.s) != cudaSuccess) return fail(WCSPH_E_CUDA);
+  }
   *out = sim;
   return 0;
 }
@@ -480,7 +681,11 @@ int wcsph_sim_destroy(wcsph_sim* sim) {
   cudaSetDevice(S.opt.device);
   cudaStreamSynchronize(S.s);
   if (S.gexec) cudaGraphExecDestroy(S.gexec);
+  if (S.gexec_reuse) cudaGraphExecDestroy(S.gexec_reuse);
   for (void* p : S.allocs) cudaFree(p);
+  if (S.h_lflags) cudaFreeHost(S.h_lflags);
+  for (cudaEvent_t e : S.step_ev)
+    if (e) cudaEventDestroy(e);
   cudaEventDestroy(S.ev0);
   cudaEventDestroy(S.ev1);
   cudaStreamDestroy(S.s);
@@ -581,6 +786,12 @@ static int append_instance(SimImpl& S, const AppendSpec& A, int32_t* slot) {
     I.geom = SlabGeom{sl.x_lo, sl.x_hi, W, sl.has_left ? 1 : 0, sl.has_right ? 1 : 0};
     P.slab_margin2 = sl.margin * sl.margin;
   }
+  if (S.opt.list_interval > 0) {
+    const float skin = list_skin(S.opt) * (float)d.h, R = 2.0f * (float)d.h + skin;
+    P.HL2 = R * R;
+    P.inv_skin = 1.0f / skin;
+  }
+  I.host_steps = A.saved ? A.saved->steps : 0;
   I.used = I.active = true;
   HostInst prev = S.inst[k];
   InstParams prev_p = S.h_params[k];
@@ -620,6 +831,7 @@ static int append_instance(SimImpl& S, const AppendSpec& A, int32_t* slot) {
   WCSPH_CUDA(cudaMemcpyAsync(S.d_dyn + k, &dyn, sizeof(InstDyn), cudaMemcpyHostToDevice, S.s));
   S.n_host = base + n;
   S.appended = true;
+  S.lists_valid = false;
   if (slot) *slot = k;
   if (A.after == AppendSpec::INIT_PASS) return init_force_pass(S, k);
   if (A.after == AppendSpec::BIN_PASS) {
@@ -791,6 +1003,7 @@ int wcsph_sim_slab_pack(wcsph_sim* sim, int32_t slot, void* send, int64_t capaci
   }
   const int n = S.n_host;
   const SlabGeom G = S.inst[slot].geom;
+  S.lists_valid = false;
   int h_counts[4] = {0, 0, 0, 0};
   if (n > 0) {
     // class keys and indices in the step's sort buffers (free between passes)
@@ -848,6 +1061,7 @@ int wcsph_sim_slab_unpack(wcsph_sim* sim, int32_t slot, const void* recv, int32_
   WCSPH_CUDA(cudaStreamSynchronize(S.s));
   S.n_host += (int)m;
   S.appended = true;
+  S.lists_valid = false;
   S.graph_dirty = true;
   return 0;
 }
@@ -862,6 +1076,7 @@ int wcsph_sim_remove_instance(wcsph_sim* sim, int32_t slot) {
   WCSPH_CUDA(cudaSetDevice(S.opt.device));
   S.inst[slot].active = false;  // particles are marked dead by the next binning
   S.inst[slot].drained = false;
+  S.lists_valid = false;
   S.h_phase[slot] = PH_IDLE;
   return rebuild_tables(S);
 }
@@ -871,6 +1086,16 @@ int wcsph_sim_step(wcsph_sim* sim, int32_t nsteps) {
   SimImpl& S = sim->impl;
   WCSPH_CUDA(cudaSetDevice(S.opt.device));
   if (nsteps == 0) return 0;
+  if (S.opt.list_interval > 0) {
+    if (S.opt.use_graph && (S.graph_dirty || !S.gexec || !S.gexec_reuse)) {
+      if (int rc = autotune(S)) return rc;
+      if (int rc = capture_list_graphs(S)) return rc;
+    }
+    for (int t = 0; t < nsteps; ++t)
+      if (int rc = list_step(S, S.opt.use_graph != 0, nullptr)) return rc;
+    mark_drained(S);
+    return 0;
+  }
   StepArgs a = make_args(S);
   if (!S.opt.use_graph) {
     WCSPH_CUDA(cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s));
@@ -1104,6 +1329,22 @@ int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out3) {
   return 0;
 }
 
+int wcsph_sim_list_stats(wcsph_sim* sim, int64_t* out6) {
+  if (!sim || !out6) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  unsigned mx = 0;
+  if (S.d_lflags) WCSPH_CUDA(cudaMemcpy(&mx, S.d_lflags + 3, sizeof(mx), cudaMemcpyDeviceToHost));
+  out6[0] = S.n_builds;
+  out6[1] = S.n_reuse;
+  out6[2] = S.n_overflow;
+  out6[3] = (int64_t)mx;
+  out6[4] = S.kernels_per_step;
+  out6[5] = S.kernels_reuse;
+  return 0;
+}
+
 int wcsph_sim_profile_steps(wcsph_sim* sim, int32_t nsteps, double* ms4) {
   if (!sim || !ms4 || nsteps < 0) return WCSPH_E_INVALID;
   SimImpl& S = sim->impl;
@@ -1114,8 +1355,12 @@ int wcsph_sim_profile_steps(wcsph_sim* sim, int32_t nsteps, double* ms4) {
   StepArgs a = make_args(S);
   int rc = 0;
   for (int t = 0; t < nsteps && !rc; ++t) {
-    if (cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s) != cudaSuccess) rc = WCSPH_E_CUDA;
-    if (!rc) rc = enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step, ev);
+    if (S.opt.list_interval > 0) {
+      rc = list_step(S, false, ev);  // the same build / list-step schedule as wcsph_sim_step
+    } else {
+      if (cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s) != cudaSuccess) rc = WCSPH_E_CUDA;
+      if (!rc) rc = enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step, ev);
+    }
     if (!rc && cudaEventSynchronize(ev[3]) != cudaSuccess) rc = WCSPH_E_CUDA;
     float x[3];
     if (!rc) {

@@ -38,6 +38,14 @@ struct StepArgs {
   int* run_list;          // linear index of every non-empty cell (unordered)
   int* run_count;         // number of entries in run_list
   int init_filter;        // initial-pass Shepard filter launch (main.cpp:75)
+  // neighbour lists (list_interval > 0)
+  uint32_t* list;         // list_max entries per sorted slot: slot | image code << 27
+  int* list_cnt;          // entries per slot
+  int list_max;
+  float4* x0;             // build steps: record the positions the lists were built at
+  unsigned* list_flags;   // [0] max |x - x0| / skin, [1] max step drift / skin (float bits),
+                          // [2] sticky errors (1 skin exceeded, 2 overflow), [3] largest list
+  int list_reuse;         // this step reads the lists: periodic wrapping waits for the next build
   int probe_density;      // density pass of a probe launch: 0 none, 1 summation, 2 Shepard
   // diagnostics (probe phase)
   float4* diag_acc;
@@ -56,8 +64,10 @@ __global__ void k_step_begin(StepArgs a) {
     InstDyn& d = a.dyn[k];
     const InstParams& P = a.params[k];
     const int ph = a.phase[k];
-    d.range_lo = 0x7fffffff;
-    d.range_hi = 0;
+    if (!a.list_reuse) {  // the binning sets them again; a list step keeps the build's order
+      d.range_lo = 0x7fffffff;
+      d.range_hi = 0;
+    }
     if (ph == PH_STEP && P.active) {
       const float dt = d.finished ? 0.0f : bits_f(d.dt_next_bits);
       d.dt_cur = dt;
@@ -74,7 +84,7 @@ __global__ void k_step_begin(StepArgs a) {
       d.dt_cur = 0.0f;
     }
   }
-  if (k == 0) *a.n_alive = a.n_host;
+  if (k == 0 && !a.list_reuse) *a.n_alive = a.n_host;
 }
 
 // ------------------------------------------------------- kick + binning
@@ -90,6 +100,7 @@ __global__ void k_kick_bin(StepArgs a) {
   float4 x = a.main.pos[p];
   float4 v = a.main.vel[p];
   float4 vh = v;
+  unsigned drift_bits = 0u;  // this step's drift / skin (float bits; positive floats order like their bits)
   if (!dead) {
     const int ph = a.phase[inst];
     const float dt = a.dyn[inst].dt_cur;
@@ -104,8 +115,10 @@ __global__ void k_kick_bin(StepArgs a) {
         x.z += dt * vh.z;
         if (P.slab_margin2 > 0.0f && dt * dt * (vh.x * vh.x + vh.y * vh.y + vh.z * vh.z) > P.slab_margin2)
           atomicOr(&a.dyn[inst].errors, kErrDrift);  // the ghost layer no longer covers this drift
+        if (a.list_flags && P.inv_skin > 0.0f)
+          drift_bits = __float_as_uint(dt * sqrtf(vh.x * vh.x + vh.y * vh.y + vh.z * vh.z) * P.inv_skin);
         v = make_float4(v.x + dt * acc.x, v.y + dt * acc.y, v.z + dt * acc.z, 0.f);
-        if (P.periodic) {
+        if (P.periodic && !a.list_reuse) {  // between list builds positions run on continuously
           float* c = &x.x;
 #pragma unroll
           for (int k = 0; k < 3; ++k) {
@@ -137,6 +150,11 @@ __global__ void k_kick_bin(StepArgs a) {
   }
   a.keys_in[p] = key;
   a.vals_in[p] = p;
+  if (a.list_flags) {  // warp-aggregated maximum of the drift ratio
+    const unsigned m = __activemask();
+    const unsigned mx = __reduce_max_sync(m, drift_bits);
+    if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && mx) atomicMax(&a.list_flags[1], mx);
+  }
 }
 
 // ------------------------------------------------- permutation + tables
@@ -177,6 +195,7 @@ __global__ void k_permute(StepArgs a) {
   if (p == 0 || kprev == kDeadKey || (int)(a.main.flags[a.vals_out[p - 1]] & kInstMask) != inst)
     a.dyn[inst].range_lo = p;
   if (knext == kDeadKey || (int)(a.main.flags[a.vals_out[p + 1]] & kInstMask) != inst) a.dyn[inst].range_hi = p + 1;
+  if (a.x0) a.x0[p] = make_float4(x.x, x.y, x.z, 0.f);  // list build: positions the lists refer to
   float pres, snds;
   tait(P, x.w, pres, snds);
   a.jA[p] = make_float4(x.x, x.y, x.z, pres / (x.w * x.w));

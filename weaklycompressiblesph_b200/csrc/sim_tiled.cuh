@@ -99,7 +99,10 @@ __device__ __forceinline__ void entry_shift(const InstParams& P, uint32_t code, 
 // H16: the kernel gradient (|dr|^2, 1/|dr|, s, F(s), F/|dr|) is evaluated in
 // packed half2 on displacements in units of the support 2h; everything else
 // stays FP32 (WCSPH_PREC_HALF2).
-template <bool H16>
+// CHECK: the queues may hold entries outside the support (neighbour lists with
+// a skin); each entry is tested for 0 < r^2 < (2h)^2 on the current positions,
+// entries outside contribute exactly zero and are not counted.
+template <bool H16, bool CHECK = false>
 __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParams& P, int ia, int ib, bool has_b,
                                               const float4& IA, const float4& IBp, const uint32_t* qa, int na,
                                               const uint32_t* qb, int nb, float (*res)[6], int lane) {
@@ -118,11 +121,12 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
   const int n = max(na, nbq);
   f2 AX = 0ull, AY = 0ull, AZ = 0ull, DS = 0ull;
   float vsa = 0.f, vsb = 0.f;
+  unsigned ca = 0, cb = 0;  // CHECK: in-support entries of this lane
   for (int k = lane; k < n; k += 32) {
-    const bool va = k < na, vb = k < nbq;
+    const bool qva = k < na, qvb = k < nbq;
     // idle halves read i_a's own record (always a valid slot; weight 0 below)
     const uint32_t self = (uint32_t)ia | (13u << 27);
-    const uint32_t ea = va ? qa[k] : self, eb = vb ? qb[k] : self;
+    const uint32_t ea = qva ? qa[k] : self, eb = qvb ? qb[k] : self;
     const int ga = ea & kSlotMask, gb = eb & kSlotMask;
     const float4 Ja = __ldg(&a.jA[ga]), Jb = __ldg(&a.jA[gb]);
     const float4 JBa = __ldg(&a.jB[ga]), JBb = __ldg(&a.jB[gb]);
@@ -137,6 +141,9 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
     }
     const f2 DX = sub2(X, pk(jxa, jxb)), DY = sub2(Y, pk(jya, jyb)), DZ = sub2(Z, pk(jza, jzb));
     const f2 R2raw = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
+    const bool va = CHECK ? qva && lo(R2raw) > 0.0f && lo(R2raw) < H2 : qva;
+    const bool vb = CHECK ? qvb && hi(R2raw) > 0.0f && hi(R2raw) < H2 : qvb;
+    if (CHECK) ca += va, cb += vb;
     const f2 R2 = pk(va ? lo(R2raw) : H2, vb ? hi(R2raw) : H2);  // finite stand-in for idle halves
     const f2 W = pk(va ? 1.0f : 0.0f, vb ? 1.0f : 0.0f);
     f2 G;  // gradW = G * dr
@@ -192,12 +199,16 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
     if (slot < 4) res[0][slot] += y;
     else if (has_b) res[1][slot - 4] += y;
   }
+  if (CHECK) {
+    ca = __reduce_add_sync(0xffffffffu, ca);
+    cb = __reduce_add_sync(0xffffffffu, cb);
+  }
   if (lane == 0) {
     res[0][4] = fmaxf(res[0][4], vsa);
-    res[0][5] += (float)na;
+    res[0][5] += (float)(CHECK ? (int)ca : na);
     if (has_b) {
       res[1][4] = fmaxf(res[1][4], vsb);
-      res[1][5] += (float)nb;
+      res[1][5] += (float)(CHECK ? (int)cb : nb);
     }
   }
 }
@@ -211,7 +222,10 @@ __device__ __forceinline__ void append2(uint32_t* q, int& n, bool he, bool ho, u
   n += __popc(me) + __popc(mo);
 }
 
-template <bool H16, int WARPS, int TILE>
+// LB (neighbour-list build): the scan keeps candidates within the list radius
+// 2h + skin, each i's queue entries are also written to its list, and the
+// pair phase tests the support per entry (CHECK).
+template <bool H16, int WARPS, int TILE, bool LB = false>
 __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
   constexpr int kTiledWarps = WARPS;
   constexpr int kTile = TILE;
@@ -243,7 +257,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
     const InstParams& P = a.params[inst];
     const int ph = a.phase[inst];
     if (!wants_force(P, a.dyn[inst], ph)) {
-      for (int p = s + lane; p < e; p += 32) copy_state(a, p);
+      for (int p = s + lane; p < e; p += 32) {
+        copy_state(a, p);
+        if (LB) a.list_cnt[p] = 0;
+      }
       continue;
     }
     const int nx = P.ncell[0], ny = P.ncell[1];
@@ -273,11 +290,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
     const int T = __shfl_sync(full, incl, 31);
     const int excl = incl - nb_cnt;
     const int own = __shfl_sync(full, excl, 13);  // tile offset of the cell's own particles
-    const float H2 = P.H2;
+    const float HS = LB ? P.HL2 : P.H2;  // scan bound
     float dt_cand = 0.f;
     bool dt_valid = false;
     for (int ib = s; ib < e; ib += 32) {
       const int nbat = min(32, e - ib);
+      int lcount = 0;  // LB: list entries written so far for i = ib + lane
 #pragma unroll
       for (int k = 0; k < 6; ++k) res[lane][k] = 0.f;
       for (int t0 = 0; t0 < T; t0 += kTile) {
@@ -349,15 +367,37 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
             DX = sub2(XB, CX), DY = sub2(YB, CY), DZ = sub2(ZB, CZ);
             const f2 RB = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
             const float ra0 = lo(RA), ra1 = hi(RA), rb0 = lo(RB), rb1 = hi(RB);
-            append2(qa, na, ra0 > 0.0f && ra0 < H2, ra1 > 0.0f && ra1 < H2, E.x, E.y, lt);
-            append2(qb, nb, has_b && rb0 > 0.0f && rb0 < H2, has_b && rb1 > 0.0f && rb1 < H2, E.x, E.y, lt);
+            append2(qa, na, ra0 > 0.0f && ra0 < HS, ra1 > 0.0f && ra1 < HS, E.x, E.y, lt);
+            append2(qb, nb, has_b && rb0 > 0.0f && rb0 < HS, has_b && rb1 > 0.0f && rb1 < HS, E.x, E.y, lt);
           }
           __syncwarp();
-          hydro_queues2<H16>(a, P, ia, ibb, has_b, IA, IB, qa, na, qb, nb, &res[ii], lane);
+          if (LB) {  // append this tile pass's queue entries to the lists of ia and ibb
+            const int L = a.list_max;
+            const int oa = __shfl_sync(full, lcount, ii), ob = __shfl_sync(full, lcount, ii + 1);
+            uint32_t* la = a.list + (size_t)ia * L;
+            for (int k = lane; k < na; k += 32)
+              if (oa + k < L) la[oa + k] = qa[k];
+            if (has_b) {
+              uint32_t* lb = a.list + (size_t)ibb * L;
+              for (int k = lane; k < nb; k += 32)
+                if (ob + k < L) lb[ob + k] = qb[k];
+            }
+            if (lane == ii) lcount += na;
+            if (has_b && lane == ii + 1) lcount += nb;
+          }
+          hydro_queues2<H16, LB>(a, P, ia, ibb, has_b, IA, IB, qa, na, qb, nb, &res[ii], lane);
           __syncwarp();
         }
       }
       __syncwarp();
+      if (LB) {
+        if (lane < nbat) {
+          a.list_cnt[ib + lane] = min(lcount, a.list_max);
+          if (lcount > a.list_max) atomicOr(&a.list_flags[2], 2u);  // overflow: rebuild next step
+        }
+        const int mx = __reduce_max_sync(full, lane < nbat ? lcount : 0);
+        if (lane == 0) atomicMax(&a.list_flags[3], (unsigned)mx);
+      }
       if (lane < nbat) {
         const int p = ib + lane;
         const float* r = res[lane];
@@ -378,13 +418,13 @@ struct TiledLaunch {
   int blocks = 0;
 };
 
-template <bool H16, int WARPS, int TILE>
+template <bool H16, int WARPS, int TILE, bool LB>
 inline int launch_pair_tiled_v(const StepArgs& a, cudaStream_t s) {
   static TiledLaunch L[16];
   int dev = 0;
   WCSPH_CUDA(cudaGetDevice(&dev));
   TiledLaunch& T = L[dev & 15];
-  auto kern = k_hydro_tiled<H16, WARPS, TILE>;
+  auto kern = k_hydro_tiled<H16, WARPS, TILE, LB>;
   const int bytes = (int)sizeof(TiledSmem<WARPS, TILE>);
   if (T.device != dev) {
     WCSPH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
@@ -404,16 +444,16 @@ inline int launch_pair_tiled_v(const StepArgs& a, cudaStream_t s) {
 // order of any sum, so results are bit-identical whichever is chosen.
 constexpr int kTileShapes = 3;
 
-template <bool H16>
+template <bool H16, bool LB = false>
 inline int launch_hydro_tiled(const StepArgs& a, int n, cudaStream_t s, int shape = 0) {
   if (n > kMaxTiledParticles) {
     set_error("the tiled path holds at most %d particles per solver (got %d)", kMaxTiledParticles, n);
     return WCSPH_E_CAPACITY;
   }
   switch (shape) {
-    case 1: return launch_pair_tiled_v<H16, 2, 512>(a, s);
-    case 2: return launch_pair_tiled_v<H16, 8, 512>(a, s);
-    default: return launch_pair_tiled_v<H16, 4, 512>(a, s);
+    case 1: return launch_pair_tiled_v<H16, 2, 512, LB>(a, s);
+    case 2: return launch_pair_tiled_v<H16, 8, 512, LB>(a, s);
+    default: return launch_pair_tiled_v<H16, 4, 512, LB>(a, s);
   }
 }
 

@@ -91,6 +91,8 @@ struct InstParams {
   float dt_nu;            // 0.125 h^2 / nu (or +inf)
   float kill_lo[3], kill_hi[3];
   float slab_margin2;     // slab instances: squared largest drift a step may make (0: not a slab)
+  float HL2;              // neighbour lists: squared list radius (2h + skin)^2
+  float inv_skin;         // neighbour lists: 1 / skin (0: lists off)
   double t_end;
 };
 

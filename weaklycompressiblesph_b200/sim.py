@@ -26,7 +26,9 @@ def _f32(a, shape):
 
 class Solver:
     def __init__(self, max_particles, precision=N.PREC_FP32, max_cells=None, max_instances=64, device=0,
-                 use_graph=True, autotune=True):
+                 use_graph=True, autotune=True, list_interval=0, list_skin=0.0):
+        """list_interval > 0 turns on neighbour lists (radius 2h + list_skin h,
+        rebuilt at least every list_interval steps; see wcsph_sim_options)."""
         o = N.SimOptions()
         o.device = device
         o.precision = precision
@@ -35,6 +37,8 @@ class Solver:
         o.max_instances = int(max_instances)
         o.use_graph = 1 if use_graph else 0
         o.autotune = 1 if autotune else 0
+        o.list_interval = int(list_interval)
+        o.list_skin = float(list_skin)
         self.opt = o
         h = C.c_void_p()
         N.call("wcsph_sim_create", C.byref(o), C.byref(h))
@@ -207,6 +211,12 @@ class Solver:
     def stream(self):
         """The solver's cudaStream_t as an integer handle."""
         return int(N.lib().wcsph_sim_stream(self._h) or 0)
+
+    def list_stats(self):
+        out = (C.c_int64 * 6)()
+        N.call("wcsph_sim_list_stats", self._h, out)
+        return dict(builds=int(out[0]), list_steps=int(out[1]), overflows=int(out[2]), longest=int(out[3]),
+                    kernels_build=int(out[4]), kernels_list=int(out[5]))
 
     def profile_steps(self, nsteps):
         """Advance nsteps eagerly with CUDA events per phase; returns ms summed
