@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--precision", default="best", choices=["best", "fp32", "tiled", "half2"])
     ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
                     help="N>1: independent replicas (weak scaling) or one dam break cut into x-slabs (strong)")
+    ap.add_argument("--list-interval", type=int, default=0,
+                    help="neighbour lists rebuilt at least every K steps (0: search every step)")
+    ap.add_argument("--list-skin", type=float, default=0.0, help="list skin in units of h (0: 0.2)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-only", action="store_true",
                     help="time only the FDPS drop-in pass (dispatch + retrieve from host records), --steps passes")
@@ -194,15 +197,18 @@ def best_precision():
     return BEST_PRECISION
 
 
-def run_device(case, prec_name, steps, warmup, device, clocks=False):
+def run_device(case, prec_name, steps, warmup, device, clocks=False, list_interval=0, list_skin=0.0):
     """Timed device-resident steps; returns dict of measurements."""
     from weaklycompressiblesph_b200.sim import Solver
     res = {}
-    with Solver(case.n + 1024, precision=precision_code(prec_name), device=device, max_instances=4) as s:
+    lists = list_interval > 0 and prec_name != "fp32"
+    with Solver(case.n + 1024, precision=precision_code(prec_name), device=device, max_instances=4,
+                list_interval=list_interval if lists else 0, list_skin=list_skin) as s:
         k = s.add(case)
         s.step(warmup)
         s.synchronize()
         pairs = s.last_pairs()
+        ls0 = s.list_stats() if lists else None
         sampler = ClockSampler(device) if clocks else None
         if sampler:
             sampler.__enter__()
@@ -214,6 +220,12 @@ def run_device(case, prec_name, steps, warmup, device, clocks=False):
         res["ms_per_step"] = ms / steps
         res["pairs_per_step"] = 0.5 * (pairs + pairs_end)
         res["kernels_per_step"] = s.kernels_per_step()
+        if lists:
+            ls1 = s.list_stats()
+            b, r = ls1["builds"] - ls0["builds"], ls1["list_steps"] - ls0["list_steps"]
+            res["kernels_per_step"] = (b * ls1["kernels_build"] + r * ls1["kernels_list"]) / max(1, b + r)
+            res["lists"] = {"interval": list_interval, "skin_h": list_skin or 0.2, "timed_builds": b,
+                            "timed_list_steps": r, "overflows": ls1["overflows"], "longest": ls1["longest"]}
         # per-phase kernel times (eager launches, CUDA events on the solver stream)
         prof_steps = max(3, min(20, steps // 5))
         ph = s.profile_steps(prof_steps)
@@ -426,7 +438,8 @@ def main():
         args.no_plain = args.no_e2e = args.no_ensemble = True
         dev = run_slab(case, prec, args.steps, args.warmup, rank, world, local, pg, clocks=(rank == 0))
     else:
-        dev = run_device(case, prec, args.steps, args.warmup, local, clocks=(rank == 0))
+        dev = run_device(case, prec, args.steps, args.warmup, local, clocks=(rank == 0),
+                         list_interval=args.list_interval, list_skin=args.list_skin)
     ms = max_over_ranks(pg, dev["ms_per_step"])
     pairs_all = sum_over_ranks(pg, dev["pairs_per_step"])
     value = pairs_all / (ms * 1e-3)
@@ -493,7 +506,8 @@ def main():
         "autotune": dev.get("tuning"),
         "ensemble": ens,
         "serving": srv,
-        "gpu_launches": dev["kernels_per_step"] * args.steps,
+        "gpu_launches": int(round(dev["kernels_per_step"] * args.steps)),
+        "neighbour_lists": dev.get("lists"),
         "clocks": dev.get("clocks"),
         "sim_time_s": dev["status"]["time"],
     }

@@ -8,9 +8,10 @@
 //                 so that the lists' image shifts stay valid)
 //   k_refresh     state copied in place (the sorted order of the build is
 //                 kept), EoS j-records refreshed, |x - x0| checked
-//   k_hydro_list  the tiled kernel's pair phase over each particle's list,
-//                 every entry tested for 0 < r^2 < (2h)^2 on the current
-//                 positions, then the shared epilogue
+//   k_hydro_list  the tiled kernel's pair phase over each particle's list
+//                 (warp per cell of the build's cell table), every entry
+//                 tested for 0 < r^2 < (2h)^2 on the current positions, then
+//                 the shared epilogue
 // A pair within the support now was within 2h + |dx_i| + |dx_j| at the
 // build, so the lists hold every pair the support test can accept while no
 // particle has moved more than skin / 2 since the build.  The host rebuilds
@@ -22,7 +23,9 @@
 
 namespace wcsph {
 
-constexpr int kListWarps = 8;
+constexpr int kListWarps = 4;
+constexpr int kListMaxEntries = 256;  // entries per list (the solver's list_max)
+constexpr int kListPerLane = kListMaxEntries / 32;
 
 // Copy main -> alt in place, refresh the j-records, check the displacement.
 __global__ void k_refresh(StepArgs a) {
@@ -61,82 +64,112 @@ __global__ void k_refresh(StepArgs a) {
   if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && mx) atomicMax(&a.list_flags[0], mx);
 }
 
-// Pair sums of ia (and ib = ia + 1 when has_b: same instance) from their lists.
-template <bool H16>
-__device__ __forceinline__ void list_group(const StepArgs& a, int ia, bool has_b, float (*res)[6], int lane,
-                                           unsigned long long& pairs) {
-  const int ib = has_b ? ia + 1 : ia;
-  const uint32_t fa = a.alt.flags[ia], fb = a.alt.flags[ib];
-  const int inst = fa & kInstMask;
-  const InstParams& P = a.params[inst];
-  const int ph = a.phase[inst];
-  if (!wants_force(P, a.dyn[inst], ph)) {
-    if (lane == 0) copy_state(a, ia);
-    if (lane == 1 && has_b) copy_state(a, ib);
-    return;
-  }
-  const bool da = fa & kDeadBit, db = fb & kDeadBit;
-  const int na = da ? 0 : a.list_cnt[ia];
-  const int nb = (!has_b || db) ? 0 : a.list_cnt[ib];
-  if (lane < 12) (&res[0][0])[lane] = 0.f;
-  __syncwarp();
-  const uint32_t* qa = a.list + (size_t)ia * a.list_max;
-  const uint32_t* qb = a.list + (size_t)ib * a.list_max;
-  hydro_queues2<H16, true>(a, P, ia, ib, has_b, a.jA[ia], a.jA[ib], qa, na, qb, nb, res, lane);
-  __syncwarp();
-  float dt_cand = 0.f;
-  bool dt_valid = false;
-  if (lane < (has_b ? 2 : 1)) {
-    const int p = ia + lane;
-    const uint32_t fp = lane ? fb : fa;
-    const float* r = res[lane];
-    if (fp & kDeadBit) {
-      copy_state(a, p);
-    } else {
-      if (!(fp & kGhostBit)) pairs += (unsigned long long)r[5];
-      finish_hydro(a, p, P, inst, ph, fp, r[0], r[1], r[2], r[3], r[4], (unsigned)r[5], dt_cand, dt_valid);
-    }
-  }
-  dt_min(a.dyn, inst, dt_cand, dt_valid);
-}
-
-// One warp per pair of consecutive sorted slots (a pair split across two
-// instances is summed one particle at a time).
-template <bool H16>
-__global__ void __launch_bounds__(kListWarps * 32) k_hydro_list(StepArgs a) {
-  __shared__ float s_res[kListWarps][2][6];
+// The pair phase of the tiled kernel over the lists.  The cell table of the
+// last build is still valid (list steps do not re-sort), so the work is laid
+// out as in k_hydro_tiled: warp per non-empty cell, batches of 32 particles,
+// pairs of i at a time; each pair's two lists are copied into shared-memory
+// queues with coalesced loads, the shared pair routine tests the support per
+// entry, and lane l finishes particle batch + l with the shared epilogue.
+template <bool H16, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_hydro_list(StepArgs a) {
+  __shared__ uint32_t s_q[WARPS][2][kListMaxEntries];
+  __shared__ float s_res[WARPS][32][6];
+  const unsigned full = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t* qa = s_q[warp][0];
+  uint32_t* qb = s_q[warp][1];
   float(*res)[6] = s_res[warp];
-  const int n = *a.n_alive;
+  const int L = a.list_max;
+  const int nrun = *a.run_count;
   unsigned long long pairs = 0;
-  for (int q = blockIdx.x * kListWarps + warp; 2 * q < n; q += gridDim.x * kListWarps) {
-    const int ia = 2 * q, ib = ia + 1;
-    const bool two = ib < n;
-    const bool same = two && (a.alt.flags[ia] & kInstMask) == (a.alt.flags[ib] & kInstMask);
-    list_group<H16>(a, ia, same, res, lane, pairs);
-    if (two && !same) {
-      __syncwarp();
-      list_group<H16>(a, ib, false, res, lane, pairs);
+  const int stride = gridDim.x * WARPS;
+  for (int c = blockIdx.x * WARPS + warp; c < nrun; c += stride) {
+    const int lin = a.run_list[c];
+    const int s = a.cell_start[lin], e = a.cell_end[lin];
+    const int inst = a.alt.flags[s] & kInstMask;
+    const InstParams& P = a.params[inst];
+    const int ph = a.phase[inst];
+    if (!wants_force(P, a.dyn[inst], ph)) {
+      for (int p = s + lane; p < e; p += 32) copy_state(a, p);
+      continue;
     }
-    __syncwarp();
+    float dt_cand = 0.f;
+    bool dt_valid = false;
+    for (int ib = s; ib < e; ib += 32) {
+      const int nbat = min(32, e - ib);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) res[lane][k] = 0.f;
+      // list lengths of the batch in one load (particles removed since the
+      // build keep their state and sum nothing)
+      const int my_n = lane < nbat && !(a.alt.flags[ib + lane] & kDeadBit) ? min(a.list_cnt[ib + lane], L) : 0;
+      // entries of the next pair are loaded into registers while the current
+      // pair is summed
+      uint32_t ra[kListPerLane], rb[kListPerLane];
+      auto fetch = [&](int ii) {
+        const int na = __shfl_sync(full, my_n, ii), nb = __shfl_sync(full, my_n, min(ii + 1, 31));
+        const bool has_b = ii + 1 < nbat;
+        const uint32_t* la = a.list + (size_t)(ib + ii) * L;
+        const uint32_t* lb = a.list + (size_t)(ib + (has_b ? ii + 1 : ii)) * L;
+#pragma unroll
+        for (int j = 0; j < kListPerLane; ++j) {
+          const int k = lane + 32 * j;
+          ra[j] = k < na ? __ldg(&la[k]) : 0u;
+          rb[j] = has_b && k < nb ? __ldg(&lb[k]) : 0u;
+        }
+      };
+      fetch(0);
+      for (int ii = 0; ii < nbat; ii += 2) {
+        const int ia = ib + ii;
+        const bool has_b = ii + 1 < nbat;
+        const int ibb = has_b ? ia + 1 : ia;
+        const int na = __shfl_sync(full, my_n, ii), nb = has_b ? __shfl_sync(full, my_n, ii + 1) : 0;
+#pragma unroll
+        for (int j = 0; j < kListPerLane; ++j) {
+          const int k = lane + 32 * j;
+          if (k < na) qa[k] = ra[j];
+          if (k < nb) qb[k] = rb[j];
+        }
+        __syncwarp();
+        if (ii + 2 < nbat) fetch(ii + 2);
+        hydro_queues2<H16, true>(a, P, ia, ibb, has_b, __ldg(&a.jA[ia]), __ldg(&a.jA[ibb]), qa, na, qb, nb,
+                                 &res[ii], lane);
+        __syncwarp();
+      }
+      __syncwarp();
+      if (lane < nbat) {
+        const int p = ib + lane;
+        const uint32_t fp = a.alt.flags[p];
+        if (fp & kDeadBit) {
+          copy_state(a, p);
+        } else {
+          const float* r = res[lane];
+          if (!(fp & kGhostBit)) pairs += (unsigned long long)r[5];
+          finish_hydro(a, p, P, inst, ph, fp, r[0], r[1], r[2], r[3], r[4], (unsigned)r[5], dt_cand, dt_valid);
+        }
+      }
+      __syncwarp();
+    }
+    dt_min(a.dyn, inst, dt_cand, dt_valid);
   }
-  pairs = __reduce_add_sync(0xffffffffu, (unsigned)pairs);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(full, pairs, o);
   if (lane == 0 && pairs) atomicAdd(a.pair_count, pairs);
 }
 
 template <bool H16>
 inline int launch_hydro_list(const StepArgs& a, int n, cudaStream_t s) {
+  (void)n;
   static int blocks[16] = {0};
   int dev = 0;
   WCSPH_CUDA(cudaGetDevice(&dev));
+  auto kern = k_hydro_list<H16, kListWarps>;
   if (!blocks[dev & 15]) {
     int per_sm = 0, sms = 0;
-    WCSPH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hydro_list<H16>, kListWarps * 32, 0));
+    WCSPH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kListWarps * 32, 0));
     WCSPH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     blocks[dev & 15] = std::max(1, per_sm) * sms;
   }
-  const int need = (n / 2 + kListWarps) / kListWarps + 1;
-  k_hydro_list<H16><<<std::min(need, blocks[dev & 15]), kListWarps * 32, 0, s>>>(a);
+  kern<<<blocks[dev & 15], kListWarps * 32, 0, s>>>(a);
   WCSPH_CUDA(cudaGetLastError());
   return 0;
 }
