@@ -1,5 +1,6 @@
 """Config-2 validation: the dam break at dx = 0.005 (1,024,000 fluid + 571,308
-wall particles), FP32 (tiled) vs half2-gradient paths.
+wall particles), FP32 (tiled) vs half2-gradient paths, and the tiled path
+with neighbour lists.
 
     python tests/validate_dam_break.py [--steps 5000] [--every 500] [--dx 0.005]
 
@@ -45,10 +46,10 @@ def check(case, s, k):
             "neighbors_exact": bool(np.array_equal(pr["nbr"], cnt))}
 
 
-def run(case, precision, steps, every):
+def run(case, precision, steps, every, list_interval=0):
     front = []
     checks = []
-    with Solver(case.n + 1024, precision=precision) as s:
+    with Solver(case.n + 1024, precision=precision, list_interval=list_interval) as s:
         k = s.add(case)
         fluid = case.type == N.HYDRO
         t0 = time.perf_counter()
@@ -67,7 +68,8 @@ def run(case, precision, steps, every):
             s.step(n)
             done += n
         wall = time.perf_counter() - t0
-    return {"front": front, "checks": checks, "wall_s": wall}
+        lists = s.list_stats() if list_interval else None
+    return {"front": front, "checks": checks, "wall_s": wall, "lists": lists}
 
 
 def main():
@@ -75,14 +77,19 @@ def main():
     ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--every", type=int, default=1000)
     ap.add_argument("--dx", type=float, default=0.005)
+    ap.add_argument("--list-interval", type=int, default=30,
+                    help="also run the tiled path with neighbour lists rebuilt at least every K steps (0: skip)")
     args = ap.parse_args()
     case = cases.dam_break(dx=args.dx)
     out = {"case": case.name, "particles": case.n, "steps": args.steps}
     res = {}
-    for name, prec in (("fp32_tiled", N.PREC_TILED), ("half2", N.PREC_HALF2)):
-        res[name] = run(case, prec, args.steps, args.every)
+    paths = [("fp32_tiled", N.PREC_TILED, 0), ("half2", N.PREC_HALF2, 0)]
+    if args.list_interval:
+        paths.append(("tiled_lists", N.PREC_TILED, args.list_interval))
+    for name, prec, k in paths:
+        res[name] = run(case, prec, args.steps, args.every, list_interval=k)
         out[name] = {"checks": res[name]["checks"], "sim_time_end": res[name]["front"][-1][0],
-                     "front_end": res[name]["front"][-1][1]}
+                     "front_end": res[name]["front"][-1][1], "lists": res[name]["lists"]}
     f32 = np.array(res["fp32_tiled"]["front"])
     h16 = np.array(res["half2"]["front"])
     # compare fronts at common physical times (interpolate half2 onto fp32 times)
@@ -91,6 +98,10 @@ def main():
     out["surge_front"] = {"max_abs_diff_m": float(np.abs(hi - f32[:, 1]).max()),
                           "max_rel_diff_vs_travel": float(np.abs(hi - f32[:, 1]).max() / max(f32[:, 1].max() - col, 1e-9)),
                           "fp32_samples": [(round(t, 5), round(x, 5)) for t, x in f32[:: max(1, len(f32) // 10)]]}
+    if "tiled_lists" in res:
+        li = np.array(res["tiled_lists"]["front"])
+        lf = np.interp(f32[:, 0], li[:, 0], li[:, 1])
+        out["surge_front_lists_vs_fp32"] = {"max_abs_diff_m": float(np.abs(lf - f32[:, 1]).max())}
     print(json.dumps(out))
 
 
