@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--precision", default="best", choices=["best", "fp32", "tiled", "half2"])
     ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
                     help="N>1: independent replicas (weak scaling) or one dam break cut into x-slabs (strong)")
-    ap.add_argument("--list-interval", type=int, default=0,
+    ap.add_argument("--list-interval", type=int, default=30,
                     help="neighbour lists rebuilt at least every K steps (0: search every step)")
     ap.add_argument("--list-skin", type=float, default=0.0, help="list skin in units of h (0: 0.2)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -444,11 +444,15 @@ def main():
     pairs_all = sum_over_ranks(pg, dev["pairs_per_step"])
     value = pairs_all / (ms * 1e-3)
     steps_per_s = 1e3 / ms
-    plain = None
+    plain = search = None
     if prec != "fp32" and not args.no_plain:
         p = run_device(case, "fp32", max(10, args.steps // 4), args.warmup, local)
         plain = {"value": p["pairs_per_step"] / (p["ms_per_step"] * 1e-3), "steps_per_s": 1e3 / p["ms_per_step"],
                  "ms_per_step": p["ms_per_step"]}
+        if dev.get("lists"):  # the same path with a neighbour search every step
+            q = run_device(case, prec, args.steps, args.warmup, local)
+            search = {"value": q["pairs_per_step"] / (q["ms_per_step"] * 1e-3), "steps_per_s": 1e3 / q["ms_per_step"],
+                      "ms_per_step": q["ms_per_step"], "hydro_ms": q["phase_ms"][2]}
     peak, peak_kind = load_peaks()
     hydro_ms = dev["phase_ms"][2]
     bpp = BYTES_PER_PAIR[prec]
@@ -458,8 +462,8 @@ def main():
     if os.path.exists(tp):
         with open(tp) as f:
             t = json.load(f)
-        if t.get("workload") == args.workload and t.get("precision") == prec:
-            traffic = t.get("bytes_per_launch")
+        key = f"{args.workload}/{prec}" + ("/lists" if dev.get("lists") else "")
+        traffic = t.get(key, {}).get("bytes_per_launch")
     e2e = None
     cpu = None
     if rank == 0 and not args.no_e2e and args.workload != "periodic8m":
@@ -489,6 +493,8 @@ def main():
                                 "dam16k": "3-D dam break dx=0.02 (16,000 fluid + 38,508 wall particles)",
                                 "periodic8m": "periodic jittered lattice 200^3 dx=0.01"}[args.workload],
                    "n_particles": case.n, "precision": prec, "h_over_dx": case.phys.h_over_dx,
+                   "neighbour_search": (f"lists of radius 2h + {dev['lists']['skin_h']:g} h, rebuilt at least every "
+                                        f"{dev['lists']['interval']} steps" if dev.get("lists") else "every step"),
                    "density_mode": case.phys.density_mode,
                    "parallelism": f"slab x{world}" if slab_mode else f"replicas x{world}",
                    "l2": "working set > L2 (126 MB): particle state and records "
@@ -496,11 +502,14 @@ def main():
         "steps_per_s": steps_per_s * 1.0,
         "pairs_per_step": dev["pairs_per_step"],
         "plain_fp32": plain,
+        "search_every_step": search,
         "phase_ms": {"bin_sort_permute": dev["phase_ms"][0], "density": dev["phase_ms"][1],
                      "hydro": dev["phase_ms"][2], "total": dev["phase_ms"][3]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "kernel": "hydro pass",
-                     "model": f"{bpp} B per true pair (j-record) / hydro kernel time", "peak_kind": peak_kind},
+                     "model": f"{bpp} B per true pair (j-record) / hydro kernel time"
+                              + (" (build and list steps averaged)" if dev.get("lists") else ""),
+                     "peak_kind": peak_kind},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "autotune": dev.get("tuning"),
