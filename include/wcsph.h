@@ -202,8 +202,8 @@ typedef struct wcsph_sim_options {
   int32_t list_interval;       /* 0: search neighbours every step (exact order of the reference
                                   loop).  K > 0 (tiled and half2 precisions): neighbour lists of
                                   radius 2h + list_skin h, rebuilt at least every K steps and
-                                  whenever a density pass is due, the instance set changes, or
-                                  the measured drift nears half the skin; the steps between
+                                  whenever the instance set changes or the measured drift nears
+                                  half the skin; the steps between (density passes included)
                                   read the lists and test 0 < r^2 < (2h)^2 on current positions,
                                   so the pairs summed are the same as with a fresh search (the
                                   summation order differs) */

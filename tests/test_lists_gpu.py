@@ -22,8 +22,9 @@ def run(case, prec, steps, **kw):
 
 @pytest.mark.parametrize("prec", [N.PREC_TILED, N.PREC_HALF2], ids=["tiled", "half2"])
 def test_lists_match_per_step_search(prec, native):
-    """60 steps (Shepard steps 1, 31) with lists rebuilt every 8 steps: the
-    same trajectory as the per-step search up to FP32 summation order."""
+    """60 steps (Shepard steps 1, 31, from the lists when they fall on a list
+    step) with lists rebuilt every 8 steps: the same trajectory as the
+    per-step search up to FP32 summation order."""
     case = small_dam(dx=0.04, seed=5)
     ref, ref_st, ref_pairs, _ = run(case, prec, 60)
     got, st, pairs, stats = run(case, prec, 60, list_interval=8)
@@ -45,7 +46,7 @@ def test_list_step_sums_exactly_the_support(native, oracle_lib):
     case = small_dam(dx=0.04, seed=6, vel_sigma=0.5)
     with Solver(case.n, precision=N.PREC_TILED, list_interval=6) as s:
         k = s.add(case)
-        s.step(4)  # step 1 builds (Shepard due), steps 2-4 read the lists
+        s.step(4)  # step 1 builds (the lists are new), steps 2-4 read them
         stats = s.list_stats()
         pairs = s.last_pairs()
         st = s.read(k)
@@ -75,13 +76,21 @@ def test_lists_periodic_faces(native):
     assert rel_l2(got["dens"], ref["dens"]) < 1e-6
 
 
-def test_summation_density_builds_every_step(native):
-    """A density pass reads the cell tables, so with summation density (every
-    step) every step is a build."""
+def test_lists_with_density_passes(native):
+    """Summation density every step (the periodic micro-benchmark's mode) runs
+    its density passes from the lists: list steps happen and the flow matches
+    the per-step search."""
     case = cases.periodic_lattice(n_side=16, dx=0.01, seed=5)
     assert case.phys.density_mode == N.DENSITY_SUMMATION
-    _, st, _, stats = run(case, N.PREC_TILED, 6, list_interval=10)
-    assert stats["builds"] == 6 and stats["list_steps"] == 0 and st["steps"] == 6
+    ref, ref_st, _, _ = run(case, N.PREC_TILED, 30)
+    got, st, _, stats = run(case, N.PREC_TILED, 30, list_interval=10)
+    assert stats["list_steps"] > 0 and st["steps"] == 30
+    L = np.array(case.hi) - np.array(case.lo)
+    d = got["pos"] - ref["pos"]
+    d -= L * np.round(d / L)
+    assert np.linalg.norm(d) / np.linalg.norm(ref["pos"]) < 1e-6
+    assert rel_l2(got["dens"], ref["dens"]) < 1e-6
+    assert rel_l2(got["vel"], ref["vel"]) < 1e-4
 
 
 def test_tiny_skin_builds_every_step(native):

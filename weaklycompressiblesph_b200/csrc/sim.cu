@@ -30,7 +30,6 @@ struct HostInst {
   bool used = false;     // slot holds an instance (active or draining)
   bool slab = false;     // one slab of a decomposed simulation (wcsph_sim_add_slab)
   SlabGeom geom{};
-  long long host_steps = 0;  // steps launched since the instance's step count was known (list schedule)
   bool active = false;   // stepping
   bool drained = false;  // removed, and a pass has been enqueued since (its particles are dead keys)
   wcsph_instance_desc desc{};
@@ -274,7 +273,7 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
 }
 
 // A step that reads the neighbour lists (sim_list.cuh): no sort, no scan.
-static int enqueue_reuse(SimImpl& S, StepArgs a, int* launches, cudaEvent_t* ev = nullptr) {
+static int enqueue_reuse(SimImpl& S, StepArgs a, bool density, int* launches, cudaEvent_t* ev = nullptr) {
   const int n = S.n_host;
   a.list_reuse = 1;
   a.x0 = S.x0;  // read by k_refresh (the displacement since the build)
@@ -286,6 +285,11 @@ static int enqueue_reuse(SimImpl& S, StepArgs a, int* launches, cudaEvent_t* ev 
     k_refresh<<<nblk(n), kBlock, 0, S.s>>>(a);
     L += 2;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));
+    if (density) {  // the kernels return at once for instances with no density pass due
+      k_density_list<<<nblk(n), kBlock, 0, S.s>>>(a);
+      k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
+      L += 2;
+    }
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[2], S.s));
     if (S.opt.precision == WCSPH_PREC_HALF2) {
       if (int rc = launch_hydro_list<true>(a, n, S.s)) return rc;
@@ -456,20 +460,6 @@ static int fill_params(const wcsph_instance_desc& d, HostInst& I, InstParams& P)
 }
 
 // ------------------------------------------------------- neighbour lists
-// Density passes read the cell tables, so a step with one due is a build step.
-// The host keeps each instance's step count (finished instances over-count,
-// which can only add builds).
-static bool density_due(const SimImpl& S) {
-  for (const auto& I : S.inst) {
-    if (!I.active) continue;
-    if (I.desc.density_mode == WCSPH_DENSITY_SUMMATION) return true;
-    if (I.desc.density_mode == WCSPH_DENSITY_SHEPARD && I.desc.shepard_interval > 0 &&
-        I.host_steps % I.desc.shepard_interval == 0)
-      return true;
-  }
-  return false;
-}
-
 // Flags of the latest completed step.  Sticky errors are handled after
 // draining the stream, so that they are seen and cleared exactly once.
 static int read_list_flags(SimImpl& S) {
@@ -494,13 +484,13 @@ static int read_list_flags(SimImpl& S) {
   return 0;
 }
 
-// One step in list mode.  Build when the lists are stale, K steps old, a
-// density pass is due, or the displacement since the build plus 2.5 steps of
+// One step in list mode.  Build when the lists are stale, K steps old, or
+// the displacement since the build plus 2.5 steps of
 // the latest drift would pass half the skin (the decision sees the step
 // before the one in flight).  At most two steps are in flight; a build is
 // waited for, since its lists may have overflowed.
 static int list_step(SimImpl& S, bool graph, cudaEvent_t* ev) {
-  const bool build = !S.lists_valid || S.since_build >= S.opt.list_interval || density_due(S) ||
+  const bool build = !S.lists_valid || S.since_build >= S.opt.list_interval ||
                      S.last_disp + 2.5f * S.last_drift > 0.5f;
   if (graph) {
     WCSPH_CUDA(cudaGraphLaunch(build ? S.gexec : S.gexec_reuse, S.s));
@@ -509,7 +499,7 @@ static int list_step(SimImpl& S, bool graph, cudaEvent_t* ev) {
     WCSPH_CUDA(cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s));
     WCSPH_CUDA(cudaMemsetAsync(S.d_lflags, 0, 2 * sizeof(unsigned), S.s));
     const int rc = build ? enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step, ev, true)
-                         : enqueue_reuse(S, a, &S.kernels_reuse, ev);
+                         : enqueue_reuse(S, a, S.any_density, &S.kernels_reuse, ev);
     if (rc) return rc;
     WCSPH_CUDA(cudaMemcpyAsync(S.h_lflags, S.d_lflags, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, S.s));
   }
@@ -522,8 +512,6 @@ static int list_step(SimImpl& S, bool graph, cudaEvent_t* ev) {
     ++S.since_build;
     ++S.n_reuse;
   }
-  for (auto& I : S.inst)
-    if (I.active) ++I.host_steps;
   const int par = (int)(S.steps_launched & 1);
   WCSPH_CUDA(cudaEventRecord(S.step_ev[par], S.s));
   ++S.steps_launched;
@@ -555,7 +543,7 @@ static int capture_list_graphs(SimImpl& S) {
       rc = WCSPH_E_CUDA;
     if (!rc)
       rc = kind == 0 ? enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step, nullptr, true)
-                     : enqueue_reuse(S, a, &S.kernels_reuse);
+                     : enqueue_reuse(S, a, S.any_density, &S.kernels_reuse);
     if (!rc && cudaMemcpyAsync(S.h_lflags, S.d_lflags, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, S.s) !=
                    cudaSuccess)
       rc = WCSPH_E_CUDA;
@@ -791,7 +779,6 @@ static int append_instance(SimImpl& S, const AppendSpec& A, int32_t* slot) {
     P.HL2 = R * R;
     P.inv_skin = 1.0f / skin;
   }
-  I.host_steps = A.saved ? A.saved->steps : 0;
   I.used = I.active = true;
   HostInst prev = S.inst[k];
   InstParams prev_p = S.h_params[k];

@@ -8,6 +8,7 @@
 //                 so that the lists' image shifts stay valid)
 //   k_refresh     state copied in place (the sorted order of the build is
 //                 kept), EoS j-records refreshed, |x - x0| checked
+//   k_density_list, k_eos   the density pass from the lists, when one is due
 //   k_hydro_list  the tiled kernel's pair phase over each particle's list
 //                 (warp per cell of the build's cell table), every entry
 //                 tested for 0 < r^2 < (2h)^2 on the current positions, then
@@ -62,6 +63,49 @@ __global__ void k_refresh(StepArgs a) {
   const unsigned m = __activemask();
   const unsigned mx = __reduce_max_sync(m, disp_bits);
   if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && mx) atomicMax(&a.list_flags[0], mx);
+}
+
+// Density pass over the lists: k_density_plain's sums (summation, or the
+// Shepard filter of force.h:12-29) over each particle's list entries that are
+// within the support now, in the order the build scanned them (neighbour cells
+// in offset order, slots ascending, as for_each_neighbor visits them).
+// Particles removed since the build keep their density.
+__global__ void k_density_list(StepArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= *a.n_alive) return;
+  const uint32_t f = a.alt.flags[p];
+  const int inst = f & kInstMask;
+  const InstParams& P = a.params[inst];
+  const int kind = density_kind(a, P, a.dyn[inst], a.phase[inst]);
+  if (!kind) return;
+  if (f & kDeadBit) {
+    a.rho_new[p] = a.alt.pos[p].w;
+    return;
+  }
+  const float4 I = a.jA[p];
+  const float rho_i = a.jB[p].w;
+  float sum = 0.5f, one = 0.5f / rho_i;  // self term: w(0) = 1/2
+  const float iH = P.inv_H, H2 = P.H2;
+  const bool shep = kind == 2;
+  const uint32_t* l = a.list + (size_t)p * a.list_max;
+  const int n = min(a.list_cnt[p], a.list_max);
+  for (int k = 0; k < n; ++k) {
+    const uint32_t e = __ldg(&l[k]);
+    const int q = e & kSlotMask;
+    const float4 J = __ldg(&a.jA[q]);
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    if (P.periodic) entry_shift(P, e >> 27, sx, sy, sz);
+    const float dx = __fsub_rn(I.x, __fadd_rn(J.x, sx));
+    const float dy = __fsub_rn(I.y, __fadd_rn(J.y, sy));
+    const float dz = __fsub_rn(I.z, __fadd_rn(J.z, sz));
+    const float r2 = dist2(dx, dy, dz);
+    if (r2 > 0.0f && r2 < H2) {
+      const float w = spline_w(sqrtf(r2) * iH);
+      sum += w;
+      if (shep) one += w / __ldg(&a.jB[q].w);
+    }
+  }
+  a.rho_new[p] = shep ? sum / one : P.mass * P.Kw * sum;
 }
 
 // The pair phase of the tiled kernel over the lists.  The cell table of the
