@@ -286,7 +286,7 @@ static int enqueue_reuse(SimImpl& S, StepArgs a, bool density, int* launches, cu
     L += 2;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));
     if (density) {  // the kernels return at once for instances with no density pass due
-      k_density_list<<<nblk(n), kBlock, 0, S.s>>>(a);
+      if (int rc = launch_density_list<8>(a, S.s)) return rc;
       k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
       L += 2;
     }

@@ -67,45 +67,83 @@ __global__ void k_refresh(StepArgs a) {
 
 // Density pass over the lists: k_density_plain's sums (summation, or the
 // Shepard filter of force.h:12-29) over each particle's list entries that are
-// within the support now, in the order the build scanned them (neighbour cells
-// in offset order, slots ascending, as for_each_neighbor visits them).
-// Particles removed since the build keep their density.
-__global__ void k_density_list(StepArgs a) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= *a.n_alive) return;
-  const uint32_t f = a.alt.flags[p];
-  const int inst = f & kInstMask;
-  const InstParams& P = a.params[inst];
-  const int kind = density_kind(a, P, a.dyn[inst], a.phase[inst]);
-  if (!kind) return;
-  if (f & kDeadBit) {
-    a.rho_new[p] = a.alt.pos[p].w;
-    return;
-  }
-  const float4 I = a.jA[p];
-  const float rho_i = a.jB[p].w;
-  float sum = 0.5f, one = 0.5f / rho_i;  // self term: w(0) = 1/2
-  const float iH = P.inv_H, H2 = P.H2;
-  const bool shep = kind == 2;
-  const uint32_t* l = a.list + (size_t)p * a.list_max;
-  const int n = min(a.list_cnt[p], a.list_max);
-  for (int k = 0; k < n; ++k) {
-    const uint32_t e = __ldg(&l[k]);
-    const int q = e & kSlotMask;
-    const float4 J = __ldg(&a.jA[q]);
-    float sx = 0.f, sy = 0.f, sz = 0.f;
-    if (P.periodic) entry_shift(P, e >> 27, sx, sy, sz);
-    const float dx = __fsub_rn(I.x, __fadd_rn(J.x, sx));
-    const float dy = __fsub_rn(I.y, __fadd_rn(J.y, sy));
-    const float dz = __fsub_rn(I.z, __fadd_rn(J.z, sz));
-    const float r2 = dist2(dx, dy, dz);
-    if (r2 > 0.0f && r2 < H2) {
-      const float w = spline_w(sqrtf(r2) * iH);
-      sum += w;
-      if (shep) one += w / __ldg(&a.jB[q].w);
+// within the support now.  Warp per cell of the build's cell table, four
+// particles at a time, eight lanes per particle walking its list (coalesced
+// list loads), the eight partial sums combined by shuffles.  Particles
+// removed since the build keep their density.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_density_list(StepArgs a) {
+  const unsigned full = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sub = lane & 7, grp = lane >> 3;
+  const int nrun = *a.run_count;
+  const int stride = gridDim.x * WARPS;
+  for (int c = blockIdx.x * WARPS + warp; c < nrun; c += stride) {
+    const int lin = a.run_list[c];
+    const int s = a.cell_start[lin], e = a.cell_end[lin];
+    const int inst = a.alt.flags[s] & kInstMask;
+    const InstParams& P = a.params[inst];
+    const int kind = density_kind(a, P, a.dyn[inst], a.phase[inst]);
+    if (!kind) continue;
+    const bool shep = kind == 2;
+    const float iH = P.inv_H, H2 = P.H2;
+    for (int ib = s; ib < e; ib += 4) {
+      const int p = ib + grp;
+      const bool valid = p < e;
+      const bool dead = valid && (a.alt.flags[p] & kDeadBit);
+      const int n = valid && !dead ? min(a.list_cnt[p], a.list_max) : 0;
+      const float4 I = valid ? __ldg(&a.jA[p]) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const uint32_t* l = a.list + (size_t)(valid ? p : s) * a.list_max;
+      float sum = 0.f, one = 0.f;
+      for (int k = sub; k < n; k += 8) {
+        const uint32_t ent = __ldg(&l[k]);
+        const int q = ent & kSlotMask;
+        const float4 J = __ldg(&a.jA[q]);
+        float sx = 0.f, sy = 0.f, sz = 0.f;
+        if (P.periodic) entry_shift(P, ent >> 27, sx, sy, sz);
+        const float dx = __fsub_rn(I.x, __fadd_rn(J.x, sx));
+        const float dy = __fsub_rn(I.y, __fadd_rn(J.y, sy));
+        const float dz = __fsub_rn(I.z, __fadd_rn(J.z, sz));
+        const float r2 = dist2(dx, dy, dz);
+        if (r2 > 0.0f && r2 < H2) {
+          const float w = spline_w(sqrtf(r2) * iH);
+          sum += w;
+          if (shep) one += w / __ldg(&a.jB[q].w);
+        }
+      }
+#pragma unroll
+      for (int o = 4; o > 0; o >>= 1) {
+        sum += __shfl_xor_sync(full, sum, o);
+        one += __shfl_xor_sync(full, one, o);
+      }
+      if (valid && sub == 0) {
+        if (dead) {
+          a.rho_new[p] = a.alt.pos[p].w;
+        } else {
+          const float rho_i = __ldg(&a.jB[p].w);
+          const float t = 0.5f + sum;  // self term: w(0) = 1/2
+          a.rho_new[p] = shep ? t / (0.5f / rho_i + one) : P.mass * P.Kw * t;
+        }
+      }
     }
   }
-  a.rho_new[p] = shep ? sum / one : P.mass * P.Kw * sum;
+}
+
+template <int WARPS>
+inline int launch_density_list(const StepArgs& a, cudaStream_t s) {
+  static int blocks[16] = {0};
+  int dev = 0;
+  WCSPH_CUDA(cudaGetDevice(&dev));
+  auto kern = k_density_list<WARPS>;
+  if (!blocks[dev & 15]) {
+    int per_sm = 0, sms = 0;
+    WCSPH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, 0));
+    WCSPH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    blocks[dev & 15] = std::max(1, per_sm) * sms;
+  }
+  kern<<<blocks[dev & 15], WARPS * 32, 0, s>>>(a);
+  WCSPH_CUDA(cudaGetLastError());
+  return 0;
 }
 
 // The pair phase of the tiled kernel over the lists.  The cell table of the
