@@ -26,7 +26,6 @@ namespace wcsph {
 
 constexpr int kListWarps = 4;
 constexpr int kListMaxEntries = 256;  // entries per list (the solver's list_max)
-constexpr int kListPerLane = kListMaxEntries / 32;
 
 // Copy main -> alt in place, refresh the j-records, check the displacement.
 __global__ void k_refresh(StepArgs a) {
@@ -150,16 +149,24 @@ inline int launch_density_list(const StepArgs& a, cudaStream_t s) {
 // last build is still valid (list steps do not re-sort), so the work is laid
 // out as in k_hydro_tiled: warp per non-empty cell, batches of 32 particles,
 // pairs of i at a time; each pair's two lists are copied into shared-memory
-// queues with coalesced loads, the shared pair routine tests the support per
-// entry, and lane l finishes particle batch + l with the shared epilogue.
+// queues with asynchronous copies (cp.async) one pair ahead, into the other
+// of two buffers; the shared pair routine tests the support per entry, and
+// lane l finishes particle batch + l with the shared epilogue.  Five blocks of
+// four warps per SM (94 registers).
+// Asynchronous 4-byte copy global -> shared (cp.async, L1-allocating).
+__device__ __forceinline__ void cp_async4(uint32_t* dst_smem, const uint32_t* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 template <bool H16, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_hydro_list(StepArgs a) {
-  __shared__ uint32_t s_q[WARPS][2][kListMaxEntries];
+__global__ void __launch_bounds__(WARPS * 32, 5) k_hydro_list(StepArgs a) {
+  __shared__ uint32_t s_q[WARPS][2][2][kListMaxEntries];  // [buffer][i of the pair][entry]
   __shared__ float s_res[WARPS][32][6];
   const unsigned full = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t* qa = s_q[warp][0];
-  uint32_t* qb = s_q[warp][1];
   float(*res)[6] = s_res[warp];
   const int L = a.list_max;
   const int nrun = *a.run_count;
@@ -184,37 +191,29 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_list(StepArgs a) {
       // list lengths of the batch in one load (particles removed since the
       // build keep their state and sum nothing)
       const int my_n = lane < nbat && !(a.alt.flags[ib + lane] & kDeadBit) ? min(a.list_cnt[ib + lane], L) : 0;
-      // entries of the next pair are loaded into registers while the current
-      // pair is summed
-      uint32_t ra[kListPerLane], rb[kListPerLane];
-      auto fetch = [&](int ii) {
+      // the next pair's lists are copied asynchronously into the other
+      // buffer while the current pair is summed
+      auto fetch = [&](int ii, int buf) {
         const int na = __shfl_sync(full, my_n, ii), nb = __shfl_sync(full, my_n, min(ii + 1, 31));
         const bool has_b = ii + 1 < nbat;
         const uint32_t* la = a.list + (size_t)(ib + ii) * L;
         const uint32_t* lb = a.list + (size_t)(ib + (has_b ? ii + 1 : ii)) * L;
-#pragma unroll
-        for (int j = 0; j < kListPerLane; ++j) {
-          const int k = lane + 32 * j;
-          ra[j] = k < na ? __ldg(&la[k]) : 0u;
-          rb[j] = has_b && k < nb ? __ldg(&lb[k]) : 0u;
-        }
+        for (int k = lane; k < na; k += 32) cp_async4(&s_q[warp][buf][0][k], &la[k]);
+        if (has_b)
+          for (int k = lane; k < nb; k += 32) cp_async4(&s_q[warp][buf][1][k], &lb[k]);
+        cp_async_commit();
       };
-      fetch(0);
-      for (int ii = 0; ii < nbat; ii += 2) {
+      fetch(0, 0);
+      for (int ii = 0, buf = 0; ii < nbat; ii += 2, buf ^= 1) {
         const int ia = ib + ii;
         const bool has_b = ii + 1 < nbat;
         const int ibb = has_b ? ia + 1 : ia;
         const int na = __shfl_sync(full, my_n, ii), nb = has_b ? __shfl_sync(full, my_n, ii + 1) : 0;
-#pragma unroll
-        for (int j = 0; j < kListPerLane; ++j) {
-          const int k = lane + 32 * j;
-          if (k < na) qa[k] = ra[j];
-          if (k < nb) qb[k] = rb[j];
-        }
+        cp_async_wait_all();
         __syncwarp();
-        if (ii + 2 < nbat) fetch(ii + 2);
-        hydro_queues2<H16, true>(a, P, ia, ibb, has_b, __ldg(&a.jA[ia]), __ldg(&a.jA[ibb]), qa, na, qb, nb,
-                                 &res[ii], lane);
+        if (ii + 2 < nbat) fetch(ii + 2, buf ^ 1);
+        hydro_queues2<H16, true>(a, P, ia, ibb, has_b, __ldg(&a.jA[ia]), __ldg(&a.jA[ibb]), s_q[warp][buf][0], na,
+                                 s_q[warp][buf][1], nb, &res[ii], lane);
         __syncwarp();
       }
       __syncwarp();
