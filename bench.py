@@ -367,13 +367,15 @@ def measure_ensemble(device, steps=None):
     from weaklycompressiblesph_b200 import cases, ensemble
     steps = steps or ARGS.ensemble_steps
     ens = cases.ensemble_cases(count=64, seed=2024)
-    b = ensemble.run_batched(ens, steps=steps, warmup=3, device=device)
+    b = ensemble.run_batched(ens, steps=steps, warmup=3, device=device, list_interval=ARGS.list_interval)
     s = ensemble.run_serial(ens, steps=steps, warmup=3, precision="fp32", device=device)
     return {"instances": len(ens), "particles": b["particles"], "steps": steps,
             "batched_particle_steps_per_s": b["particle_steps_per_s"],
             "serial_plain_particle_steps_per_s": s["particle_steps_per_s"],
             "speedup_vs_serial_plain": b["particle_steps_per_s"] / s["particle_steps_per_s"],
-            "sample": f"{steps} timed steps per instance (config: 2000)"}
+            "sample": f"{steps} timed steps per instance (config: 2000)",
+            "neighbour_search": (f"lists, rebuilt at least every {ARGS.list_interval} steps" if ARGS.list_interval
+                                 else "every step") + "; serial baseline: plain FP32, search every step"}
 
 
 def measure_serving(device):
@@ -387,7 +389,8 @@ def measure_serving(device):
     from weaklycompressiblesph_b200.serving import Server, run_alone
     reqs = cases.serving_requests(count=16, rate=20.0, seed=7, n_min=2e4, n_max=2e5, t_end=0.1)
     total = sum(c.n for _, c in reqs)
-    with Server(budget_bytes=150e9, max_particles=total + 1024, device=device, read_results=False) as srv:
+    with Server(budget_bytes=150e9, max_particles=total + 1024, device=device, read_results=False,
+                list_interval=ARGS.list_interval) as srv:
         out = srv.run(reqs)
     el = 0.0
     ps = 0
@@ -399,6 +402,8 @@ def measure_serving(device):
             "wall_s": out["wall_s"], "particle_steps_per_s": out["particle_steps_per_s"],
             "serial_plain_particle_steps_per_s": ps / el,
             "speedup_vs_serial_plain": out["particle_steps_per_s"] / (ps / el),
+            "neighbour_search": (f"lists, rebuilt at least every {ARGS.list_interval} steps" if ARGS.list_interval
+                                 else "every step") + "; serial baseline: plain FP32, search every step",
             "sample": "16 requests, counts log-uniform [2e4, 2e5], t_end 0.1 s, Poisson 20/s, budget 150 GB "
                       "(config: counts to 2e6, t_end 1.0 s)"}
 

@@ -22,11 +22,13 @@ def _sync_time(solver, fn):
     return time.perf_counter() - t0
 
 
-def run_batched(cases, steps, precision="tiled", warmup=3, device=0):
+def run_batched(cases, steps, precision="tiled", warmup=3, device=0, list_interval=0):
     """Step all cases together; returns dict with wall seconds for `steps`
-    steps, particle-steps/s and per-instance status."""
+    steps, particle-steps/s and per-instance status.  list_interval > 0 uses
+    neighbour lists (see Solver)."""
     total = sum(c.n for c in cases)
-    with Solver(total + 1024, precision=PRECISIONS[precision], max_instances=len(cases) + 1, device=device) as s:
+    with Solver(total + 1024, precision=PRECISIONS[precision], max_instances=len(cases) + 1, device=device,
+                list_interval=list_interval) as s:
         slots = [s.add(c) for c in cases]
         s.step(warmup)
         el = _sync_time(s, lambda: s.step(steps))

@@ -28,23 +28,26 @@ from .sim import Solver
 BYTES_PER_PARTICLE_ESTIMATE = None
 
 
-def particle_bytes():
+def particle_bytes(list_interval=0):
     """Device bytes per particle of a solver (from the library's own sizing)."""
-    a = Solver.device_bytes(1 << 20, max_cells=1, max_instances=1)
-    b = Solver.device_bytes(2 << 20, max_cells=1, max_instances=1)
+    a = Solver.device_bytes(1 << 20, max_cells=1, max_instances=1, list_interval=list_interval)
+    b = Solver.device_bytes(2 << 20, max_cells=1, max_instances=1, list_interval=list_interval)
     return (b - a) / float(1 << 20)
 
 
 class Server:
     def __init__(self, budget_bytes=150e9, precision=N.PREC_TILED, max_instances=256, chunk_steps=25, device=0,
-                 max_particles=None, read_results=True):
-        per = particle_bytes()
+                 max_particles=None, read_results=True, list_interval=0):
+        """list_interval > 0 steps the requests with neighbour lists (see
+        Solver); results then depend on the mix, so a request's result is no
+        longer bit-identical to running it alone."""
+        per = particle_bytes(list_interval)
         cap = int(budget_bytes / (per + 8.0))  # + 2 cells per particle of table headroom
         if max_particles is not None:
             cap = min(cap, int(max_particles))
         self.capacity = cap
         self.solver = Solver(cap, precision=precision, max_cells=2 * cap, max_instances=max_instances,
-                             device=device)
+                             device=device, list_interval=list_interval)
         self.chunk_steps = chunk_steps
         self.max_instances = max_instances
         self.read_results = read_results

@@ -46,9 +46,9 @@ class Solver:
         self.slots = {}
 
     @staticmethod
-    def device_bytes(max_particles, max_cells=None, max_instances=64):
+    def device_bytes(max_particles, max_cells=None, max_instances=64, list_interval=0):
         o = N.SimOptions(0, 0, int(max_particles), int(max_cells or max(1 << 20, 2 * max_particles)),
-                         int(max_instances), 1, 0, 0)
+                         int(max_instances), 1, 0, int(list_interval))
         return int(N.lib().wcsph_sim_device_bytes(C.byref(o)))
 
     def close(self):
