@@ -30,7 +30,7 @@ def test_lists_match_per_step_search(prec, native):
     got, st, pairs, stats = run(case, prec, 60, list_interval=8)
     assert stats["list_steps"] > 0 and stats["overflows"] == 0
     assert stats["builds"] + stats["list_steps"] == 60
-    assert stats["builds"] >= 60 // 8 and stats["longest"] <= 256
+    assert stats["builds"] >= 60 // 8 and stats["longest"] <= 192
     assert st["steps"] == ref_st["steps"] == 60
     assert abs(st["time"] - ref_st["time"]) <= 1e-5 * ref_st["time"]
     assert rel_l2(got["pos"], ref["pos"]) < 1e-6

@@ -25,7 +25,7 @@
 namespace wcsph {
 
 constexpr int kListWarps = 4;
-constexpr int kListMaxEntries = 256;  // entries per list (the solver's list_max)
+constexpr int kListMaxEntries = 192;  // entries per list (the solver's list_max; the dam break needs up to ~120)
 
 // Copy main -> alt in place, refresh the j-records, check the displacement.
 __global__ void k_refresh(StepArgs a) {
