@@ -125,3 +125,16 @@ def test_list_options_rejected(native):
         Solver(1000, precision=N.PREC_FP32, list_interval=4)
     with pytest.raises(N.WcsphError):
         Solver(1000, precision=N.PREC_TILED, list_interval=-1)
+
+
+def test_list_overflow_falls_back_to_search(native):
+    """h = 2.5 dx gives about 500 neighbours, more than a list holds: every
+    build overflows, the next step builds again, and the results are those of
+    the per-step search."""
+    case = small_dam(dx=0.05, seed=8, phys=cases.Physics(h_over_dx=2.5))
+    ref, ref_st, _, _ = run(case, N.PREC_TILED, 6)
+    got, st, _, stats = run(case, N.PREC_TILED, 6, list_interval=10)
+    assert stats["overflows"] >= 1 and stats["list_steps"] == 0 and stats["builds"] == 6
+    assert st["steps"] == ref_st["steps"] == 6
+    assert rel_l2(got["pos"], ref["pos"]) < 1e-6
+    assert rel_l2(got["vel"], ref["vel"]) < 1e-4
