@@ -294,7 +294,10 @@ int wcsph_sim_remove_instance(wcsph_sim* sim, int32_t slot);
 int wcsph_sim_step(wcsph_sim* sim, int32_t nsteps);
 int wcsph_sim_synchronize(wcsph_sim* sim);
 
-/* Instance status: physical time, steps taken, live particle count, finished flag. */
+/* Instance status: physical time, steps taken, live particle count, finished
+ * flag.  With neighbour lists the live count is that of the latest list build
+ * (particles removed on the steps between leave the sums and the reads at
+ * once, the count at the next build). */
 int wcsph_sim_instance_status(wcsph_sim* sim, int32_t slot, double* time, int64_t* steps, int32_t* n_alive,
                               int32_t* finished);
 /* Copy an instance's state to host arrays in its ORIGINAL particle order
