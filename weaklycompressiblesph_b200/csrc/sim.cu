@@ -472,6 +472,11 @@ static int read_list_flags(SimImpl& S) {
     WCSPH_CUDA(cudaStreamSynchronize(S.s));
     S.lists_valid = false;
     if (e & 2u) ++S.n_overflow;
+    if (e & kListErrCopy) {
+      set_error("wcsph_sim_step: a bulk copy of a neighbour list did not complete; the step's pair sums are "
+                "incomplete");
+      return WCSPH_E_CUDA;
+    }
     if (e & 1u) {
       set_error("wcsph_sim_step: a particle moved more than half the neighbour-list skin between list builds; "
                 "the step's pair sums may be incomplete (raise list_skin or lower list_interval)");

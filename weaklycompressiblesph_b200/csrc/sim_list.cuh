@@ -148,22 +148,53 @@ inline int launch_density_list(const StepArgs& a, cudaStream_t s) {
 // The pair phase of the tiled kernel over the lists.  The cell table of the
 // last build is still valid (list steps do not re-sort), so the work is laid
 // out as in k_hydro_tiled: warp per non-empty cell, batches of 32 particles,
-// pairs of i at a time; each pair's two lists are copied into shared-memory
-// queues with asynchronous copies (cp.async) one pair ahead, into the other
-// of two buffers; the shared pair routine tests the support per entry, and
-// lane l finishes particle batch + l with the shared epilogue.  Five blocks of
-// four warps per SM (94 registers).
-// Asynchronous 4-byte copy global -> shared (cp.async, L1-allocating).
-__device__ __forceinline__ void cp_async4(uint32_t* dst_smem, const uint32_t* src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+// pairs of i at a time; each pair's two list rows are brought into
+// shared-memory queues by TMA bulk copies one pair ahead, into the other of
+// two buffers, each with its own mbarrier; the shared pair routine tests the
+// support per entry, and lane l finishes particle batch + l with the shared
+// epilogue.
+// Bulk copies global -> shared (TMA, cp.async.bulk, no multicast) completing
+// on a shared-memory mbarrier, and the barrier operations they need.
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+// Order this thread's earlier generic accesses of shared memory before later
+// async-proxy (bulk copy) writes to it.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  unsigned long long state;
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;\n"
+               : "=l"(state)
+               : "r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+  (void)state;
+}
+// bytes: a multiple of 16; dst and src 16-byte aligned.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+constexpr unsigned kListErrCopy = 4u;     // list_flags[2]: a bulk copy of a list did not complete
+constexpr int kMbarSpinLimit = 1 << 22;   // try_wait rounds before giving up on a copy
 
 template <bool H16, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 5) k_hydro_list(StepArgs a) {
-  __shared__ uint32_t s_q[WARPS][2][2][kListMaxEntries];  // [buffer][i of the pair][entry]
+  // [warp][buffer][i of the pair][entry]; a list row is 768 bytes, 16-byte aligned
+  __shared__ __align__(16) uint32_t s_q[WARPS][2][2][kListMaxEntries];
+  __shared__ __align__(8) unsigned long long s_bar[WARPS][2];  // one mbarrier per buffer
   __shared__ float s_res[WARPS][32][6];
   const unsigned full = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -171,6 +202,14 @@ __global__ void __launch_bounds__(WARPS * 32, 5) k_hydro_list(StepArgs a) {
   const int L = a.list_max;
   const int nrun = *a.run_count;
   unsigned long long pairs = 0;
+  if (lane == 0) {
+    mbar_init(&s_bar[warp][0], 1);
+    mbar_init(&s_bar[warp][1], 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  unsigned parity = 0u;  // bit b: parity of buffer b's next completion
+  bool copy_failed = false;
   const int stride = gridDim.x * WARPS;
   for (int c = blockIdx.x * WARPS + warp; c < nrun; c += stride) {
     const int lin = a.run_list[c];
@@ -191,29 +230,41 @@ __global__ void __launch_bounds__(WARPS * 32, 5) k_hydro_list(StepArgs a) {
       // list lengths of the batch in one load (particles removed since the
       // build keep their state and sum nothing)
       const int my_n = lane < nbat && !(a.alt.flags[ib + lane] & kDeadBit) ? min(a.list_cnt[ib + lane], L) : 0;
-      // the next pair's lists are copied asynchronously into the other
-      // buffer while the current pair is summed
+      // lane 0 copies the next pair's two list rows into the other buffer
+      // (bulk copies rounded up to 16 bytes, within the 768-byte rows) while
+      // the current pair is summed
       auto fetch = [&](int ii, int buf) {
         const int na = __shfl_sync(full, my_n, ii), nb = __shfl_sync(full, my_n, min(ii + 1, 31));
-        const bool has_b = ii + 1 < nbat;
-        const uint32_t* la = a.list + (size_t)(ib + ii) * L;
-        const uint32_t* lb = a.list + (size_t)(ib + (has_b ? ii + 1 : ii)) * L;
-        for (int k = lane; k < na; k += 32) cp_async4(&s_q[warp][buf][0][k], &la[k]);
-        if (has_b)
-          for (int k = lane; k < nb; k += 32) cp_async4(&s_q[warp][buf][1][k], &lb[k]);
-        cp_async_commit();
+        if (lane == 0 && !copy_failed) {
+          const bool has_b = ii + 1 < nbat;
+          const unsigned ba = (unsigned)(na * 4 + 15) & ~15u, bb = has_b ? (unsigned)(nb * 4 + 15) & ~15u : 0u;
+          fence_proxy_async();  // the buffer's previous reads come first
+          mbar_arrive_expect_tx(&s_bar[warp][buf], ba + bb);
+          if (ba) bulk_g2s(&s_q[warp][buf][0][0], a.list + (size_t)(ib + ii) * L, ba, &s_bar[warp][buf]);
+          if (bb) bulk_g2s(&s_q[warp][buf][1][0], a.list + (size_t)(ib + ii + 1) * L, bb, &s_bar[warp][buf]);
+        }
       };
       fetch(0, 0);
       for (int ii = 0, buf = 0; ii < nbat; ii += 2, buf ^= 1) {
         const int ia = ib + ii;
         const bool has_b = ii + 1 < nbat;
         const int ibb = has_b ? ia + 1 : ia;
-        const int na = __shfl_sync(full, my_n, ii), nb = has_b ? __shfl_sync(full, my_n, ii + 1) : 0;
-        cp_async_wait_all();
+        int na = __shfl_sync(full, my_n, ii), nb = has_b ? __shfl_sync(full, my_n, ii + 1) : 0;
+        // every lane waits for the copies, boundedly: after a copy that never
+        // lands the warp issues and waits for no more copies, sums nothing for
+        // its remaining particles and reports the failure (kListErrCopy)
+        if (!copy_failed) {
+          bool ok = false;
+          for (int t = 0; t < kMbarSpinLimit && !ok; ++t) ok = mbar_try_wait(&s_bar[warp][buf], (parity >> buf) & 1u);
+          parity ^= 1u << buf;
+          copy_failed = !__all_sync(full, ok);
+        }
+        if (copy_failed) na = nb = 0;
         __syncwarp();
         if (ii + 2 < nbat) fetch(ii + 2, buf ^ 1);
         hydro_queues2<H16, true>(a, P, ia, ibb, has_b, __ldg(&a.jA[ia]), __ldg(&a.jA[ibb]), s_q[warp][buf][0], na,
                                  s_q[warp][buf][1], nb, &res[ii], lane);
+        fence_proxy_async();  // this buffer is refilled by a bulk copy two pairs on
         __syncwarp();
       }
       __syncwarp();
@@ -232,6 +283,7 @@ __global__ void __launch_bounds__(WARPS * 32, 5) k_hydro_list(StepArgs a) {
     }
     dt_min(a.dyn, inst, dt_cand, dt_valid);
   }
+  if (copy_failed && lane == 0) atomicOr(&a.list_flags[2], kListErrCopy);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(full, pairs, o);
   if (lane == 0 && pairs) atomicAdd(a.pair_count, pairs);
