@@ -53,7 +53,7 @@ struct SimImpl {
   int* d_phase = nullptr;
   int* d_n_alive = nullptr;
   int* run_list = nullptr;
-  int* d_counters = nullptr;  // [0] run_count
+  int* d_counters = nullptr;  // [0] run_count, [4] density pass in this launch (slab pack: [0..3] between passes)
   unsigned long long* d_pairs = nullptr;
   double* d_cons = nullptr;
   float4* diag_acc = nullptr;
@@ -188,6 +188,7 @@ static StepArgs make_args(SimImpl& S) {
   a.pair_count = S.d_pairs;
   a.run_list = S.run_list;
   a.run_count = S.d_counters;
+  a.dens_any = S.d_counters + 4;
   a.diag_acc = S.diag_acc;
   a.diag_dt = S.diag_dt;
   a.diag_nbr = S.diag_nbr;
@@ -219,6 +220,7 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
   if (build_lists) a.x0 = S.x0;
   else S.lists_valid = false;  // any other pass re-sorts or changes what the lists refer to
   if (ev) WCSPH_CUDA(cudaEventRecord(ev[0], S.s));
+  WCSPH_CUDA(cudaMemsetAsync(S.d_counters + 4, 0, sizeof(int), S.s));
   k_step_begin<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
   ++L;
   if (n > 0) {
@@ -278,6 +280,7 @@ static int enqueue_reuse(SimImpl& S, StepArgs a, bool density, int* launches, cu
   a.list_reuse = 1;
   a.x0 = S.x0;  // read by k_refresh (the displacement since the build)
   if (ev) WCSPH_CUDA(cudaEventRecord(ev[0], S.s));
+  WCSPH_CUDA(cudaMemsetAsync(S.d_counters + 4, 0, sizeof(int), S.s));
   k_step_begin<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
   int L = 1;
   if (n > 0) {
@@ -636,7 +639,7 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
   rc |= alloc(S, (void**)&S.d_phase, (size_t)opt->max_instances * sizeof(int));
   rc |= alloc(S, (void**)&S.d_n_alive, sizeof(int));
   rc |= alloc(S, (void**)&S.run_list, N * sizeof(int));
-  rc |= alloc(S, (void**)&S.d_counters, 4 * sizeof(int));
+  rc |= alloc(S, (void**)&S.d_counters, 8 * sizeof(int));
   rc |= alloc(S, (void**)&S.d_pairs, sizeof(unsigned long long));
   rc |= alloc(S, (void**)&S.d_cons, 8 * sizeof(double));
   S.cub_bytes = cub_sort_bytes((long long)N);

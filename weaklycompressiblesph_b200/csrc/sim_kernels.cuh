@@ -46,6 +46,7 @@ struct StepArgs {
   unsigned* list_flags;   // [0] max |x - x0| / skin, [1] max step drift / skin (float bits),
                           // [2] sticky errors (1 skin exceeded, 2 overflow), [3] largest list
   int list_reuse;         // this step reads the lists: periodic wrapping waits for the next build
+  int* dens_any;          // set by k_step_begin when any instance has a density pass in this launch
   int probe_density;      // density pass of a probe launch: 0 none, 1 summation, 2 Shepard
   // diagnostics (probe phase)
   float4* diag_acc;
@@ -55,6 +56,22 @@ struct StepArgs {
 };
 
 __device__ __forceinline__ float bits_f(unsigned b) { return __uint_as_float(b); }
+
+// Density pass of an instance in the current launch: 0 none, 1 summation, 2 Shepard.
+__device__ __forceinline__ int density_kind(const StepArgs& a, const InstParams& P, const InstDyn& d, int ph) {
+  if (ph == PH_IDLE || !P.active) return 0;
+  if (ph == PH_PROBE) return a.probe_density;
+  if (ph == PH_INIT) {
+    if (a.init_filter) return P.density_mode == WCSPH_DENSITY_SHEPARD ? 2 : 0;
+    return P.density_mode == WCSPH_DENSITY_SUMMATION ? 1 : 0;
+  }
+  if (d.dt_cur <= 0.0f) return 0;  // finished: the state no longer changes
+  if (P.density_mode == WCSPH_DENSITY_SUMMATION) return 1;
+  if (P.density_mode == WCSPH_DENSITY_SHEPARD && P.shepard_interval > 0 &&
+      ((d.steps - 1) % P.shepard_interval) == 0)  // main.cpp:105, step index before increment
+    return 2;
+  return 0;
+}
 
 // ------------------------------------------------------------ step begin
 // One thread per instance: rotate dt, advance time, mark finished.
@@ -83,6 +100,7 @@ __global__ void k_step_begin(StepArgs a) {
     } else {
       d.dt_cur = 0.0f;
     }
+    if (a.dens_any && (ph == PH_INIT || ph == PH_PROBE || density_kind(a, P, d, ph))) atomicOr(a.dens_any, 1);
   }
   if (k == 0 && !a.list_reuse) *a.n_alive = a.n_host;
 }
@@ -203,22 +221,6 @@ __global__ void k_permute(StepArgs a) {
   a.jC[p] = snds;
 }
 
-// Density pass of an instance in the current launch: 0 none, 1 summation, 2 Shepard.
-__device__ __forceinline__ int density_kind(const StepArgs& a, const InstParams& P, const InstDyn& d, int ph) {
-  if (ph == PH_IDLE || !P.active) return 0;
-  if (ph == PH_PROBE) return a.probe_density;
-  if (ph == PH_INIT) {
-    if (a.init_filter) return P.density_mode == WCSPH_DENSITY_SHEPARD ? 2 : 0;
-    return P.density_mode == WCSPH_DENSITY_SUMMATION ? 1 : 0;
-  }
-  if (d.dt_cur <= 0.0f) return 0;  // finished: the state no longer changes
-  if (P.density_mode == WCSPH_DENSITY_SUMMATION) return 1;
-  if (P.density_mode == WCSPH_DENSITY_SHEPARD && P.shepard_interval > 0 &&
-      ((d.steps - 1) % P.shepard_interval) == 0)  // main.cpp:105, step index before increment
-    return 2;
-  return 0;
-}
-
 // Does the hydro pass run for an instance in the current launch?
 __device__ __forceinline__ bool wants_force(const InstParams& P, const InstDyn& d, int ph) {
   if (!P.active) return false;
@@ -266,6 +268,7 @@ __device__ __forceinline__ void for_each_neighbor(const StepArgs& a, const InstP
 // Summation rho_i = m sum_j W_ij (self included) or the Shepard filter of
 // force.h:12-29, sum m W / sum (m/rho_j) W, from the pre-filter densities.
 __global__ void k_density_plain(StepArgs a) {
+  if (a.dens_any && !*a.dens_any) return;  // no density pass in this launch
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= *a.n_alive) return;
   const int inst = a.alt.flags[p] & kInstMask;
@@ -287,6 +290,7 @@ __global__ void k_density_plain(StepArgs a) {
 
 // Refresh the j-records of particles whose density was just recomputed.
 __global__ void k_eos(StepArgs a) {
+  if (a.dens_any && !*a.dens_any) return;  // no density pass in this launch
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= *a.n_alive) return;
   const int inst = a.alt.flags[p] & kInstMask;

@@ -72,6 +72,7 @@ __global__ void k_refresh(StepArgs a) {
 // removed since the build keep their density.
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_density_list(StepArgs a) {
+  if (a.dens_any && !*a.dens_any) return;  // no density pass in this launch
   const unsigned full = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sub = lane & 7, grp = lane >> 3;
