@@ -278,15 +278,14 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
 static int enqueue_reuse(SimImpl& S, StepArgs a, bool density, int* launches, cudaEvent_t* ev = nullptr) {
   const int n = S.n_host;
   a.list_reuse = 1;
-  a.x0 = S.x0;  // read by k_refresh (the displacement since the build)
+  a.x0 = S.x0;  // read by k_kick_refresh (the displacement since the build)
   if (ev) WCSPH_CUDA(cudaEventRecord(ev[0], S.s));
   WCSPH_CUDA(cudaMemsetAsync(S.d_counters + 4, 0, sizeof(int), S.s));
   k_step_begin<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
   int L = 1;
   if (n > 0) {
-    k_kick_bin<<<nblk(n), kBlock, 0, S.s>>>(a);
-    k_refresh<<<nblk(n), kBlock, 0, S.s>>>(a);
-    L += 2;
+    k_kick_refresh<<<nblk(n), kBlock, 0, S.s>>>(a);
+    ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));
     if (density) {  // the kernels return at once for instances with no density pass due
       if (int rc = launch_density_list<8>(a, S.s)) return rc;

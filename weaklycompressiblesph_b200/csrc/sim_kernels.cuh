@@ -108,6 +108,56 @@ __global__ void k_step_begin(StepArgs a) {
 // ------------------------------------------------------- kick + binning
 // KDK first half (class.h:146-159 as main.cpp:98-103 runs it), periodic wrap,
 // escapee removal (Dam2.h:117-122), then the Morton cell key of each particle.
+// KDK first half of one live particle p of a stepping instance
+// (class.h:146-159 as main.cpp:98-103 runs it), periodic wrap (not on list
+// steps), escapee removal (Dam2.h:117-122).  Returns true when the state
+// changed; dead is set when the particle left the kill box; drift_bits
+// receives this step's drift in units of the neighbour-list skin.
+__device__ __forceinline__ bool kick_particle(const StepArgs& a, const InstParams& P, int inst, int p, uint32_t f,
+                                              float4& x, float4& v, float4& vh, bool& dead, unsigned& drift_bits) {
+  const int ph = a.phase[inst];
+  const float dt = a.dyn[inst].dt_cur;
+  if (!(ph == PH_STEP && dt > 0.0f)) return false;
+  const float4 acc = a.main.acc[p];
+  x.w += -x.w * dt * acc.w;  // continuity, FREEZE included (class.h:151)
+  if (!(f & kFreezeBit)) {
+    const float hdt = 0.5f * dt;
+    vh = make_float4(v.x + hdt * acc.x, v.y + hdt * acc.y, v.z + hdt * acc.z, 0.f);
+    x.x += dt * vh.x;
+    x.y += dt * vh.y;
+    x.z += dt * vh.z;
+    if (P.slab_margin2 > 0.0f && dt * dt * (vh.x * vh.x + vh.y * vh.y + vh.z * vh.z) > P.slab_margin2)
+      atomicOr(&a.dyn[inst].errors, kErrDrift);  // the ghost layer no longer covers this drift
+    if (a.list_flags && P.inv_skin > 0.0f)
+      drift_bits = __float_as_uint(dt * sqrtf(vh.x * vh.x + vh.y * vh.y + vh.z * vh.z) * P.inv_skin);
+    v = make_float4(v.x + dt * acc.x, v.y + dt * acc.y, v.z + dt * acc.z, 0.f);
+    if (P.periodic && !a.list_reuse) {  // between list builds positions run on continuously
+      float* c = &x.x;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float hi = P.lo[k] + P.L[k];
+        if (c[k] >= hi) c[k] = __fsub_rn(c[k], P.L[k]);
+        else if (c[k] < P.lo[k]) c[k] = __fadd_rn(c[k], P.L[k]);
+      }
+    }
+    if (P.kill_on) {
+      const float* c = &x.x;
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        if (P.kill_lo[k] < P.kill_hi[k] && (c[k] < P.kill_lo[k] || c[k] > P.kill_hi[k])) dead = true;
+    }
+  }
+  return true;
+}
+
+// Warp-aggregated maximum of a ratio (float bits) into a list flag word.
+__device__ __forceinline__ void list_flag_max(unsigned* word, unsigned bits) {
+  const unsigned m = __activemask();
+  const unsigned mx = __reduce_max_sync(m, bits);
+  if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && mx) atomicMax(word, mx);
+}
+
+// The kick, then the Morton cell key of each particle.
 __global__ void k_kick_bin(StepArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.n_host) return;
@@ -118,43 +168,10 @@ __global__ void k_kick_bin(StepArgs a) {
   float4 x = a.main.pos[p];
   float4 v = a.main.vel[p];
   float4 vh = v;
-  unsigned drift_bits = 0u;  // this step's drift / skin (float bits; positive floats order like their bits)
-  if (!dead) {
-    const int ph = a.phase[inst];
-    const float dt = a.dyn[inst].dt_cur;
-    if (ph == PH_STEP && dt > 0.0f) {
-      const float4 acc = a.main.acc[p];
-      x.w += -x.w * dt * acc.w;  // continuity, FREEZE included (class.h:151)
-      if (!(f & kFreezeBit)) {
-        const float hdt = 0.5f * dt;
-        vh = make_float4(v.x + hdt * acc.x, v.y + hdt * acc.y, v.z + hdt * acc.z, 0.f);
-        x.x += dt * vh.x;
-        x.y += dt * vh.y;
-        x.z += dt * vh.z;
-        if (P.slab_margin2 > 0.0f && dt * dt * (vh.x * vh.x + vh.y * vh.y + vh.z * vh.z) > P.slab_margin2)
-          atomicOr(&a.dyn[inst].errors, kErrDrift);  // the ghost layer no longer covers this drift
-        if (a.list_flags && P.inv_skin > 0.0f)
-          drift_bits = __float_as_uint(dt * sqrtf(vh.x * vh.x + vh.y * vh.y + vh.z * vh.z) * P.inv_skin);
-        v = make_float4(v.x + dt * acc.x, v.y + dt * acc.y, v.z + dt * acc.z, 0.f);
-        if (P.periodic && !a.list_reuse) {  // between list builds positions run on continuously
-          float* c = &x.x;
-#pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            const float hi = P.lo[k] + P.L[k];
-            if (c[k] >= hi) c[k] = __fsub_rn(c[k], P.L[k]);
-            else if (c[k] < P.lo[k]) c[k] = __fadd_rn(c[k], P.L[k]);
-          }
-        }
-        if (P.kill_on) {
-          const float* c = &x.x;
-#pragma unroll
-          for (int k = 0; k < 3; ++k)
-            if (P.kill_lo[k] < P.kill_hi[k] && (c[k] < P.kill_lo[k] || c[k] > P.kill_hi[k])) dead = true;
-        }
-      }
-      a.main.pos[p] = x;
-      a.main.vel[p] = v;
-    }
+  unsigned drift_bits = 0u;
+  if (!dead && kick_particle(a, P, inst, p, f, x, v, vh, dead, drift_bits)) {
+    a.main.pos[p] = x;
+    a.main.vel[p] = v;
   }
   a.main.vh[p] = vh;
   uint32_t key = kDeadKey;
@@ -168,11 +185,7 @@ __global__ void k_kick_bin(StepArgs a) {
   }
   a.keys_in[p] = key;
   a.vals_in[p] = p;
-  if (a.list_flags) {  // warp-aggregated maximum of the drift ratio
-    const unsigned m = __activemask();
-    const unsigned mx = __reduce_max_sync(m, drift_bits);
-    if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && mx) atomicMax(&a.list_flags[1], mx);
-  }
+  if (a.list_flags) list_flag_max(&a.list_flags[1], drift_bits);
 }
 
 // ------------------------------------------------- permutation + tables

@@ -4,10 +4,10 @@
 // every particle, the candidates within 2h + skin (the list radius) and whose
 // permutation records the positions x0 the lists refer to.  The steps up to
 // the next build skip the binning sort and the candidate scan:
-//   k_kick_bin    KDK first half (periodic wrapping waits for the next build,
-//                 so that the lists' image shifts stay valid)
-//   k_refresh     state copied in place (the sorted order of the build is
-//                 kept), EoS j-records refreshed, |x - x0| checked
+//   k_kick_refresh  KDK first half (periodic wrapping waits for the next
+//                 build, so that the lists' image shifts stay valid), state
+//                 written in the build's order, EoS j-records refreshed,
+//                 |x - x0| checked
 //   k_density_list, k_eos   the density pass from the lists, when one is due
 //   k_hydro_list  the tiled kernel's pair phase over each particle's list
 //                 (warp per cell of the build's cell table), every entry
@@ -16,7 +16,7 @@
 // A pair within the support now was within 2h + |dx_i| + |dx_j| at the
 // build, so the lists hold every pair the support test can accept while no
 // particle has moved more than skin / 2 since the build.  The host rebuilds
-// before that (the kick reports each step's largest drift, k_refresh the
+// before that (k_kick_refresh reports each step's largest drift and the
 // largest displacement); a displacement beyond skin / 2 sets a sticky error
 // that the next wcsph_sim_step reports.
 #pragma once
@@ -27,23 +27,31 @@ namespace wcsph {
 constexpr int kListWarps = 4;
 constexpr int kListMaxEntries = 192;  // entries per list (the solver's list_max; the dam break needs up to ~120)
 
-// Copy main -> alt in place, refresh the j-records, check the displacement.
-__global__ void k_refresh(StepArgs a) {
+// A list step's kick (kick_particle, no wrapping) with the state written
+// straight to the alt buffers in the build's order, the EoS j-records
+// refreshed, and |x - x0| checked.  The main buffers are rewritten from alt by
+// the list pass (every particle below the live count is in a cell of the
+// build's table) and by k_copy_dead (the tail).
+__global__ void k_kick_refresh(StepArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.n_host) return;
-  const uint32_t f = a.main.flags[p];
-  const float4 x = a.main.pos[p];
-  const float4 v = a.main.vel[p];
+  uint32_t f = a.main.flags[p];
+  const int inst = f & kInstMask;
+  const InstParams& P = a.params[inst];
+  bool dead = (f & kDeadBit) || !P.active;
+  float4 x = a.main.pos[p];
+  float4 v = a.main.vel[p];
+  float4 vh = v;
+  unsigned drift_bits = 0u, disp_bits = 0u;
+  if (!dead) kick_particle(a, P, inst, p, f, x, v, vh, dead, drift_bits);
+  if (dead) f |= kDeadBit;
   a.alt.pos[p] = x;
   a.alt.vel[p] = v;
-  a.alt.vh[p] = a.main.vh[p];
+  a.alt.vh[p] = vh;
   a.alt.acc[p] = a.main.acc[p];
   a.alt.pid[p] = a.main.pid[p];
   a.alt.flags[p] = f;
-  const int inst = f & kInstMask;
-  const InstParams& P = a.params[inst];
-  unsigned disp_bits = 0u;
-  if (!(f & kDeadBit) && P.active) {
+  if (!dead) {
     float pres, snds;
     tait(P, x.w, pres, snds);
     a.jA[p] = make_float4(x.x, x.y, x.z, pres / (x.w * x.w));
@@ -54,14 +62,13 @@ __global__ void k_refresh(StepArgs a) {
     const float r = sqrtf(dx * dx + dy * dy + dz * dz) * P.inv_skin;
     disp_bits = __float_as_uint(r);
     if (r > 0.5f) atomicOr(&a.list_flags[2], 1u);  // a pair may be missing from the lists
-  } else {  // removed this step: never in anyone's support again
+  } else {  // removed: never in anyone's support again
     a.jA[p] = make_float4(1.0e30f, 1.0e30f, 1.0e30f, 0.f);
     a.jB[p] = make_float4(0.f, 0.f, 0.f, 1.f);
     a.jC[p] = 0.f;
   }
-  const unsigned m = __activemask();
-  const unsigned mx = __reduce_max_sync(m, disp_bits);
-  if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && mx) atomicMax(&a.list_flags[0], mx);
+  list_flag_max(&a.list_flags[0], disp_bits);
+  list_flag_max(&a.list_flags[1], drift_bits);
 }
 
 // Density pass over the lists: k_density_plain's sums (summation, or the
