@@ -45,7 +45,7 @@ struct SimImpl {
   SimArrays buf_main{}, buf_alt{};
   uint32_t *keys_in = nullptr, *keys_out = nullptr;
   int *vals_in = nullptr, *vals_out = nullptr;
-  float4 *jA = nullptr, *jB = nullptr;
+  JRec* jr = nullptr;
   float *jC = nullptr, *rho_new = nullptr;
   int *cell_start = nullptr, *cell_end = nullptr;
   InstParams* d_params = nullptr;
@@ -112,7 +112,7 @@ static size_t cub_sort_bytes(long long n) {
 static size_t per_particle_bytes() {
   return 2 * (4 * sizeof(float4) + sizeof(int) + sizeof(uint32_t))  // main + alt state
          + 2 * (sizeof(uint32_t) + sizeof(int))                     // sort keys/values in/out
-         + 2 * sizeof(float4) + 2 * sizeof(float)                   // jA, jB, jC, rho_new
+         + 2 * sizeof(float4) + 2 * sizeof(float)                   // j-records (jr, jC), rho_new
          + sizeof(float4) + 2 * sizeof(float) + sizeof(int)         // diagnostics
          + sizeof(int);                                             // non-empty cell list
 }
@@ -176,8 +176,7 @@ static StepArgs make_args(SimImpl& S) {
   a.vals_in = S.vals_in;
   a.keys_out = S.keys_out;
   a.vals_out = S.vals_out;
-  a.jA = S.jA;
-  a.jB = S.jB;
+  a.jr = S.jr;
   a.jC = S.jC;
   a.rho_new = S.rho_new;
   a.cell_start = S.cell_start;
@@ -623,8 +622,7 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
   rc |= alloc(S, (void**)&S.keys_out, N * sizeof(uint32_t));
   rc |= alloc(S, (void**)&S.vals_in, N * sizeof(int));
   rc |= alloc(S, (void**)&S.vals_out, N * sizeof(int));
-  rc |= alloc(S, (void**)&S.jA, N * sizeof(float4));
-  rc |= alloc(S, (void**)&S.jB, N * sizeof(float4));
+  rc |= alloc(S, (void**)&S.jr, N * sizeof(JRec));
   rc |= alloc(S, (void**)&S.jC, N * sizeof(float));
   rc |= alloc(S, (void**)&S.rho_new, N * sizeof(float));
   rc |= alloc(S, (void**)&S.diag_acc, N * sizeof(float4));

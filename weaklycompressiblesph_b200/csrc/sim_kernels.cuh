@@ -5,12 +5,27 @@
 //     pos = (x, y, z, rho)   vel = (vx, vy, vz, -)   vh = (vx_half, ..., -)
 //     acc = (ax, ay, az, div v)   pid (original index)   flags (instance | FREEZE | dead)
 //   j-records written after the EoS, read by the pair kernels (36 B / particle):
-//     jA = (x, y, z, P/rho^2)   jB = (vx, vy, vz, rho)   jC = c
+//     jr[p].a = (x, y, z, P/rho^2)   jr[p].b = (vx, vy, vz, rho)   jC = c
+//     (a and b interleaved: one 32-byte sector per particle, read by the
+//     pair phases with one 256-bit load)
 //   cell table: start/end per linear cell, instance-major.
 #pragma once
 #include "wcsph_common.cuh"
 
 namespace wcsph {
+
+struct __align__(32) JRec {
+  float4 a, b;
+};
+
+// One particle's j-record in a single 256-bit read-only load (sm_100).
+__device__ __forceinline__ JRec ld_jrec(const JRec* p) {
+  JRec r;
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(r.a.x), "=f"(r.a.y), "=f"(r.a.z), "=f"(r.a.w), "=f"(r.b.x), "=f"(r.b.y), "=f"(r.b.z), "=f"(r.b.w)
+      : "l"(p));
+  return r;
+}
 
 struct SimArrays {
   float4 *pos, *vel, *vh, *acc;  // one buffer set
@@ -27,7 +42,7 @@ struct StepArgs {
   int* vals_in;
   const uint32_t* keys_out;
   const int* vals_out;
-  float4 *jA, *jB;
+  JRec* jr;
   float* jC;
   float* rho_new;         // density pass output
   int *cell_start, *cell_end;
@@ -229,8 +244,8 @@ __global__ void k_permute(StepArgs a) {
   if (a.x0) a.x0[p] = make_float4(x.x, x.y, x.z, 0.f);  // list build: positions the lists refer to
   float pres, snds;
   tait(P, x.w, pres, snds);
-  a.jA[p] = make_float4(x.x, x.y, x.z, pres / (x.w * x.w));
-  a.jB[p] = make_float4(v.x, v.y, v.z, x.w);
+  a.jr[p].a = make_float4(x.x, x.y, x.z, pres / (x.w * x.w));
+  a.jr[p].b = make_float4(v.x, v.y, v.z, x.w);
   a.jC[p] = snds;
 }
 
@@ -265,7 +280,7 @@ __device__ __forceinline__ void for_each_neighbor(const StepArgs& a, const InstP
         const int lin = row + x;
         const int s = a.cell_start[lin], e = a.cell_end[lin];
         for (int q = s; q < e; ++q) {
-          const float4 J = __ldg(&a.jA[q]);
+          const float4 J = __ldg(&a.jr[q].a);
           const float dx = __fsub_rn(xi, __fadd_rn(J.x, sx));
           const float dy = __fsub_rn(yi, __fadd_rn(J.y, sy));
           const float dz = __fsub_rn(zi, __fadd_rn(J.z, sz));
@@ -288,15 +303,15 @@ __global__ void k_density_plain(StepArgs a) {
   const InstParams& P = a.params[inst];
   const int kind = density_kind(a, P, a.dyn[inst], a.phase[inst]);
   if (!kind) return;
-  const float4 I = a.jA[p];
-  const float rho_i = a.jB[p].w;
+  const float4 I = a.jr[p].a;
+  const float rho_i = a.jr[p].b.w;
   float sum = 0.5f, one = 0.5f / rho_i;  // self term: w(0) = 1/2
   const float iH = P.inv_H;
   const bool shep = kind == 2;
   for_each_neighbor(a, P, I.x, I.y, I.z, [&](int q, const float4&, float, float, float, float r2) {
     const float w = spline_w(sqrtf(r2) * iH);
     sum += w;
-    if (shep) one += w / __ldg(&a.jB[q].w);
+    if (shep) one += w / __ldg(&a.jr[q].b.w);
   });
   a.rho_new[p] = shep ? sum / one : P.mass * P.Kw * sum;
 }
@@ -313,8 +328,8 @@ __global__ void k_eos(StepArgs a) {
   const float rho = a.rho_new[p];
   float pres, snds;
   tait(P, rho, pres, snds);
-  a.jA[p].w = pres / (rho * rho);
-  a.jB[p].w = rho;
+  a.jr[p].a.w = pres / (rho * rho);
+  a.jr[p].b.w = rho;
   a.jC[p] = snds;
   if (ph != PH_PROBE) a.alt.pos[p].w = rho;
 }
@@ -346,7 +361,7 @@ __device__ __forceinline__ void finish_hydro(const StepArgs& a, int p, const Ins
   float4 x = a.alt.pos[p];
   float4 v = a.alt.vel[p];
   float4 acc;
-  const float rho_i = a.jB[p].w, ci = a.jC[p];
+  const float rho_i = a.jr[p].b.w, ci = a.jC[p];
   const float m = P.mass, h = P.h;
   ax *= m;
   ay *= m;
@@ -415,8 +430,8 @@ __global__ void __launch_bounds__(256) k_hydro_plain(StepArgs a) {
     const InstParams& P = a.params[inst];
     const int ph = a.phase[inst];
     if (wants_force(P, a.dyn[inst], ph)) {
-      const float4 I = a.jA[p];
-      const float4 IB = a.jB[p];
+      const float4 I = a.jr[p].a;
+      const float4 IB = a.jr[p].b;
       const float ci = a.jC[p];
       const float rho_i = IB.w, po_i = I.w;
       float ax = 0.f, ay = 0.f, az = 0.f, dsum = 0.f, vsig = 0.f;
@@ -424,7 +439,7 @@ __global__ void __launch_bounds__(256) k_hydro_plain(StepArgs a) {
       const int vs = P.vsig_mode;
       for_each_neighbor(a, P, I.x, I.y, I.z, [&](int q, const float4& J, float dx, float dy, float dz, float r2) {
         ++cnt;
-        const float4 JB = __ldg(&a.jB[q]);
+        const float4 JB = __ldg(&a.jr[q].b);
         const float cj = __ldg(&a.jC[q]);
         const float rinv = rsqrtf(r2);
         const float g = spline_F(r2 * rinv * iH) * Kg * rinv;

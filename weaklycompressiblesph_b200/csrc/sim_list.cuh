@@ -54,8 +54,8 @@ __global__ void k_kick_refresh(StepArgs a) {
   if (!dead) {
     float pres, snds;
     tait(P, x.w, pres, snds);
-    a.jA[p] = make_float4(x.x, x.y, x.z, pres / (x.w * x.w));
-    a.jB[p] = make_float4(v.x, v.y, v.z, x.w);
+    a.jr[p].a = make_float4(x.x, x.y, x.z, pres / (x.w * x.w));
+    a.jr[p].b = make_float4(v.x, v.y, v.z, x.w);
     a.jC[p] = snds;
     const float4 o = a.x0[p];
     const float dx = x.x - o.x, dy = x.y - o.y, dz = x.z - o.z;
@@ -63,8 +63,8 @@ __global__ void k_kick_refresh(StepArgs a) {
     disp_bits = __float_as_uint(r);
     if (r > 0.5f) atomicOr(&a.list_flags[2], 1u);  // a pair may be missing from the lists
   } else {  // removed: never in anyone's support again
-    a.jA[p] = make_float4(1.0e30f, 1.0e30f, 1.0e30f, 0.f);
-    a.jB[p] = make_float4(0.f, 0.f, 0.f, 1.f);
+    a.jr[p].a = make_float4(1.0e30f, 1.0e30f, 1.0e30f, 0.f);
+    a.jr[p].b = make_float4(0.f, 0.f, 0.f, 1.f);
     a.jC[p] = 0.f;
   }
   list_flag_max(&a.list_flags[0], disp_bits);
@@ -99,13 +99,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_density_list(StepArgs a) {
       const bool valid = p < e;
       const bool dead = valid && (a.alt.flags[p] & kDeadBit);
       const int n = valid && !dead ? min(a.list_cnt[p], a.list_max) : 0;
-      const float4 I = valid ? __ldg(&a.jA[p]) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 I = valid ? __ldg(&a.jr[p].a) : make_float4(0.f, 0.f, 0.f, 0.f);
       const uint32_t* l = a.list + (size_t)(valid ? p : s) * a.list_max;
       float sum = 0.f, one = 0.f;
       for (int k = sub; k < n; k += 8) {
         const uint32_t ent = __ldg(&l[k]);
         const int q = ent & kSlotMask;
-        const float4 J = __ldg(&a.jA[q]);
+        const float4 J = __ldg(&a.jr[q].a);
         float sx = 0.f, sy = 0.f, sz = 0.f;
         if (P.periodic) entry_shift(P, ent >> 27, sx, sy, sz);
         const float dx = __fsub_rn(I.x, __fadd_rn(J.x, sx));
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_density_list(StepArgs a) {
         if (r2 > 0.0f && r2 < H2) {
           const float w = spline_w(sqrtf(r2) * iH);
           sum += w;
-          if (shep) one += w / __ldg(&a.jB[q].w);
+          if (shep) one += w / __ldg(&a.jr[q].b.w);
         }
       }
 #pragma unroll
@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_density_list(StepArgs a) {
         if (dead) {
           a.rho_new[p] = a.alt.pos[p].w;
         } else {
-          const float rho_i = __ldg(&a.jB[p].w);
+          const float rho_i = __ldg(&a.jr[p].b.w);
           const float t = 0.5f + sum;  // self term: w(0) = 1/2
           a.rho_new[p] = shep ? t / (0.5f / rho_i + one) : P.mass * P.Kw * t;
         }
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(WARPS * 32, 5) k_hydro_list(StepArgs a) {
         if (copy_failed) na = nb = 0;
         __syncwarp();
         if (ii + 2 < nbat) fetch(ii + 2, buf ^ 1);
-        hydro_queues2<H16, true>(a, P, ia, ibb, has_b, __ldg(&a.jA[ia]), __ldg(&a.jA[ibb]), s_q[warp][buf][0], na,
+        hydro_queues2<H16, true>(a, P, ia, ibb, has_b, __ldg(&a.jr[ia].a), __ldg(&a.jr[ibb].a), s_q[warp][buf][0], na,
                                  s_q[warp][buf][1], nb, &res[ii], lane);
         fence_proxy_async();  // this buffer is refilled by a bulk copy two pairs on
         __syncwarp();

@@ -106,7 +106,7 @@ template <bool H16, bool CHECK = false>
 __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParams& P, int ia, int ib, bool has_b,
                                               const float4& IA, const float4& IBp, const uint32_t* qa, int na,
                                               const uint32_t* qb, int nb, float (*res)[6], int lane) {
-  const float4 VA = __ldg(&a.jB[ia]), VB = __ldg(&a.jB[ib]);
+  const float4 VA = __ldg(&a.jr[ia].b), VB = __ldg(&a.jr[ib].b);
   const f2 X = pk(IA.x, IBp.x), Y = pk(IA.y, IBp.y), Z = pk(IA.z, IBp.z);
   const f2 VX = pk(VA.x, VB.x), VY = pk(VA.y, VB.y), VZ = pk(VA.z, VB.z);
   const f2 RHO = pk(VA.w, VB.w), PO = pk(IA.w, IBp.w);
@@ -128,8 +128,8 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
     const uint32_t self = (uint32_t)ia | (13u << 27);
     const uint32_t ea = qva ? qa[k] : self, eb = qvb ? qb[k] : self;
     const int ga = ea & kSlotMask, gb = eb & kSlotMask;
-    const float4 Ja = __ldg(&a.jA[ga]), Jb = __ldg(&a.jA[gb]);
-    const float4 JBa = __ldg(&a.jB[ga]), JBb = __ldg(&a.jB[gb]);
+    const JRec Ra = ld_jrec(&a.jr[ga]), Rb = ld_jrec(&a.jr[gb]);
+    const float4 &Ja = Ra.a, &Jb = Rb.a, &JBa = Ra.b, &JBb = Rb.b;
     const f2 CJ = pk(__ldg(&a.jC[ga]), __ldg(&a.jC[gb]));
     float jxa = Ja.x, jya = Ja.y, jza = Ja.z, jxb = Jb.x, jyb = Jb.y, jzb = Jb.z;
     if (per) {  // the same rounded image position the scan tested
@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
             const int sk = __shfl_sync(full, nb_start, k), ek = __shfl_sync(full, excl, k);
             kk[r] = k;
             gk[r] = sk + (u - ek);
-            if (u < t0 + tn) J[r] = __ldg(&a.jA[gk[r]]);
+            if (u < t0 + tn) J[r] = __ldg(&a.jr[gk[r]].a);
           }
 #pragma unroll
           for (int r = 0; r < kStageUnroll; ++r) {
@@ -350,10 +350,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
           const int ibb = has_b ? ia + 1 : ia;
           // i positions from the tile when the own cell (lane 13) is staged in this pass
           const int oa = own + (ia - s) - t0, ob = own + (ibb - s) - t0;
-          const float4 IA = (oa >= 0 && oa < tn) ? make_float4(tx[oa], ty[oa], tz[oa], __ldg(&a.jA[ia].w))
-                                                 : __ldg(&a.jA[ia]);
-          const float4 IB = (ob >= 0 && ob < tn) ? make_float4(tx[ob], ty[ob], tz[ob], __ldg(&a.jA[ibb].w))
-                                                 : __ldg(&a.jA[ibb]);
+          const float4 IA = (oa >= 0 && oa < tn) ? make_float4(tx[oa], ty[oa], tz[oa], __ldg(&a.jr[ia].a.w))
+                                                 : __ldg(&a.jr[ia].a);
+          const float4 IB = (ob >= 0 && ob < tn) ? make_float4(tx[ob], ty[ob], tz[ob], __ldg(&a.jr[ibb].a.w))
+                                                 : __ldg(&a.jr[ibb].a);
           const f2 XA = dup(IA.x), YA = dup(IA.y), ZA = dup(IA.z);
           const f2 XB = dup(IB.x), YB = dup(IB.y), ZB = dup(IB.z);
           int na = 0, nb = 0;
