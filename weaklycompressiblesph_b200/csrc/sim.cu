@@ -287,7 +287,7 @@ static int enqueue_reuse(SimImpl& S, StepArgs a, bool density, int* launches, cu
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));
     if (density) {  // the kernels return at once for instances with no density pass due
-      if (int rc = launch_density_list<8>(a, S.s)) return rc;
+      if (int rc = launch_density_list(a, n, S.s)) return rc;
       k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
       L += 2;
     }
@@ -473,11 +473,6 @@ static int read_list_flags(SimImpl& S) {
     WCSPH_CUDA(cudaStreamSynchronize(S.s));
     S.lists_valid = false;
     if (e & 2u) ++S.n_overflow;
-    if (e & kListErrCopy) {
-      set_error("wcsph_sim_step: a bulk copy of a neighbour list did not complete; the step's pair sums are "
-                "incomplete");
-      return WCSPH_E_CUDA;
-    }
     if (e & 1u) {
       set_error("wcsph_sim_step: a particle moved more than half the neighbour-list skin between list builds; "
                 "the step's pair sums may be incomplete (raise list_skin or lower list_interval)");

@@ -93,12 +93,106 @@ __device__ __forceinline__ void entry_shift(const InstParams& P, uint32_t code, 
   sz = (float)((int)(code / 9u) - 1) * P.L[2];
 }
 
-// Pair terms of i_a (low half) and i_b (high half) over their queues; adds
-// the warp totals into res[0] (i_a) and res[1] (i_b): ax, ay, az, sum g drdv,
-// v_sig, count.  Lanes past a queue's end contribute exactly zero.
+// Operands of pair2.  PairI: the i-side of the two halves (two i-particles,
+// or one i duplicated); PairC: the instance constants, built once per i.
+struct PairI {
+  f2 X, Y, Z, VX, VY, VZ, RHO, PO, CI;
+};
+struct PairC {
+  float H2, iH, KgiH;
+  f2 IH, KG, EH2, HH, NU4, BETA, MHALPHA;
+  int vs;
+  bool per;
+};
+__device__ __forceinline__ PairC pair_consts(const InstParams& P) {
+  PairC c;
+  c.H2 = P.H2, c.iH = P.inv_H, c.KgiH = P.Kg * P.inv_H;
+  c.IH = dup(P.inv_H), c.KG = dup(P.Kg), c.EH2 = dup(P.eh2), c.HH = dup(P.h), c.NU4 = dup(P.nu4);
+  c.BETA = dup(P.beta), c.MHALPHA = dup(-0.5f * P.alpha);
+  c.vs = P.vsig_mode, c.per = P.periodic;
+  return c;
+}
+
+// Pair terms of two (i, j) pairs at once, one per f32x2 half (force.h:38-57
+// for uniform h, m, nu within an instance): j-records Ra, Rb with image codes
+// ea, eb (entry >> 27) and sound speeds CJ; qva, qvb say whether a half holds
+// a pair (idle halves must still name a valid record; they add exactly zero).
+// Accumulates a_x, a_y, a_z, sum g dr.dv and the v_sig maximum per half.
+// CHECK: halves outside 0 < r^2 < (2h)^2 add exactly zero, and na, nb count
+// the halves summed.
 // H16: the kernel gradient (|dr|^2, 1/|dr|, s, F(s), F/|dr|) is evaluated in
 // packed half2 on displacements in units of the support 2h; everything else
 // stays FP32 (WCSPH_PREC_HALF2).
+template <bool H16, bool CHECK>
+__device__ __forceinline__ void pair2(const InstParams& P, const PairC& C, const PairI& I, const JRec& Ra,
+                                      const JRec& Rb, uint32_t ea, uint32_t eb, f2 CJ, bool qva, bool qvb, f2& AX,
+                                      f2& AY, f2& AZ, f2& DS, float& vsa, float& vsb, unsigned& na, unsigned& nb) {
+  const f2 ONE = dup(1.0f), HALF = dup(0.5f), TWELVE = dup(12.0f), MTHREE = dup(-3.0f), TWO = dup(2.0f);
+  const f2 MONE = dup(-1.0f);
+  const float4 &Ja = Ra.a, &Jb = Rb.a, &JBa = Ra.b, &JBb = Rb.b;
+  float jxa = Ja.x, jya = Ja.y, jza = Ja.z, jxb = Jb.x, jyb = Jb.y, jzb = Jb.z;
+  if (C.per) {  // the same rounded image position the scan tested
+    float sx, sy, sz;
+    entry_shift(P, ea, sx, sy, sz);
+    jxa = __fadd_rn(jxa, sx), jya = __fadd_rn(jya, sy), jza = __fadd_rn(jza, sz);
+    entry_shift(P, eb, sx, sy, sz);
+    jxb = __fadd_rn(jxb, sx), jyb = __fadd_rn(jyb, sy), jzb = __fadd_rn(jzb, sz);
+  }
+  const f2 DX = sub2(I.X, pk(jxa, jxb)), DY = sub2(I.Y, pk(jya, jyb)), DZ = sub2(I.Z, pk(jza, jzb));
+  const f2 R2raw = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
+  const bool va = CHECK ? qva && lo(R2raw) > 0.0f && lo(R2raw) < C.H2 : qva;
+  const bool vb = CHECK ? qvb && hi(R2raw) > 0.0f && hi(R2raw) < C.H2 : qvb;
+  if (CHECK) na += va, nb += vb;
+  const f2 R2 = pk(va ? lo(R2raw) : C.H2, vb ? hi(R2raw) : C.H2);  // finite stand-in for idle halves
+  const f2 W = pk(va ? 1.0f : 0.0f, vb ? 1.0f : 0.0f);
+  f2 G;  // gradW = G * dr
+  if (H16) {
+    const float iH = C.iH;
+    // q = dr / 2h; idle halves get a harmless |q| = 1/2
+    const __half2 qx = __floats2half2_rn(va ? lo(DX) * iH : 0.5f, vb ? hi(DX) * iH : 0.5f);
+    const __half2 qy = __floats2half2_rn(va ? lo(DY) * iH : 0.0f, vb ? hi(DY) * iH : 0.0f);
+    const __half2 qz = __floats2half2_rn(va ? lo(DZ) * iH : 0.0f, vb ? hi(DZ) * iH : 0.0f);
+    const __half2 r2h = __hmax2(__hfma2(qz, qz, __hfma2(qy, qy, __hmul2(qx, qx))), __float2half2_rn(1.0e-4f));
+    const __half2 rih = h2rsqrt(r2h);
+    const __half2 sh = __hmul2(r2h, rih);  // s = |dr| / 2h
+    const __half2 ah = __hmax2(__hsub2(__float2half2_rn(1.0f), sh), __float2half2_rn(0.0f));
+    const __half2 bh = __hmax2(__hsub2(__float2half2_rn(0.5f), sh), __float2half2_rn(0.0f));
+    const __half2 Fh = __hfma2(__float2half2_rn(12.0f), __hmul2(bh, bh),
+                               __hmul2(__float2half2_rn(-3.0f), __hmul2(ah, ah)));
+    const float2 gq = __half22float2(__hmul2(Fh, rih));  // F(s) / |q|
+    G = mul2(pk(gq.x, gq.y), mul2(dup(C.KgiH), W));       // g = F Kg / |dr| = (F/|q|) Kg / 2h
+  } else {
+    const f2 RINV = rsqrt2(R2);
+    const f2 S = mul2(mul2(R2, RINV), C.IH);
+    const f2 A = max0_2(sub2(ONE, S)), B = max0_2(sub2(HALF, S));
+    const f2 F = fma2(TWELVE, mul2(B, B), mul2(MTHREE, mul2(A, A)));  // 12 (1/2-s)+^2 - 3 (1-s)+^2
+    G = mul2(mul2(F, C.KG), mul2(RINV, W));
+  }
+  const f2 DVX = sub2(I.VX, pk(JBa.x, JBb.x)), DVY = sub2(I.VY, pk(JBa.y, JBb.y)), DVZ = sub2(I.VZ, pk(JBa.z, JBb.z));
+  const f2 DRDV = fma2(DZ, DVZ, fma2(DY, DVY, mul2(DX, DVX)));
+  const f2 RDEN = rcp2(add2(R2, C.EH2));
+  const f2 MUr = mul2(mul2(DRDV, RDEN), C.HH);
+  const f2 MU = pk(va && lo(DRDV) < 0.0f ? lo(MUr) : 0.0f, vb && hi(DRDV) < 0.0f ? hi(MUr) : 0.0f);
+  const f2 RS = rcp2(add2(I.RHO, pk(JBa.w, JBb.w)));
+  const f2 AV = mul2(mul2(fma2(C.BETA, MU, mul2(C.MHALPHA, add2(I.CI, CJ))), MU), mul2(RS, TWO));
+  if (C.vs) {
+    vsa = fmaxf(vsa, -lo(MU));
+    vsb = fmaxf(vsb, -hi(MU));
+  } else {
+    vsa = fmaxf(vsa, lo(MU));
+    vsb = fmaxf(vsb, hi(MU));
+  }
+  const f2 NPG = mul2(mul2(add2(add2(I.PO, pk(Ja.w, Jb.w)), AV), G), MONE);
+  const f2 VISC = mul2(mul2(mul2(C.NU4, G), R2), mul2(RS, RDEN));
+  AX = fma2(NPG, DX, fma2(VISC, DVX, AX));
+  AY = fma2(NPG, DY, fma2(VISC, DVY, AY));
+  AZ = fma2(NPG, DZ, fma2(VISC, DVZ, AZ));
+  DS = fma2(G, DRDV, DS);
+}
+
+// Pair terms of i_a (low half) and i_b (high half) over their queues; adds
+// the warp totals into res[0] (i_a) and res[1] (i_b): ax, ay, az, sum g drdv,
+// v_sig, count.  Lanes past a queue's end contribute exactly zero.
 // CHECK: the queues may hold entries outside the support (neighbour lists with
 // a skin); each entry is tested for 0 < r^2 < (2h)^2 on the current positions,
 // entries outside contribute exactly zero and are not counted.
@@ -107,16 +201,12 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
                                               const float4& IA, const float4& IBp, const uint32_t* qa, int na,
                                               const uint32_t* qb, int nb, float (*res)[6], int lane) {
   const float4 VA = __ldg(&a.jr[ia].b), VB = __ldg(&a.jr[ib].b);
-  const f2 X = pk(IA.x, IBp.x), Y = pk(IA.y, IBp.y), Z = pk(IA.z, IBp.z);
-  const f2 VX = pk(VA.x, VB.x), VY = pk(VA.y, VB.y), VZ = pk(VA.z, VB.z);
-  const f2 RHO = pk(VA.w, VB.w), PO = pk(IA.w, IBp.w);
-  const f2 CI = pk(__ldg(&a.jC[ia]), __ldg(&a.jC[ib]));
-  const float H2 = P.H2;
-  const f2 IH = dup(P.inv_H), KG = dup(P.Kg), EH2 = dup(P.eh2), HH = dup(P.h), NU4 = dup(P.nu4);
-  const f2 ONE = dup(1.0f), HALF = dup(0.5f), TWELVE = dup(12.0f), MTHREE = dup(-3.0f), TWO = dup(2.0f);
-  const f2 BETA = dup(P.beta), MHALPHA = dup(-0.5f * P.alpha), MONE = dup(-1.0f);
-  const int vs = P.vsig_mode;
-  const bool per = P.periodic;
+  PairI I;
+  I.X = pk(IA.x, IBp.x), I.Y = pk(IA.y, IBp.y), I.Z = pk(IA.z, IBp.z);
+  I.VX = pk(VA.x, VB.x), I.VY = pk(VA.y, VB.y), I.VZ = pk(VA.z, VB.z);
+  I.RHO = pk(VA.w, VB.w), I.PO = pk(IA.w, IBp.w);
+  I.CI = pk(__ldg(&a.jC[ia]), __ldg(&a.jC[ib]));
+  const PairC C = pair_consts(P);
   const int nbq = has_b ? nb : 0;
   const int n = max(na, nbq);
   f2 AX = 0ull, AY = 0ull, AZ = 0ull, DS = 0ull;
@@ -129,66 +219,8 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
     const uint32_t ea = qva ? qa[k] : self, eb = qvb ? qb[k] : self;
     const int ga = ea & kSlotMask, gb = eb & kSlotMask;
     const JRec Ra = ld_jrec(&a.jr[ga]), Rb = ld_jrec(&a.jr[gb]);
-    const float4 &Ja = Ra.a, &Jb = Rb.a, &JBa = Ra.b, &JBb = Rb.b;
     const f2 CJ = pk(__ldg(&a.jC[ga]), __ldg(&a.jC[gb]));
-    float jxa = Ja.x, jya = Ja.y, jza = Ja.z, jxb = Jb.x, jyb = Jb.y, jzb = Jb.z;
-    if (per) {  // the same rounded image position the scan tested
-      float sx, sy, sz;
-      entry_shift(P, ea >> 27, sx, sy, sz);
-      jxa = __fadd_rn(jxa, sx), jya = __fadd_rn(jya, sy), jza = __fadd_rn(jza, sz);
-      entry_shift(P, eb >> 27, sx, sy, sz);
-      jxb = __fadd_rn(jxb, sx), jyb = __fadd_rn(jyb, sy), jzb = __fadd_rn(jzb, sz);
-    }
-    const f2 DX = sub2(X, pk(jxa, jxb)), DY = sub2(Y, pk(jya, jyb)), DZ = sub2(Z, pk(jza, jzb));
-    const f2 R2raw = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
-    const bool va = CHECK ? qva && lo(R2raw) > 0.0f && lo(R2raw) < H2 : qva;
-    const bool vb = CHECK ? qvb && hi(R2raw) > 0.0f && hi(R2raw) < H2 : qvb;
-    if (CHECK) ca += va, cb += vb;
-    const f2 R2 = pk(va ? lo(R2raw) : H2, vb ? hi(R2raw) : H2);  // finite stand-in for idle halves
-    const f2 W = pk(va ? 1.0f : 0.0f, vb ? 1.0f : 0.0f);
-    f2 G;  // gradW = G * dr
-    if (H16) {
-      const float iH = P.inv_H;
-      // q = dr / 2h; idle halves get a harmless |q| = 1/2
-      const __half2 qx = __floats2half2_rn(va ? lo(DX) * iH : 0.5f, vb ? hi(DX) * iH : 0.5f);
-      const __half2 qy = __floats2half2_rn(va ? lo(DY) * iH : 0.0f, vb ? hi(DY) * iH : 0.0f);
-      const __half2 qz = __floats2half2_rn(va ? lo(DZ) * iH : 0.0f, vb ? hi(DZ) * iH : 0.0f);
-      const __half2 r2h = __hmax2(__hfma2(qz, qz, __hfma2(qy, qy, __hmul2(qx, qx))), __float2half2_rn(1.0e-4f));
-      const __half2 rih = h2rsqrt(r2h);
-      const __half2 sh = __hmul2(r2h, rih);  // s = |dr| / 2h
-      const __half2 ah = __hmax2(__hsub2(__float2half2_rn(1.0f), sh), __float2half2_rn(0.0f));
-      const __half2 bh = __hmax2(__hsub2(__float2half2_rn(0.5f), sh), __float2half2_rn(0.0f));
-      const __half2 Fh = __hfma2(__float2half2_rn(12.0f), __hmul2(bh, bh),
-                                 __hmul2(__float2half2_rn(-3.0f), __hmul2(ah, ah)));
-      const float2 gq = __half22float2(__hmul2(Fh, rih));  // F(s) / |q|
-      G = mul2(pk(gq.x, gq.y), mul2(dup(P.Kg * iH), W));    // g = F Kg / |dr| = (F/|q|) Kg / 2h
-    } else {
-      const f2 RINV = rsqrt2(R2);
-      const f2 S = mul2(mul2(R2, RINV), IH);
-      const f2 A = max0_2(sub2(ONE, S)), B = max0_2(sub2(HALF, S));
-      const f2 F = fma2(TWELVE, mul2(B, B), mul2(MTHREE, mul2(A, A)));  // 12 (1/2-s)+^2 - 3 (1-s)+^2
-      G = mul2(mul2(F, KG), mul2(RINV, W));
-    }
-    const f2 DVX = sub2(VX, pk(JBa.x, JBb.x)), DVY = sub2(VY, pk(JBa.y, JBb.y)), DVZ = sub2(VZ, pk(JBa.z, JBb.z));
-    const f2 DRDV = fma2(DZ, DVZ, fma2(DY, DVY, mul2(DX, DVX)));
-    const f2 RDEN = rcp2(add2(R2, EH2));
-    const f2 MUr = mul2(mul2(DRDV, RDEN), HH);
-    const f2 MU = pk(va && lo(DRDV) < 0.0f ? lo(MUr) : 0.0f, vb && hi(DRDV) < 0.0f ? hi(MUr) : 0.0f);
-    const f2 RS = rcp2(add2(RHO, pk(JBa.w, JBb.w)));
-    const f2 AV = mul2(mul2(fma2(BETA, MU, mul2(MHALPHA, add2(CI, CJ))), MU), mul2(RS, TWO));
-    if (vs) {
-      vsa = fmaxf(vsa, -lo(MU));
-      vsb = fmaxf(vsb, -hi(MU));
-    } else {
-      vsa = fmaxf(vsa, lo(MU));
-      vsb = fmaxf(vsb, hi(MU));
-    }
-    const f2 NPG = mul2(mul2(add2(add2(PO, pk(Ja.w, Jb.w)), AV), G), MONE);
-    const f2 VISC = mul2(mul2(mul2(NU4, G), R2), mul2(RS, RDEN));
-    AX = fma2(NPG, DX, fma2(VISC, DVX, AX));
-    AY = fma2(NPG, DY, fma2(VISC, DVY, AY));
-    AZ = fma2(NPG, DZ, fma2(VISC, DVZ, AZ));
-    DS = fma2(G, DRDV, DS);
+    pair2<H16, CHECK>(P, C, I, Ra, Rb, ea >> 27, eb >> 27, CJ, qva, qvb, AX, AY, AZ, DS, vsa, vsb, ca, cb);
   }
   const float v8[8] = {lo(AX), lo(AY), lo(AZ), lo(DS), hi(AX), hi(AY), hi(AZ), hi(DS)};
   const float y = butterfly8(v8, lane);
