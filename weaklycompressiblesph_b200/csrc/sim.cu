@@ -451,6 +451,7 @@ static int fill_params(const wcsph_instance_desc& d, HostInst& I, InstParams& P)
   P.B = (float)B;
   P.gamma = (float)d.gamma;
   P.cs2_coef = (float)(B * d.gamma / d.rho0);
+  P.c0 = (float)std::sqrt(B * d.gamma / d.rho0);
   P.rho_floor = (float)d.rho_floor;
   P.g = (float)d.g;
   P.dt_nu = d.nu > 0 ? (float)(0.125 * d.h * d.h / d.nu) : INFINITY;

@@ -127,11 +127,20 @@ inline int launch_density_list(const StepArgs& a, int n, cudaStream_t s) {
   return 0;
 }
 
+// snds7 of the two densities in the f32x2 halves, bit-identical to snds7.
+__device__ __forceinline__ f2 snds7_2(f2 RHO, f2 RHO0, f2 IRHO0, f2 C0) {
+  const f2 X = add2(dup(1.0f), mul2(sub2(RHO, RHO0), IRHO0));
+  const f2 T = mul2(C0, mul2(mul2(X, X), X));
+  return pk(fmaxf(fabsf(lo(T)), 1.0e-8f), fmaxf(fabsf(hi(T)), 1.0e-8f));
+}
+
 // The list pass with one thread per particle slot below the build's live
 // count (the particles of the build's cell table; the dead tail is k_copy_dead's):
 // each thread walks its own list row four entries per 16-byte load and sums
 // two entries at a time in the f32x2 halves of pair2, support tested per
-// entry; no shared memory, no cross-lane reduction.
+// entry; no shared memory, no cross-lane reduction.  For gamma = 7 the sound
+// speed of j is recomputed from its density (snds7_2, the stored value bit
+// for bit) instead of gathered: one gather per entry fewer.
 template <bool H16>
 __global__ void __launch_bounds__(128, 5) k_hydro_list(StepArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -153,6 +162,8 @@ __global__ void __launch_bounds__(128, 5) k_hydro_list(StepArgs a) {
       I.VX = dup(R.b.x), I.VY = dup(R.b.y), I.VZ = dup(R.b.z), I.RHO = dup(R.b.w);
       I.CI = dup(a.jC[p]);
       const PairC C = pair_consts(P);
+      const bool g7 = P.gamma == 7.0f;
+      const f2 RHO0 = dup(P.rho0), IRHO0 = dup(P.inv_rho0), C0 = dup(P.c0);
       const int n = min(a.list_cnt[p], a.list_max);
       const uint4* row = reinterpret_cast<const uint4*>(a.list + (size_t)p * a.list_max);
       const uint32_t self = (uint32_t)p | (13u << 27);  // idle halves: i's own record, weight 0
@@ -165,7 +176,13 @@ __global__ void __launch_bounds__(128, 5) k_hydro_list(StepArgs a) {
         const int g0 = e0 & kSlotMask, g1 = e1 & kSlotMask, g2 = e2 & kSlotMask, g3 = e3 & kSlotMask;
         const JRec R0 = ld_jrec(&a.jr[g0]), R1 = ld_jrec(&a.jr[g1]);
         const JRec R2 = ld_jrec(&a.jr[g2]), R3 = ld_jrec(&a.jr[g3]);
-        const f2 C01 = pk(__ldg(&a.jC[g0]), __ldg(&a.jC[g1])), C23 = pk(__ldg(&a.jC[g2]), __ldg(&a.jC[g3]));
+        f2 C01, C23;
+        if (g7) {  // c_j from rho_j: no gather of c
+          C01 = snds7_2(pk(R0.b.w, R1.b.w), RHO0, IRHO0, C0);
+          C23 = snds7_2(pk(R2.b.w, R3.b.w), RHO0, IRHO0, C0);
+        } else {
+          C01 = pk(__ldg(&a.jC[g0]), __ldg(&a.jC[g1])), C23 = pk(__ldg(&a.jC[g2]), __ldg(&a.jC[g3]));
+        }
         pair2<H16, true>(P, C, I, R0, R1, e0 >> 27, e1 >> 27, C01, true, k + 1 < n, AX, AY, AZ, DS, vsa, vsb, ca, cb);
         pair2<H16, true>(P, C, I, R2, R3, e2 >> 27, e3 >> 27, C23, k + 2 < n, k + 3 < n, AX, AY, AZ, DS, vsa, vsb,
                          ca, cb);

@@ -87,7 +87,7 @@ struct InstParams {
   int density_mode, shepard_interval, vsig_mode, kill_on;
   // physics in FP32, precomputed
   float h, H2, inv_H, Kg, Kw, W0, mass, nu4, eh2, alpha, beta, c_cfl;
-  float rho0, inv_rho0, B, gamma, cs2_coef /* B*gamma/rho0 */, rho_floor, g;
+  float rho0, inv_rho0, B, gamma, cs2_coef /* B*gamma/rho0 */, c0 /* sqrt(cs2_coef) */, rho_floor, g;
   float dt_nu;            // 0.125 h^2 / nu (or +inf)
   float kill_lo[3], kill_hi[3];
   float slab_margin2;     // slab instances: squared largest drift a step may make (0: not a slab)
@@ -141,26 +141,34 @@ __device__ __forceinline__ bool neighbor_cell(const InstParams& P, int k, int q,
   return true;
 }
 
+// Sound speed of the Tait EoS for gamma = 7: sqrt(B gamma/rho0 x^6) = c0 |x^3|
+// with x = 1 + (rho - rho0)/rho0, floored at sqrt(1e-16).  Every step is
+// rounded explicitly, so that the packed form in the list pass (snds7_2)
+// reproduces it bit for bit from rho alone.
+__device__ __forceinline__ float snds7(const InstParams& P, float rho) {
+  const float x = __fadd_rn(1.0f, __fmul_rn(__fsub_rn(rho, P.rho0), P.inv_rho0));
+  const float x3 = __fmul_rn(__fmul_rn(x, x), x);
+  return fmaxf(fabsf(__fmul_rn(P.c0, x3)), 1.0e-8f);
+}
+
 // Tait EoS (EoS.h:75-90): P = max(B ((rho/rho0)^gamma - 1), 0),
 // c = sqrt(max(B gamma/rho0 (rho/rho0)^(gamma-1), 1e-16)).
 // (rho/rho0)^gamma - 1 is evaluated on d = (rho - rho0)/rho0 without the
 // cancellation of x^gamma - 1 near rho0 (weakly compressible: |d| ~ 1e-3):
 // for gamma = 7 the binomial expansion d (7 + d (21 + d (35 + ...))) in Horner
-// form, otherwise expm1(gamma log1p(d)).
+// form (and c by snds7), otherwise expm1(gamma log1p(d)).
 __device__ __forceinline__ void tait(const InstParams& P, float rho, float& pres, float& snds) {
   const float d = (rho - P.rho0) * P.inv_rho0;
-  float xgm1, xg1;
+  float xgm1;
   if (P.gamma == 7.0f) {
     xgm1 = d * (7.0f + d * (21.0f + d * (35.0f + d * (35.0f + d * (21.0f + d * (7.0f + d))))));
-    const float x = 1.0f + d, x2 = x * x, x3 = x2 * x;
-    xg1 = x3 * x3;
+    snds = snds7(P, rho);
   } else {
     const float l = log1pf(d);
     xgm1 = expm1f(P.gamma * l);
-    xg1 = expf((P.gamma - 1.0f) * l);
+    snds = sqrtf(fmaxf(P.cs2_coef * expf((P.gamma - 1.0f) * l), 1.0e-16f));
   }
   pres = fmaxf(P.B * xgm1, 0.0f);
-  snds = sqrtf(fmaxf(P.cs2_coef * xg1, 1.0e-16f));
 }
 
 }  // namespace wcsph
