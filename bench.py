@@ -51,7 +51,7 @@ def parse():
                     help="N>1: independent replicas (weak scaling) or one dam break cut into x-slabs (strong)")
     ap.add_argument("--list-interval", type=int, default=30,
                     help="neighbour lists rebuilt at least every K steps (0: search every step)")
-    ap.add_argument("--list-skin", type=float, default=0.0, help="list skin in units of h (0: 0.2)")
+    ap.add_argument("--list-skin", type=float, default=0.0, help="list skin in units of h (0: 0.3)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-only", action="store_true",
                     help="time only the FDPS drop-in pass (dispatch + retrieve from host records), --steps passes")
@@ -224,7 +224,7 @@ def run_device(case, prec_name, steps, warmup, device, clocks=False, list_interv
             ls1 = s.list_stats()
             b, r = ls1["builds"] - ls0["builds"], ls1["list_steps"] - ls0["list_steps"]
             res["kernels_per_step"] = (b * ls1["kernels_build"] + r * ls1["kernels_list"]) / max(1, b + r)
-            res["lists"] = {"interval": list_interval, "skin_h": list_skin or 0.2, "timed_builds": b,
+            res["lists"] = {"interval": list_interval, "skin_h": list_skin or 0.3, "timed_builds": b,
                             "timed_list_steps": r, "overflows": ls1["overflows"], "longest": ls1["longest"]}
         # per-phase kernel times (eager launches, CUDA events on the solver stream)
         prof_steps = max(3, min(20, steps // 5))

@@ -207,7 +207,7 @@ typedef struct wcsph_sim_options {
                                   read the lists and test 0 < r^2 < (2h)^2 on current positions,
                                   so the pairs summed are the same as with a fresh search (the
                                   summation order differs) */
-  float list_skin;             /* skin in units of h (0: 0.2) */
+  float list_skin;             /* skin in units of h (0: 0.3) */
   int32_t reserved_;
 } wcsph_sim_options;
 

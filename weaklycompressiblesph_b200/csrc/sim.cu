@@ -93,8 +93,8 @@ struct SimImpl {
   float last_disp = 0.f, last_drift = 0.f;  // from the latest completed step, in units of the skin
 };
 
-constexpr int kListMax = kListMaxEntries;  // entries per particle list (2h + 0.2 h holds ~90-120 at h = 1.3 dx)
-static float list_skin(const wcsph_sim_options& o) { return o.list_skin > 0.f ? o.list_skin : 0.2f; }
+constexpr int kListMax = kListMaxEntries;  // entries per particle list (2h + 0.3 h holds ~100-115 at h = 1.3 dx)
+static float list_skin(const wcsph_sim_options& o) { return o.list_skin > 0.f ? o.list_skin : 0.3f; }
 
 static int alloc(SimImpl& S, void** p, size_t bytes) {
   WCSPH_CUDA(cudaMalloc(p, bytes ? bytes : 16));
