@@ -245,14 +245,17 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[2], S.s));
     if (S.opt.precision == WCSPH_PREC_FP32) {
       k_hydro_plain<true><<<nblk(n), kBlock, 0, S.s>>>(a);
+    } else if (build_lists) {  // the scan writes the lists, the list pass sums them
+      const bool h16 = S.opt.precision == WCSPH_PREC_HALF2;
+      if (int rc = h16 ? launch_hydro_tiled<true, true>(a, n, S.s, S.tile_shape)
+                       : launch_hydro_tiled<false, true>(a, n, S.s, S.tile_shape))
+        return rc;
+      if (int rc = h16 ? launch_hydro_list<true>(a, n, S.s) : launch_hydro_list<false>(a, n, S.s)) return rc;
+      ++L;
     } else if (S.opt.precision == WCSPH_PREC_TILED) {
-      if (int rc = build_lists ? launch_hydro_tiled<false, true>(a, n, S.s, S.tile_shape)
-                               : launch_hydro_tiled<false>(a, n, S.s, S.tile_shape))
-        return rc;
+      if (int rc = launch_hydro_tiled<false>(a, n, S.s, S.tile_shape)) return rc;
     } else {
-      if (int rc = build_lists ? launch_hydro_tiled<true, true>(a, n, S.s, S.tile_shape)
-                               : launch_hydro_tiled<true>(a, n, S.s, S.tile_shape))
-        return rc;
+      if (int rc = launch_hydro_tiled<true>(a, n, S.s, S.tile_shape)) return rc;
     }
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[3], S.s));
@@ -277,7 +280,8 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
 static int enqueue_reuse(SimImpl& S, StepArgs a, bool density, int* launches, cudaEvent_t* ev = nullptr) {
   const int n = S.n_host;
   a.list_reuse = 1;
-  a.x0 = S.x0;  // read by k_kick_refresh (the displacement since the build)
+  a.x0 = S.x0;    // read by k_kick_refresh (the displacement since the build)
+  a.alt = a.main;  // in place: no re-sort, each particle's state is its own thread's
   if (ev) WCSPH_CUDA(cudaEventRecord(ev[0], S.s));
   WCSPH_CUDA(cudaMemsetAsync(S.d_counters + 4, 0, sizeof(int), S.s));
   k_step_begin<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
@@ -298,9 +302,7 @@ static int enqueue_reuse(SimImpl& S, StepArgs a, bool density, int* launches, cu
       if (int rc = launch_hydro_list<false>(a, n, S.s)) return rc;
     }
     ++L;
-    if (ev) WCSPH_CUDA(cudaEventRecord(ev[3], S.s));
-    k_copy_dead<<<nblk(n), kBlock, 0, S.s>>>(a);
-    ++L;
+    if (ev) WCSPH_CUDA(cudaEventRecord(ev[3], S.s));  // the dead tail stays in place
   }
   WCSPH_CUDA(cudaGetLastError());
   if (launches) *launches = L;

@@ -255,8 +255,10 @@ __device__ __forceinline__ bool wants_force(const InstParams& P, const InstDyn& 
   return ph == PH_INIT || ph == PH_PROBE || (ph == PH_STEP && d.dt_cur > 0.0f);
 }
 
-// Neighbour-cell iteration shared by the plain kernels.  Calls body(q, dx, dy, dz, r2)
-// for every in-support j (0 < r2 < (2h)^2, FP32 predicate of the oracle).
+// Neighbour-cell iteration shared by the plain kernels.  Calls
+// body(q, J, dx, dy, dz, r2, code) for every in-support j (0 < r2 < (2h)^2,
+// FP32 predicate of the oracle); code is the periodic image code of the tiled
+// kernel's queue entries ((sx+1) + 3 (sy+1) + 9 (sz+1) in units of the box).
 template <typename Body>
 __device__ __forceinline__ void for_each_neighbor(const StepArgs& a, const InstParams& P, float xi, float yi, float zi,
                                                   Body&& body) {
@@ -279,13 +281,15 @@ __device__ __forceinline__ void for_each_neighbor(const StepArgs& a, const InstP
         if (!neighbor_cell(P, 0, cx + ox, x, sx)) continue;
         const int lin = row + x;
         const int s = a.cell_start[lin], e = a.cell_end[lin];
+        const uint32_t code = (uint32_t)((sx > 0.f) - (sx < 0.f) + 1 + 3 * ((sy > 0.f) - (sy < 0.f) + 1) +
+                                         9 * ((sz > 0.f) - (sz < 0.f) + 1));
         for (int q = s; q < e; ++q) {
           const float4 J = __ldg(&a.jr[q].a);
           const float dx = __fsub_rn(xi, __fadd_rn(J.x, sx));
           const float dy = __fsub_rn(yi, __fadd_rn(J.y, sy));
           const float dz = __fsub_rn(zi, __fadd_rn(J.z, sz));
           const float r2 = dist2(dx, dy, dz);
-          if (r2 > 0.0f && r2 < H2) body(q, J, dx, dy, dz, r2);
+          if (r2 > 0.0f && r2 < H2) body(q, J, dx, dy, dz, r2, code);
         }
       }
     }
@@ -308,7 +312,7 @@ __global__ void k_density_plain(StepArgs a) {
   float sum = 0.5f, one = 0.5f / rho_i;  // self term: w(0) = 1/2
   const float iH = P.inv_H;
   const bool shep = kind == 2;
-  for_each_neighbor(a, P, I.x, I.y, I.z, [&](int q, const float4&, float, float, float, float r2) {
+  for_each_neighbor(a, P, I.x, I.y, I.z, [&](int q, const float4&, float, float, float, float r2, uint32_t) {
     const float w = spline_w(sqrtf(r2) * iH);
     sum += w;
     if (shep) one += w / __ldg(&a.jr[q].b.w);
@@ -437,7 +441,8 @@ __global__ void __launch_bounds__(256) k_hydro_plain(StepArgs a) {
       float ax = 0.f, ay = 0.f, az = 0.f, dsum = 0.f, vsig = 0.f;
       const float h = P.h, eh2 = P.eh2, Kg = P.Kg, iH = P.inv_H, alpha = P.alpha, beta = P.beta, nu4 = P.nu4;
       const int vs = P.vsig_mode;
-      for_each_neighbor(a, P, I.x, I.y, I.z, [&](int q, const float4& J, float dx, float dy, float dz, float r2) {
+      for_each_neighbor(a, P, I.x, I.y, I.z, [&](int q, const float4& J, float dx, float dy, float dz, float r2,
+                                                  uint32_t) {
         ++cnt;
         const float4 JB = __ldg(&a.jr[q].b);
         const float cj = __ldg(&a.jC[q]);

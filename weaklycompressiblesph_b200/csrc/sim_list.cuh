@@ -1,13 +1,13 @@
 // Neighbour-list steps (wcsph_sim_options.list_interval > 0).
 //
-// A build step is an ordinary step whose tiled hydro kernel also writes, for
-// every particle, the candidates within 2h + skin (the list radius) and whose
-// permutation records the positions x0 the lists refer to.  The steps up to
-// the next build skip the binning sort and the candidate scan:
-//   k_kick_refresh  KDK first half (periodic wrapping waits for the next
-//                 build, so that the lists' image shifts stay valid), state
-//                 written in the build's order, EoS j-records refreshed,
-//                 |x - x0| checked
+// A build step is an ordinary step whose tiled kernel only scans: it writes,
+// for every particle, the candidates within 2h + skin (the list radius), and
+// the pair terms are summed by the list pass (k_hydro_list); its permutation
+// records the positions x0 the lists refer to.  The steps up to the next
+// build skip the binning sort and the candidate scan:
+//   k_kick_refresh  KDK first half in place (periodic wrapping waits for the
+//                 next build, so that the lists' image shifts stay valid),
+//                 EoS j-records refreshed, |x - x0| checked
 //   k_density_list, k_eos   the density pass from the lists, when one is due
 //   k_hydro_list  the pair terms over each particle's list (thread per
 //                 particle), every entry tested for 0 < r^2 < (2h)^2 on the
@@ -25,11 +25,10 @@ namespace wcsph {
 
 constexpr int kListMaxEntries = 192;  // entries per list (the solver's list_max; the dam break needs up to ~120)
 
-// A list step's kick (kick_particle, no wrapping) with the state written
-// straight to the alt buffers in the build's order, the EoS j-records
-// refreshed, and |x - x0| checked.  The main buffers are rewritten from alt by
-// the list pass (every particle below the live count is in a cell of the
-// build's table) and by k_copy_dead (the tail).
+// A list step's kick (kick_particle, no wrapping), in place in the build's
+// order, with the EoS j-records refreshed and |x - x0| checked.  List steps
+// run on one buffer set (alt = main): every particle's state is read and
+// written by its own thread only, so the list pass updates it in place too.
 __global__ void k_kick_refresh(StepArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.n_host) return;
@@ -41,14 +40,12 @@ __global__ void k_kick_refresh(StepArgs a) {
   float4 v = a.main.vel[p];
   float4 vh = v;
   unsigned drift_bits = 0u, disp_bits = 0u;
-  if (!dead) kick_particle(a, P, inst, p, f, x, v, vh, dead, drift_bits);
-  if (dead) f |= kDeadBit;
-  a.alt.pos[p] = x;
-  a.alt.vel[p] = v;
-  a.alt.vh[p] = vh;
-  a.alt.acc[p] = a.main.acc[p];
-  a.alt.pid[p] = a.main.pid[p];
-  a.alt.flags[p] = f;
+  if (!dead && kick_particle(a, P, inst, p, f, x, v, vh, dead, drift_bits)) {
+    a.main.pos[p] = x;
+    a.main.vel[p] = v;
+  }
+  a.main.vh[p] = vh;
+  if (dead && !(f & kDeadBit)) a.main.flags[p] = f | kDeadBit;
   if (!dead) {
     float pres, snds;
     tait(P, x.w, pres, snds);
@@ -135,7 +132,8 @@ __device__ __forceinline__ f2 snds7_2(f2 RHO, f2 RHO0, f2 IRHO0, f2 C0) {
 }
 
 // The list pass with one thread per particle slot below the build's live
-// count (the particles of the build's cell table; the dead tail is k_copy_dead's):
+// count (the particles of the build's cell table; the dead tail is
+// k_copy_dead's), on list steps and right after the scan of a build step:
 // each thread walks its own list row four entries per 16-byte load and sums
 // two entries at a time in the f32x2 halves of pair2, support tested per
 // entry; no shared memory, no cross-lane reduction.  For gamma = 7 the sound
@@ -164,12 +162,26 @@ __global__ void __launch_bounds__(128, 5) k_hydro_list(StepArgs a) {
       const PairC C = pair_consts(P);
       const bool g7 = P.gamma == 7.0f;
       const f2 RHO0 = dup(P.rho0), IRHO0 = dup(P.inv_rho0), C0 = dup(P.c0);
-      const int n = min(a.list_cnt[p], a.list_max);
+      const int cnt_build = a.list_cnt[p];
+      const int n = cnt_build <= a.list_max ? cnt_build : 0;
       const uint4* row = reinterpret_cast<const uint4*>(a.list + (size_t)p * a.list_max);
       const uint32_t self = (uint32_t)p | (13u << 27);  // idle halves: i's own record, weight 0
       f2 AX = 0ull, AY = 0ull, AZ = 0ull, DS = 0ull;
       float vsa = 0.f, vsb = 0.f;
       unsigned ca = 0, cb = 0;
+      if (cnt_build > a.list_max) {
+        // The list overflowed at this step's build (the host rebuilds at the
+        // next step, so no list step ever sees it): sum over the cell search
+        // of the build's cell table instead, one j at a time.
+        for_each_neighbor(a, P, R.a.x, R.a.y, R.a.z,
+                          [&](int q, const float4&, float, float, float, float, uint32_t code) {
+                            const JRec Rq = ld_jrec(&a.jr[q]);
+                            const float cq = g7 ? lo(snds7_2(dup(Rq.b.w), RHO0, IRHO0, C0)) : __ldg(&a.jC[q]);
+                            pair2<H16, false>(P, C, I, Rq, R, code, 13u, dup(cq), true, false, AX, AY, AZ, DS, vsa,
+                                              vsb, ca, cb);
+                            ++ca;
+                          });
+      }
       for (int k = 0; k < n; k += 4) {
         const uint4 e = __ldg(&row[k >> 2]);
         const uint32_t e0 = e.x, e1 = k + 1 < n ? e.y : self, e2 = k + 2 < n ? e.z : self, e3 = k + 3 < n ? e.w : self;

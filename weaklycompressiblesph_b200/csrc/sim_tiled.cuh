@@ -193,10 +193,7 @@ __device__ __forceinline__ void pair2(const InstParams& P, const PairC& C, const
 // Pair terms of i_a (low half) and i_b (high half) over their queues; adds
 // the warp totals into res[0] (i_a) and res[1] (i_b): ax, ay, az, sum g drdv,
 // v_sig, count.  Lanes past a queue's end contribute exactly zero.
-// CHECK: the queues may hold entries outside the support (neighbour lists with
-// a skin); each entry is tested for 0 < r^2 < (2h)^2 on the current positions,
-// entries outside contribute exactly zero and are not counted.
-template <bool H16, bool CHECK = false>
+template <bool H16>
 __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParams& P, int ia, int ib, bool has_b,
                                               const float4& IA, const float4& IBp, const uint32_t* qa, int na,
                                               const uint32_t* qb, int nb, float (*res)[6], int lane) {
@@ -211,7 +208,7 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
   const int n = max(na, nbq);
   f2 AX = 0ull, AY = 0ull, AZ = 0ull, DS = 0ull;
   float vsa = 0.f, vsb = 0.f;
-  unsigned ca = 0, cb = 0;  // CHECK: in-support entries of this lane
+  unsigned ca = 0, cb = 0;  // unused: every queue entry is in support
   for (int k = lane; k < n; k += 32) {
     const bool qva = k < na, qvb = k < nbq;
     // idle halves read i_a's own record (always a valid slot; weight 0 below)
@@ -220,7 +217,7 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
     const int ga = ea & kSlotMask, gb = eb & kSlotMask;
     const JRec Ra = ld_jrec(&a.jr[ga]), Rb = ld_jrec(&a.jr[gb]);
     const f2 CJ = pk(__ldg(&a.jC[ga]), __ldg(&a.jC[gb]));
-    pair2<H16, CHECK>(P, C, I, Ra, Rb, ea >> 27, eb >> 27, CJ, qva, qvb, AX, AY, AZ, DS, vsa, vsb, ca, cb);
+    pair2<H16, false>(P, C, I, Ra, Rb, ea >> 27, eb >> 27, CJ, qva, qvb, AX, AY, AZ, DS, vsa, vsb, ca, cb);
   }
   const float v8[8] = {lo(AX), lo(AY), lo(AZ), lo(DS), hi(AX), hi(AY), hi(AZ), hi(DS)};
   const float y = butterfly8(v8, lane);
@@ -231,16 +228,12 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
     if (slot < 4) res[0][slot] += y;
     else if (has_b) res[1][slot - 4] += y;
   }
-  if (CHECK) {
-    ca = __reduce_add_sync(0xffffffffu, ca);
-    cb = __reduce_add_sync(0xffffffffu, cb);
-  }
   if (lane == 0) {
     res[0][4] = fmaxf(res[0][4], vsa);
-    res[0][5] += (float)(CHECK ? (int)ca : na);
+    res[0][5] += (float)na;
     if (has_b) {
       res[1][4] = fmaxf(res[1][4], vsb);
-      res[1][5] += (float)(CHECK ? (int)cb : nb);
+      res[1][5] += (float)nb;
     }
   }
 }
@@ -254,9 +247,11 @@ __device__ __forceinline__ void append2(uint32_t* q, int& n, bool he, bool ho, u
   n += __popc(me) + __popc(mo);
 }
 
-// LB (neighbour-list build): the scan keeps candidates within the list radius
-// 2h + skin, each i's queue entries are also written to its list, and the
-// pair phase tests the support per entry (CHECK).
+// LB (neighbour-list build): scan only.  The scan keeps the candidates
+// within the list radius 2h + skin and each i's queue is written to its list
+// (list_cnt holds the full count, also past the list's capacity); the pair
+// terms and the epilogue are left to the list pass (k_hydro_list) that
+// follows, as on the steps that reuse the lists.
 template <bool H16, int WARPS, int TILE, bool LB = false>
 __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
   constexpr int kTiledWarps = WARPS;
@@ -290,8 +285,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
     const int ph = a.phase[inst];
     if (!wants_force(P, a.dyn[inst], ph)) {
       for (int p = s + lane; p < e; p += 32) {
-        copy_state(a, p);
         if (LB) a.list_cnt[p] = 0;
+        else copy_state(a, p);
       }
       continue;
     }
@@ -417,20 +412,20 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
             if (lane == ii) lcount += na;
             if (has_b && lane == ii + 1) lcount += nb;
           }
-          hydro_queues2<H16, LB>(a, P, ia, ibb, has_b, IA, IB, qa, na, qb, nb, &res[ii], lane);
+          if (!LB) hydro_queues2<H16>(a, P, ia, ibb, has_b, IA, IB, qa, na, qb, nb, &res[ii], lane);
           __syncwarp();
         }
       }
       __syncwarp();
       if (LB) {
         if (lane < nbat) {
-          a.list_cnt[ib + lane] = min(lcount, a.list_max);
+          a.list_cnt[ib + lane] = lcount;
           if (lcount > a.list_max) atomicOr(&a.list_flags[2], 2u);  // overflow: rebuild next step
         }
         const int mx = __reduce_max_sync(full, lane < nbat ? lcount : 0);
         if (lane == 0) atomicMax(&a.list_flags[3], (unsigned)mx);
       }
-      if (lane < nbat) {
+      if (!LB && lane < nbat) {
         const int p = ib + lane;
         const float* r = res[lane];
         const uint32_t fp = a.alt.flags[p];
