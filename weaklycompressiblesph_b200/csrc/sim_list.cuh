@@ -23,7 +23,7 @@
 
 namespace wcsph {
 
-constexpr int kListMaxEntries = 192;  // entries per list (the solver's list_max; the dam break needs up to ~120)
+constexpr int kListMaxEntries = 192;  // entries per list (the solver's list_max; the dam break needs up to ~140)
 
 // A list step's kick (kick_particle, no wrapping), in place in the build's
 // order, with the EoS j-records refreshed and |x - x0| checked.  List steps
