@@ -82,57 +82,107 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled every 10 ms on a thread (reads only), the device matched
+    by PCI bus id; nvidia-smi at its 200 ms floor when NVML is unavailable.
+    Call mark_start() / mark_stop() around the timed work; only samples taken in
+    between are summarised."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.lines = []
+        self.samples = []  # (time, sm_mhz, max_mhz, reasons)
+        self.t0 = self.t1 = None
+        self.stop = threading.Event()
+        self.thread = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.device)
+        try:
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _poll_nvml(self, nv, h):
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        while not self.stop.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((time.perf_counter(), sm, mx, {k for k, v in bits.items() if r & v}))
+            except Exception:
+                pass
+            self.stop.wait(0.01)
+
+    def _read_smi(self):
+        for ln in self.proc.stdout:
+            f = [x.strip() for x in ln.strip().split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm, mx = float(f[1]), float(f[2])
+            except ValueError:
+                continue
+            self.samples.append((time.perf_counter(), sm, mx,
+                                 {nm for k, nm in enumerate(self.NAMES) if f[4 + k].lower().startswith("active")}))
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            nv, h = self._nvml_handle()
+            self.thread = threading.Thread(target=self._poll_nvml, args=(nv, h), daemon=True)
         except Exception:
-            self.proc = None
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                              "--format=csv,noheader,nounits", "-lms", "200"],
+                                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.thread = threading.Thread(target=self._read_smi, daemon=True)
+            except Exception:
+                self.thread = None
+        if self.thread:
+            self.thread.start()
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def mark_start(self):
+        self.t0 = time.perf_counter()
+
+    def mark_stop(self):
+        self.t1 = time.perf_counter()
 
     def __exit__(self, *exc):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 8:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for k, nm in enumerate(names):
-                if f[4 + k].lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
-
+        t0 = self.t0 if self.t0 is not None else -math.inf
+        t1 = self.t1 if self.t1 is not None else math.inf
+        sel = [x for x in self.samples if t0 <= x[0] <= t1]
+        if not sel and self.samples:  # a region shorter than one sampling period: the nearest sample
+            sel = [min(self.samples, key=lambda x: abs(x[0] - t1))]
+        reasons = set()
+        for x in sel:
+            reasons |= x[3]
+        return {"sm_mhz": statistics.median([x[1] for x in sel]) if sel else None,
+                "sm_max_mhz": sel[-1][2] if sel else None, "reasons": sorted(reasons), "samples": len(sel),
+                "source": "nvml" if self.proc is None else "nvidia-smi"}
 
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -212,8 +262,11 @@ def run_device(case, prec_name, steps, warmup, device, clocks=False, list_interv
         sampler = ClockSampler(device) if clocks else None
         if sampler:
             sampler.__enter__()
+            time.sleep(0.05)  # the sampler's first reading comes before the timed region
+            sampler.mark_start()
         ms = cuda_events_ms(s.stream(), lambda: s.step(steps))
         if sampler:
+            sampler.mark_stop()
             sampler.__exit__()
             res["clocks"] = sampler.summary()
         pairs_end = s.last_pairs()
@@ -252,8 +305,11 @@ def run_slab(case, prec_name, steps, warmup, rank, world, device, pg, clocks=Fal
         sampler = ClockSampler(device) if clocks else None
         if sampler:
             sampler.__enter__()
+            time.sleep(0.05)
+            sampler.mark_start()
         ms = cuda_events_ms(dom.solver.stream(), lambda: drv.step(steps))
         if sampler:
+            sampler.mark_stop()
             sampler.__exit__()
         res = {"ms_per_step": ms / steps, "pairs_per_step": 0.5 * (pairs + dom.last_pairs()),
                "kernels_per_step": dom.solver.kernels_per_step() + 3,  # + classify, pack, commit (+ unpacks)
