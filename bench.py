@@ -258,6 +258,11 @@ def run_device(case, prec_name, steps, warmup, device, clocks=False, list_interv
         s.step(warmup)
         s.synchronize()
         pairs = s.last_pairs()
+        if lists:
+            # the timed steps start with a list build, so that they carry their
+            # share of builds (one at least, then one every list_interval steps
+            # or sooner when the drift rule asks) whatever their number
+            s.invalidate_lists()
         ls0 = s.list_stats() if lists else None
         sampler = ClockSampler(device) if clocks else None
         if sampler:
@@ -378,16 +383,18 @@ def run_e2e(case, steps, warmup, device):
                 epj=epj, dispatch_ms=1e3 * split[0] / steps, retrieve_ms=1e3 * split[1] / steps)
 
 
-def cpu_reference(case, walks, epi, epj, seconds, pairs_total):
-    """The reference's CalcHydroForce (oracle/_ref) on a bounded sample of the
-    same walks, all host threads.  Returns (pairs/s, sample description, cores)."""
+def cpu_reference(case, walks, epi, epj, seconds, pairs_total, whole_budget_s=None):
+    """The reference's CalcHydroForce (oracle/_ref) over the walks of the
+    workload on all host threads.  Whole passes over every walk when one fits
+    in whole_budget_s (default: seconds), else repeated passes over a bounded
+    sample of the walks (every k-th walk).  Returns (pairs/s, description,
+    cores, seconds of one whole pass or None)."""
     import oracle
     if not oracle.ref_available():
         raise RuntimeError("oracle/_ref/libwcsph_ref.so missing")
     cores = os.cpu_count() or 1
     cfg = oracle.config_from_case(case)
     cnt, tot = oracle.neighbors(oracle.pos4(case.pos.astype(np.float32)), cfg)
-    # probe: time one small sample to size the bounded run
     n_walk = walks.n_walk
     stride = max(1, n_walk // 64)
     sel = np.arange(0, n_walk, stride)
@@ -402,18 +409,32 @@ def cpu_reference(case, walks, epi, epj, seconds, pairs_total):
         pairs = int(sum(cnt[walks.i_idx[walks.i_off[k]:walks.i_off[k + 1]]].sum() for k in sel))
         return i_off, ei, j_off, ej, pairs
 
+    # probe on the sample to estimate a whole pass
     i_off, ei, j_off, ej, pairs = sample(sel)
     t0 = time.perf_counter()
     oracle.ref_hydro_walks(i_off, ei, j_off, ej, nthreads=cores)
-    t1 = time.perf_counter() - t0
-    reps = max(1, int(seconds / max(t1, 1e-3)))
+    t1 = max(time.perf_counter() - t0, 1e-4)
+    est_whole = t1 * tot / max(pairs, 1)
+    budget = seconds if whole_budget_s is None else whole_budget_s
+    consts = "(the functor's own alpha 0.01 and C_CFL 0.3, force.h:32, param.h:5: the same pairs and arithmetic as " \
+             "the config's alpha 0.1, C_CFL 0.25)"
+    if est_whole <= budget:
+        reps = max(1, int(seconds / est_whole))
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            oracle.ref_hydro_walks(walks.i_off, epi, walks.j_off, epj, nthreads=cores)
+        el = (time.perf_counter() - t0) / reps
+        desc = (f"whole passes over all {n_walk} FDPS-style walks (<=128 i each), {tot} true pairs, {reps} "
+                f"repetitions, STD::CalcHydroForce -O3 -ffast-math OpenMP {consts}")
+        return tot / el, desc, cores, el
+    reps = max(1, int(seconds / t1))
     t0 = time.perf_counter()
     for _ in range(reps):
         oracle.ref_hydro_walks(i_off, ei, j_off, ej, nthreads=cores)
     el = (time.perf_counter() - t0) / reps
     desc = (f"{len(sel)} of {n_walk} FDPS-style walks (every {stride}th, <=128 i each), {pairs} true pairs, "
-            f"{reps} repetitions, STD::CalcHydroForce -O3 -ffast-math OpenMP")
-    return pairs / el, desc, cores
+            f"{reps} repetitions, STD::CalcHydroForce -O3 -ffast-math OpenMP {consts}")
+    return pairs / el, desc, cores, None
 
 
 def measure_ensemble(device, steps=None):
@@ -533,8 +554,8 @@ def main():
                "d2h_bytes_per_step": e["d2h"], "path": "wcsph_hydro_dispatch/retrieve, FDPS walks of <=128 i",
                "walks": e["n_walk"], "pair_evaluations_per_pass": e["evaluated"]}
         if not args.no_cpu:
-            v, desc, cores = cpu_reference(case, e["walks"], e["epi"], e["epj"], args.cpu_seconds,
-                                           dev["pairs_per_step"])
+            v, desc, cores, _ = cpu_reference(case, e["walks"], e["epi"], e["epj"], args.cpu_seconds,
+                                              dev["pairs_per_step"])
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc}
     ens = srv = None
     if rank == 0 and not args.no_ensemble:
@@ -550,16 +571,7 @@ def main():
         "scaling": "strong" if slab_mode else "weak",
         "vs_baseline": None, "dtype": "f32" if prec != "half2" else "f16x2-pair/f32-accumulate",
         "data": "synthetic (seeded lattice IC, no dataset)",
-        "config": {"workload": {"dam1m": "3-D dam break dx=0.005 (1,024,000 fluid + 571,308 wall particles)",
-                                "dam16k": "3-D dam break dx=0.02 (16,000 fluid + 38,508 wall particles)",
-                                "periodic8m": "periodic jittered lattice 200^3 dx=0.01"}[args.workload],
-                   "n_particles": case.n, "precision": prec, "h_over_dx": case.phys.h_over_dx,
-                   "neighbour_search": (f"lists of radius 2h + {dev['lists']['skin_h']:g} h, rebuilt at least every "
-                                        f"{dev['lists']['interval']} steps" if dev.get("lists") else "every step"),
-                   "density_mode": case.phys.density_mode,
-                   "parallelism": f"slab x{world}" if slab_mode else f"replicas x{world}",
-                   "l2": "working set > L2 (126 MB): particle state and records "
-                         f"{case.n * 200 / 1e6:.0f} MB, no flush needed"},
+        "config": bench_config(args, case, prec, world),
         "steps_per_s": steps_per_s * 1.0,
         "pairs_per_step": dev["pairs_per_step"],
         "plain_fp32": plain,
@@ -590,6 +602,22 @@ def main():
     return 0
 
 
+def bench_config(args, case, prec, world):
+    """The workload description, the same in both arms (a function of the
+    command line and the case only)."""
+    lists = args.list_interval > 0 and prec != "fp32" and args.decomp != "slab"
+    return {"workload": {"dam1m": "3-D dam break dx=0.005 (1,024,000 fluid + 571,308 wall particles)",
+                         "dam16k": "3-D dam break dx=0.02 (16,000 fluid + 38,508 wall particles)",
+                         "periodic8m": "periodic jittered lattice 200^3 dx=0.01"}[args.workload],
+            "n_particles": case.n, "precision": prec, "h_over_dx": case.phys.h_over_dx,
+            "neighbour_search": (f"lists of radius 2h + {args.list_skin or 0.3:g} h, rebuilt at least every "
+                                 f"{args.list_interval} steps" if lists else "every step"),
+            "density_mode": case.phys.density_mode,
+            "parallelism": f"slab x{world}" if args.decomp == "slab" else f"replicas x{world}",
+            "l2": "working set > L2 (126 MB): particle state and records "
+                  f"{case.n * 200 / 1e6:.0f} MB, no flush needed"}
+
+
 def finish(pg):
     if pg is not None:
         pg.destroy_process_group()
@@ -608,17 +636,20 @@ def main_reference(args):
     w = fdps.build_walks(case.pos, 2.0 * case.h, group_size=128)
     epi, epj = fdps.walk_records(w, case.pos, case.vel, case.dens, pres, snds, case.h, case.mass, case.phys.nu,
                                  type_=case.type)
-    per_step = max(1.0, min(10.0, 120.0 / max(1, args.steps + args.warmup)))
+    # each step one whole pass over every walk when the whole run stays within
+    # about four minutes, else a bounded sample of the walks
+    per_step = max(1.0, min(10.0, 240.0 / max(1, args.steps + args.warmup)))
     vals = []
     for k in range(args.warmup + args.steps):
-        v, desc, cores = cpu_reference(case, w, epi, epj, per_step, None)
+        v, desc, cores, _ = cpu_reference(case, w, epi, epj, per_step, None, whole_budget_s=per_step)
         if k >= args.warmup:
             vals.append(v)
     value = statistics.median(vals)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice IC, no dataset)",
-            "config": {"workload": args.workload, "n_particles": case.n},
+            "config": bench_config(args, case, args.precision if args.precision != "best" else best_precision(),
+                                   int(os.environ.get("WORLD_SIZE", "1"))),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))

@@ -123,8 +123,10 @@ int wcsph_hydro_dispatch(int32_t tag, int32_t n_walk, const void* const* epi, co
 int wcsph_hydro_retrieve(int32_t tag, int32_t n_walk, const int32_t* n_i, void* const* force);
 
 /* Allocation-free walk pair sum.  No counterpart in the reference: it is for
- * callers that cannot allocate device memory (code running inside CUDA graph
- * capture, hosts with a fixed device-memory budget or their own allocator).
+ * callers that cannot allocate device memory, such as an application that owns
+ * all device memory through its own pool allocator or runs under a fixed
+ * device-memory budget, or a host loop where a cudaMalloc would synchronise
+ * the device in the middle of a step.
  * Everything is device-resident and caller-owned:
  *   d_n_epi, d_n_epj  n_walk int32 walk sizes
  *   d_epi             sum(n_epi) records of three float4:
@@ -312,11 +314,26 @@ int wcsph_sim_read_instance(wcsph_sim* sim, int32_t slot, float* pos3, float* ve
  * each particle.  density_pass: 0 none, 1 summation, 2 Shepard first. */
 int wcsph_sim_probe_forces(wcsph_sim* sim, int32_t slot, int32_t density_pass, float* acc3, float* div_v, float* dt_i,
                            float* dens_out, int32_t* n_neighbors);
+/* The same diagnostics computed by the passes a neighbour-list step runs
+ * (list_interval > 0): the density pass from the lists (k_density_list) and
+ * the pair terms over the lists (k_hydro_list), on the current lists and the
+ * current state (the step's refresh of the j-records without its kick).  The
+ * sums are those of src/force.h:31-60 (pairs) and src/force.h:12-29 (Shepard)
+ * over the in-support entries of each list.  When the solver holds no current
+ * lists (none built yet, or the instance set changed), a probe build pass
+ * makes them first; the steps that follow read them.  Returns WCSPH_E_STATE
+ * when the solver has no lists. */
+int wcsph_sim_probe_lists(wcsph_sim* sim, int32_t slot, int32_t density_pass, float* acc3, float* div_v, float* dt_i,
+                          float* dens_out, int32_t* n_neighbors);
 /* The sorted order of the last binning: perm[k] = original index of the
  * particle in sorted slot k of the instance, and the Morton cell key of each slot. */
 int wcsph_sim_read_order(wcsph_sim* sim, int32_t slot, int32_t* perm, uint32_t* cell_key);
-/* Conservation sums over an instance, accumulated on the device in FP64:
- * out[0] mass, out[1..3] momentum, out[4] kinetic energy, out[5] sum of acc*m. */
+/* Conservation sums over an instance's live particles, accumulated on the
+ * device in FP64 from the state after the last step (the KDK update of
+ * src/class.h:146-163): out[0] mass, out[1..3] momentum, out[4] kinetic
+ * energy, out[5] sum m (a_z + g), the vertical total of the pair forces with
+ * gravity taken out (zero up to rounding: the pair terms of force.h:38-57
+ * are antisymmetric). */
 int wcsph_sim_conservation(wcsph_sim* sim, int32_t slot, double* out6);
 
 /* Number of true in-support (ordered) pairs the hydro pass summed in the
@@ -335,6 +352,11 @@ int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out3);
  * step builds again), out[3] largest list built so far, out[4] kernel
  * launches of a build step, out[5] kernel launches of a list step. */
 int wcsph_sim_list_stats(wcsph_sim* sim, int64_t* out6);
+/* Drop the current neighbour lists (list_interval > 0): the next step builds
+ * them again, as after a change of the instance set.  For callers that edit
+ * state outside the solver, and for timing a build-inclusive sequence of
+ * steps.  A no-op without lists. */
+int wcsph_sim_invalidate_lists(wcsph_sim* sim);
 /* The solver's CUDA stream (a cudaStream_t), so callers can record events on it. */
 void* wcsph_sim_stream(wcsph_sim* sim);
 /* Run nsteps steps launched one by one (no graph) with CUDA events around each

@@ -213,3 +213,30 @@ def test_invalid_configs(native):
             s.add(case)
     with pytest.raises(N.WcsphError):
         Solver(0)
+
+
+@pytest.mark.parametrize("lists", [0, 6], ids=["search", "lists"])
+def test_conservation_sums_fp64(prec, native, lists):
+    """wcsph_sim_conservation (FP64 on the device) against FP64 sums of the
+    same state read back: mass, momentum, kinetic energy, and the vertical
+    total of the pair forces, which cancels pair by pair (force.h:38-57)."""
+    if lists and prec == N.PREC_FP32:
+        pytest.skip("neighbour lists need the tiled or half2 precision")
+    case = small_dam(dx=0.04, seed=31, vel_sigma=0.3)
+    with Solver(case.n, precision=prec, list_interval=lists) as s:
+        k = s.add(case)
+        s.step(9)
+        st = s.read(k)
+        c = s.conservation(k)
+    alive = st["alive"] == 1
+    m = case.mass
+    v = st["vel"][alive].astype(np.float64)
+    a = st["acc"][alive].astype(np.float64)
+    assert c[0] == pytest.approx(m * alive.sum(), rel=1e-12)
+    np.testing.assert_allclose(c[1:4], m * v.sum(axis=0), rtol=1e-9, atol=1e-12 * m * np.abs(v).sum())
+    assert c[4] == pytest.approx(0.5 * m * (v * v).sum(), rel=1e-9)
+    ref5 = m * (a[:, 2] + case.phys.g).sum()
+    assert c[5] == pytest.approx(ref5, rel=1e-9, abs=1e-12 * m * np.abs(a[:, 2]).sum())
+    # the pair forces cancel: their vertical total is rounding noise next to the
+    # sum of their magnitudes
+    assert abs(c[5]) < 1e-5 * m * np.abs(a[:, 2] + case.phys.g).sum()

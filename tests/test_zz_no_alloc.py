@@ -1,11 +1,13 @@
 """The allocation-free walk pair sum (wcsph_hydro_walks_noalloc).
 
-Some callers cannot allocate device memory: code running while a CUDA graph
-is captured, or hosts that give the plugin a fixed device-memory budget.  For
-them the library keeps its only scratch (the per-walk displacement tables) in
-a static device array.  This test calls the entry point through the C ABI,
+Some callers cannot allocate device memory: an application whose device
+memory all comes from its own pool or a fixed budget, or a host loop in which
+a cudaMalloc would synchronise the device in the middle of a step.  For them
+the library keeps its only scratch (the per-walk displacement tables) in a
+static device array.  This test calls the entry point through the C ABI,
 twice in a row on the same buffers, and checks both results against the
-allocating entry point (wcsph_hydro_dispatch / wcsph_hydro_retrieve) at the
+allocating entry point (wcsph_hydro_dispatch / wcsph_hydro_retrieve) and
+against the FP64 oracle's walk-mode pair sum (oracle.hydro_walks), at the
 FP32 tolerance the other parity tests use (relative L2 1e-5).  The file is
 named to be collected last.
 """
@@ -49,7 +51,7 @@ def pack(w, epi, epj):
     return n_i.astype(np.int32), n_j.astype(np.int32), ri, rj
 
 
-def test_noalloc_matches_allocating_entry_point(native):
+def test_noalloc_matches_allocating_entry_point(native, oracle_lib):
     import torch
 
     case = small_dam(dx=0.05, seed=21)
@@ -58,6 +60,9 @@ def test_noalloc_matches_allocating_entry_point(native):
     fdps.configure(pair)
     ref = np.zeros(len(epi), fdps.RESULT_HYDRO)
     fdps.calc_force_multiwalk(w, epi, epj, ref)
+    fp64 = oracle_lib.hydro_walks(w.i_off, epi, w.j_off, epj,
+                                  oracle_lib.PairParams(pair.alpha, pair.beta, pair.c_cfl, pair.eps, pair.vsig_mode,
+                                                        pair.grad_mode))
 
     n_i, n_j, ri, rj = pack(w, epi, epj)
     dev = torch.device("cuda", 0)
@@ -75,9 +80,10 @@ def test_noalloc_matches_allocating_entry_point(native):
         torch.cuda.synchronize(dev)
         out = d_out.cpu().numpy().reshape(-1, 2, 4)
         assert np.all(np.isfinite(out[:, 0, :])), f"call {call}: unwritten results"
-        assert rel_l2(out[:, 0, :3], ref["acc"]) < TOL, f"call {call}"
-        assert rel_l2(out[:, 0, 3], ref["div_v"]) < TOL, f"call {call}"
-        np.testing.assert_allclose(out[:, 1, 0], ref["dt"], rtol=TOL)
+        for chk in (ref, fp64):  # the allocating entry point, then the FP64 oracle
+            assert rel_l2(out[:, 0, :3], chk["acc"]) < TOL, f"call {call}"
+            assert rel_l2(out[:, 0, 3], chk["div_v"]) < TOL, f"call {call}"
+            np.testing.assert_allclose(out[:, 1, 0], chk["dt"], rtol=TOL)
 
 
 def test_noalloc_rejects_oversized_batches(native):

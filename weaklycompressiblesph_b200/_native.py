@@ -114,6 +114,7 @@ _SIGS = {
     "wcsph_sim_instance_status": (C.c_int, [P, C.c_int32, F64P, C.POINTER(C.c_int64), I32P, I32P]),
     "wcsph_sim_read_instance": (C.c_int, [P, C.c_int32, F32P, F32P, F32P, F32P, F32P, F32P, I32P]),
     "wcsph_sim_probe_forces": (C.c_int, [P, C.c_int32, C.c_int32, F32P, F32P, F32P, F32P, I32P]),
+    "wcsph_sim_probe_lists": (C.c_int, [P, C.c_int32, C.c_int32, F32P, F32P, F32P, F32P, I32P]),
     "wcsph_sim_read_order": (C.c_int, [P, C.c_int32, I32P, U32P]),
     "wcsph_sim_conservation": (C.c_int, [P, C.c_int32, F64P]),
     "wcsph_sim_last_pairs": (C.c_int64, [P]),
@@ -121,6 +122,7 @@ _SIGS = {
     "wcsph_sim_stream": (C.c_void_p, [P]),
     "wcsph_sim_list_stats": (C.c_int, [P, C.POINTER(C.c_int64)]),
     "wcsph_sim_tuning": (C.c_int, [P, I32P]),
+    "wcsph_sim_invalidate_lists": (C.c_int, [P]),
     "wcsph_sim_profile_steps": (C.c_int, [P, C.c_int32, F64P]),
 }
 

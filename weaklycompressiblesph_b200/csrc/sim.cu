@@ -1217,24 +1217,13 @@ int wcsph_sim_read_instance(wcsph_sim* sim, int32_t slot, float* pos3, float* ve
   return 0;
 }
 
-int wcsph_sim_probe_forces(wcsph_sim* sim, int32_t slot, int32_t density_pass, float* acc3, float* div_v, float* dt_i,
-                           float* dens_out, int32_t* n_neighbors) {
-  if (!sim || density_pass < 0 || density_pass > 2) return WCSPH_E_INVALID;
-  SimImpl& S = sim->impl;
-  if (slot < 0 || slot >= (int)S.inst.size() || !S.inst[slot].active) {
-    set_error("wcsph_sim_probe_forces: slot %d is not active", slot);
-    return WCSPH_E_INVALID;
-  }
-  WCSPH_CUDA(cudaSetDevice(S.opt.device));
-  for (size_t q = 0; q < S.inst.size(); ++q) S.h_phase[q] = PH_IDLE;
-  S.h_phase[slot] = PH_PROBE;
-  if (int rc = upload_tables(S)) return rc;
-  StepArgs a = make_args(S);
-  a.probe_density = density_pass;
-  int rc = enqueue_pass(S, a, density_pass != 0, false, nullptr);
-  int rc2 = set_all_phases(S, PH_STEP);
-  if (rc) return rc;
-  if (rc2) return rc2;
+}  // extern "C"
+
+namespace wcsph {
+
+// The diagnostic arrays of a probe pass over instance slot, in original order.
+static int read_probe(SimImpl& S, int slot, float* acc3, float* div_v, float* dt_i, float* dens_out,
+                      int32_t* n_neighbors) {
   WCSPH_CUDA(cudaStreamSynchronize(S.s));
   InstDyn d;
   WCSPH_CUDA(cudaMemcpy(&d, S.d_dyn + slot, sizeof(InstDyn), cudaMemcpyDeviceToHost));
@@ -1259,8 +1248,104 @@ int wcsph_sim_probe_forces(wcsph_sim* sim, int32_t slot, int32_t density_pass, f
     if (dens_out) dens_out[i] = drho[q];
     if (n_neighbors) n_neighbors[i] = dn[q];
   }
-  S.graph_dirty = true;
   return 0;
+}
+
+// Probe passes over the neighbour lists (sim_list.cuh) of the current build,
+// with the probed instance in PH_PROBE and every other one idle: the list
+// step's refresh without its kick (j-records from the current state), the
+// density pass from the lists when asked, and the list pass, whose epilogue
+// writes the diagnostic arrays.  Positions, order and lists are untouched.
+static int enqueue_probe_lists(SimImpl& S, int density_pass) {
+  StepArgs a = make_args(S);
+  a.probe_density = density_pass;
+  a.list_reuse = 1;
+  a.x0 = S.x0;
+  a.alt = a.main;
+  const int n = S.n_host;
+  WCSPH_CUDA(cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s));
+  WCSPH_CUDA(cudaMemsetAsync(S.d_counters + 4, 0, sizeof(int), S.s));
+  k_step_begin<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
+  if (n > 0) {
+    k_kick_refresh<<<nblk(n), kBlock, 0, S.s>>>(a);
+    if (density_pass) {
+      if (int rc = launch_density_list(a, n, S.s)) return rc;
+      k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
+    }
+    const bool h16 = S.opt.precision == WCSPH_PREC_HALF2;
+    if (int rc = h16 ? launch_hydro_list<true>(a, n, S.s) : launch_hydro_list<false>(a, n, S.s)) return rc;
+  }
+  WCSPH_CUDA(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace wcsph
+
+extern "C" {
+
+int wcsph_sim_probe_forces(wcsph_sim* sim, int32_t slot, int32_t density_pass, float* acc3, float* div_v, float* dt_i,
+                           float* dens_out, int32_t* n_neighbors) {
+  if (!sim || density_pass < 0 || density_pass > 2) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  if (slot < 0 || slot >= (int)S.inst.size() || !S.inst[slot].active) {
+    set_error("wcsph_sim_probe_forces: slot %d is not active", slot);
+    return WCSPH_E_INVALID;
+  }
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  for (size_t q = 0; q < S.inst.size(); ++q) S.h_phase[q] = PH_IDLE;
+  S.h_phase[slot] = PH_PROBE;
+  if (int rc = upload_tables(S)) return rc;
+  StepArgs a = make_args(S);
+  a.probe_density = density_pass;
+  int rc = enqueue_pass(S, a, density_pass != 0, false, nullptr);
+  int rc2 = set_all_phases(S, PH_STEP);
+  if (rc) return rc;
+  if (rc2) return rc2;
+  S.graph_dirty = true;
+  return read_probe(S, slot, acc3, div_v, dt_i, dens_out, n_neighbors);
+}
+
+int wcsph_sim_probe_lists(wcsph_sim* sim, int32_t slot, int32_t density_pass, float* acc3, float* div_v, float* dt_i,
+                          float* dens_out, int32_t* n_neighbors) {
+  if (!sim || density_pass < 0 || density_pass > 2) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  if (S.opt.list_interval <= 0) {
+    set_error("wcsph_sim_probe_lists: the solver has no neighbour lists (list_interval = 0)");
+    return WCSPH_E_STATE;
+  }
+  if (slot < 0 || slot >= (int)S.inst.size() || !S.inst[slot].active) {
+    set_error("wcsph_sim_probe_lists: slot %d is not active", slot);
+    return WCSPH_E_INVALID;
+  }
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  if (S.appended && S.n_host > 0) {
+    set_error("wcsph_sim_probe_lists: particles were appended since the last pass; step first");
+    return WCSPH_E_STATE;
+  }
+  for (size_t q = 0; q < S.inst.size(); ++q) S.h_phase[q] = PH_IDLE;
+  S.h_phase[slot] = PH_PROBE;
+  if (int rc = upload_tables(S)) return rc;
+  int rc = 0;
+  if (S.lists_valid) {
+    rc = enqueue_probe_lists(S, density_pass);
+  } else {
+    // No current lists: a build pass in probe phase (binning at the current
+    // positions, the scan writes the lists, the list pass sums them).  Its
+    // lists serve the steps that follow like those of a step's build.
+    StepArgs a = make_args(S);
+    a.probe_density = density_pass;
+    rc = enqueue_pass(S, a, density_pass != 0, false, nullptr, nullptr, true);
+    if (!rc) {
+      S.lists_valid = true;
+      S.since_build = 0;
+      S.last_disp = 0.f;
+      S.graph_dirty = true;
+    }
+  }
+  int rc2 = set_all_phases(S, PH_STEP);
+  if (rc) return rc;
+  if (rc2) return rc2;
+  return read_probe(S, slot, acc3, div_v, dt_i, dens_out, n_neighbors);
 }
 
 int wcsph_sim_read_order(wcsph_sim* sim, int32_t slot, int32_t* perm, uint32_t* cell_key) {
@@ -1332,6 +1417,12 @@ int wcsph_sim_list_stats(wcsph_sim* sim, int64_t* out6) {
   out6[3] = (int64_t)mx;
   out6[4] = S.kernels_per_step;
   out6[5] = S.kernels_reuse;
+  return 0;
+}
+
+int wcsph_sim_invalidate_lists(wcsph_sim* sim) {
+  if (!sim) return WCSPH_E_INVALID;
+  sim->impl.lists_valid = false;
   return 0;
 }
 

@@ -1,7 +1,8 @@
-// Conservation sums of one instance, accumulated in FP64 on the device:
-// out[0] total mass, out[1..3] momentum, out[4] kinetic energy, out[5] |sum m a|^2
-// is not meaningful per axis, so out[5] holds sum m (a_z + g) (the vertical
-// momentum change rate from the pair forces; zero for a closed system).
+// Conservation sums of one instance's live particles, accumulated in FP64 on
+// the device: out[0] total mass, out[1..3] momentum, out[4] kinetic energy,
+// out[5] sum m (a_z + g), the vertical component of the pair forces' total
+// (gravity taken out): zero up to rounding, since every pair term enters the
+// sums of i and j with opposite signs (force.h:38-57).
 #pragma once
 #include "sim_kernels.cuh"
 
@@ -12,7 +13,9 @@ __global__ void k_conservation(SimArrays A, const InstDyn* dyn, const InstParams
   const double m = params[slot].mass, g = params[slot].g;
   double s[6] = {0, 0, 0, 0, 0, 0};
   for (int p = lo + blockIdx.x * blockDim.x + threadIdx.x; p < hi; p += gridDim.x * blockDim.x) {
-    if (A.flags[p] & kGhostBit) continue;  // a slab's ghost copies belong to their owner's sums
+    // a slab's ghost copies belong to their owner's sums; particles removed
+    // since the last neighbour-list build stay in place until the next one
+    if (A.flags[p] & (kGhostBit | kDeadBit)) continue;
     const float4 v = A.vel[p];
     const float4 a = A.acc[p];
     s[0] += m;

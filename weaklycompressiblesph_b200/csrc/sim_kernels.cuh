@@ -121,8 +121,20 @@ __global__ void k_step_begin(StepArgs a) {
 }
 
 // ------------------------------------------------------- kick + binning
-// KDK first half (class.h:146-159 as main.cpp:98-103 runs it), periodic wrap,
-// escapee removal (Dam2.h:117-122), then the Morton cell key of each particle.
+// Periodic wrap of a position into [lo, lo + L) (one rounded FP32 operation
+// per axis); true when a coordinate moved.
+__device__ __forceinline__ bool wrap_periodic(const InstParams& P, float4& x) {
+  bool moved = false;
+  float* c = &x.x;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float hi = P.lo[k] + P.L[k];
+    if (c[k] >= hi) c[k] = __fsub_rn(c[k], P.L[k]), moved = true;
+    else if (c[k] < P.lo[k]) c[k] = __fadd_rn(c[k], P.L[k]), moved = true;
+  }
+  return moved;
+}
+
 // KDK first half of one live particle p of a stepping instance
 // (class.h:146-159 as main.cpp:98-103 runs it), periodic wrap (not on list
 // steps), escapee removal (Dam2.h:117-122).  Returns true when the state
@@ -146,15 +158,7 @@ __device__ __forceinline__ bool kick_particle(const StepArgs& a, const InstParam
     if (a.list_flags && P.inv_skin > 0.0f)
       drift_bits = __float_as_uint(dt * sqrtf(vh.x * vh.x + vh.y * vh.y + vh.z * vh.z) * P.inv_skin);
     v = make_float4(v.x + dt * acc.x, v.y + dt * acc.y, v.z + dt * acc.z, 0.f);
-    if (P.periodic && !a.list_reuse) {  // between list builds positions run on continuously
-      float* c = &x.x;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const float hi = P.lo[k] + P.L[k];
-        if (c[k] >= hi) c[k] = __fsub_rn(c[k], P.L[k]);
-        else if (c[k] < P.lo[k]) c[k] = __fadd_rn(c[k], P.L[k]);
-      }
-    }
+    if (P.periodic && !a.list_reuse) wrap_periodic(P, x);  // between list builds positions run on continuously
     if (P.kill_on) {
       const float* c = &x.x;
 #pragma unroll
@@ -172,7 +176,9 @@ __device__ __forceinline__ void list_flag_max(unsigned* word, unsigned bits) {
   if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && mx) atomicMax(word, mx);
 }
 
-// The kick, then the Morton cell key of each particle.
+// The kick, the periodic wrap (every binning pass: positions run on
+// continuously between neighbour-list builds), then the Morton cell key of
+// each particle.
 __global__ void k_kick_bin(StepArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.n_host) return;
@@ -184,7 +190,11 @@ __global__ void k_kick_bin(StepArgs a) {
   float4 v = a.main.vel[p];
   float4 vh = v;
   unsigned drift_bits = 0u;
-  if (!dead && kick_particle(a, P, inst, p, f, x, v, vh, dead, drift_bits)) {
+  bool changed = !dead && kick_particle(a, P, inst, p, f, x, v, vh, dead, drift_bits);
+  // passes without a kick (probe, initial and binning passes) wrap too, so
+  // that positions left outside the box by list steps are binned correctly
+  if (!dead && !changed && P.periodic && wrap_periodic(P, x)) changed = true;
+  if (changed) {
     a.main.pos[p] = x;
     a.main.vel[p] = v;
   }

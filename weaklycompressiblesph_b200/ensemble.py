@@ -11,7 +11,7 @@ import numpy as np
 from . import _native as N
 from .sim import Solver
 
-PRECISIONS = {"fp32": N.PREC_FP32, "tiled": N.PREC_TILED}
+PRECISIONS = {"fp32": N.PREC_FP32, "tiled": N.PREC_TILED, "half2": N.PREC_HALF2}
 
 
 def _sync_time(solver, fn):
@@ -22,10 +22,11 @@ def _sync_time(solver, fn):
     return time.perf_counter() - t0
 
 
-def run_batched(cases, steps, precision="tiled", warmup=3, device=0, list_interval=0):
+def run_batched(cases, steps, precision="tiled", warmup=3, device=0, list_interval=0, read=False):
     """Step all cases together; returns dict with wall seconds for `steps`
-    steps, particle-steps/s and per-instance status.  list_interval > 0 uses
-    neighbour lists (see Solver)."""
+    steps, particle-steps/s and per-instance status (and, with read=True, each
+    instance's final state).  list_interval > 0 uses neighbour lists (see
+    Solver)."""
     total = sum(c.n for c in cases)
     with Solver(total + 1024, precision=PRECISIONS[precision], max_instances=len(cases) + 1, device=device,
                 list_interval=list_interval) as s:
@@ -33,21 +34,27 @@ def run_batched(cases, steps, precision="tiled", warmup=3, device=0, list_interv
         s.step(warmup)
         el = _sync_time(s, lambda: s.step(steps))
         st = [s.status(k) for k in slots]
+        states = [s.read(k) for k in slots] if read else None
+        lists = s.list_stats() if list_interval else None
     return dict(seconds=el, steps=steps, particles=total, particle_steps_per_s=total * steps / el,
-                status=st, kernels_per_step=None)
+                status=st, states=states, lists=lists)
 
 
-def run_serial(cases, steps, precision="fp32", warmup=3, device=0):
+def run_serial(cases, steps, precision="fp32", warmup=3, device=0, list_interval=0, read=False):
     """The same instances one at a time (each in its own solver)."""
     el = 0.0
     total = 0
+    states = [] if read else None
     for c in cases:
-        with Solver(c.n + 1024, precision=PRECISIONS[precision], max_instances=2, device=device) as s:
-            s.add(c)
+        with Solver(c.n + 1024, precision=PRECISIONS[precision], max_instances=2, device=device,
+                    list_interval=list_interval) as s:
+            k = s.add(c)
             s.step(warmup)
             el += _sync_time(s, lambda: s.step(steps))
             total += c.n
-    return dict(seconds=el, steps=steps, particles=total, particle_steps_per_s=total * steps / el)
+            if read:
+                states.append(s.read(k))
+    return dict(seconds=el, steps=steps, particles=total, particle_steps_per_s=total * steps / el, states=states)
 
 
 def latency_percentiles(seconds):

@@ -111,9 +111,10 @@ class Server:
                     p50_s=float(np.percentile(lat, 50)), p99_s=float(np.percentile(lat, 99)))
 
 
-def run_alone(case, precision=N.PREC_TILED, chunk_steps=25, device=0):
+def run_alone(case, precision=N.PREC_TILED, chunk_steps=25, device=0, list_interval=0):
     """One request by itself, stepped to t_end; returns (seconds, steps, result)."""
-    with Solver(case.n + 1024, precision=precision, max_instances=2, device=device) as s:
+    with Solver(case.n + 1024, precision=precision, max_instances=2, device=device,
+                list_interval=list_interval) as s:
         k = s.add(case, t_end=case.t_end)
         s.synchronize()
         t0 = time.perf_counter()

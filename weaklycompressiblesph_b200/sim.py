@@ -171,13 +171,16 @@ class Solver:
                N.ptr(out["alive"], C.c_int32))
         return out
 
-    def probe(self, slot, density_pass=0):
+    def probe(self, slot, density_pass=0, lists=False):
         """Force pass on the current state without advancing it (original order).
-        Returns acc (hydro only, no gravity), div_v, dt_i, dens used, neighbour counts."""
+        Returns acc (hydro only, no gravity), div_v, dt_i, dens used, neighbour counts.
+        lists=True runs the passes of a neighbour-list step (wcsph_sim_probe_lists)
+        instead of a fresh cell search."""
         n = self.slots[slot].n
         out = dict(acc=np.zeros((n, 3), np.float32), div_v=np.zeros(n, np.float32), dt=np.zeros(n, np.float32),
                    dens=np.zeros(n, np.float32), nbr=np.zeros(n, np.int32))
-        N.call("wcsph_sim_probe_forces", self._h, slot, int(density_pass), N.ptr(out["acc"], C.c_float),
+        fn = "wcsph_sim_probe_lists" if lists else "wcsph_sim_probe_forces"
+        N.call(fn, self._h, slot, int(density_pass), N.ptr(out["acc"], C.c_float),
                N.ptr(out["div_v"], C.c_float), N.ptr(out["dt"], C.c_float), N.ptr(out["dens"], C.c_float),
                N.ptr(out["nbr"], C.c_int32))
         return out
@@ -217,6 +220,10 @@ class Solver:
         N.call("wcsph_sim_list_stats", self._h, out)
         return dict(builds=int(out[0]), list_steps=int(out[1]), overflows=int(out[2]), longest=int(out[3]),
                     kernels_build=int(out[4]), kernels_list=int(out[5]))
+
+    def invalidate_lists(self):
+        """The next step rebuilds the neighbour lists (wcsph_sim_invalidate_lists)."""
+        N.call("wcsph_sim_invalidate_lists", self._h)
 
     def profile_steps(self, nsteps):
         """Advance nsteps eagerly with CUDA events per phase; returns ms summed
