@@ -344,8 +344,13 @@ int32_t wcsph_sim_kernels_per_step(wcsph_sim* sim);
 /* The autotuner's current choice: out[0] block shape of the tiled hydro
  * kernel (0: 4 warps, 1: 2 warps, 2: 8 warps per block, 512-candidate tiles;
  * the shapes share their arithmetic, so results do not depend on the choice),
- * out[1] density kernel (always 0: per-thread), out[2] log2 particle bucket it
- * was tuned for (-1: defaults, not tuned). */
+ * out[1] launch shape of the neighbour-list pass (list_interval > 0; 0: one
+ * thread per particle, 5 blocks of 128 per SM; 1: two threads per particle,
+ * each taking alternate groups of four list entries, 4 blocks per SM; 2: one
+ * thread per particle, 4 blocks per SM; 3: two threads per particle, 5 blocks
+ * per SM.  Shapes 0 and 2 sum in one order, 1 and 3 in another: results
+ * agree to FP32 rounding), out[2] log2 particle bucket it was tuned for (-1:
+ * defaults, not tuned). */
 int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out3);
 /* Neighbour-list counters (list_interval > 0): out[0] list builds, out[1]
  * steps that read the lists, out[2] builds whose lists overflowed (the next

@@ -870,10 +870,10 @@ int wcsph_filter_retrieve(int32_t tag, int32_t n_walk, const int32_t* n_i, void*
 // ---------------------------------------------------------------------------
 // Allocation-free walk pair sum.
 //
-// For callers that cannot allocate device memory: code running while a CUDA
-// graph is being captured (a cudaMalloc there breaks the capture), hosts that
-// hand the plugin a fixed memory budget and forbid growth, and embedders whose
-// allocator owns every device byte.  The caller passes device-resident inputs
+// For callers that cannot allocate device memory: hosts that hand the plugin a
+// fixed memory budget and forbid growth, embedders whose allocator owns every
+// device byte, and host loops in which a cudaMalloc would synchronise the
+// device in the middle of a step.  The caller passes device-resident inputs
 // and outputs; the only scratch this path needs, the per-walk displacement
 // tables (exclusive prefix sums of the walk sizes), lives in the file-scope
 // array below, sized for WCSPH_NOALLOC_MAX_WALKS walks (about 512 KB, held on

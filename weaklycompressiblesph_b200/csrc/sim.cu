@@ -72,6 +72,7 @@ struct SimImpl {
   long long total_cells = 0;
   bool any_density = false;
   int tile_shape = 0;          // tiled pair-kernel shape, chosen by the autotuner
+  int list_shape = 0;          // list-pass launch shape (kListShapes), chosen by the autotuner
   int tuned_bucket = -1;       // log2 particle bucket of the last tuning
   cudaGraphExec_t gexec = nullptr;
   bool graph_dirty = true;
@@ -250,7 +251,9 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
       if (int rc = h16 ? launch_hydro_tiled<true, true>(a, n, S.s, S.tile_shape)
                        : launch_hydro_tiled<false, true>(a, n, S.s, S.tile_shape))
         return rc;
-      if (int rc = h16 ? launch_hydro_list<true>(a, n, S.s) : launch_hydro_list<false>(a, n, S.s)) return rc;
+      if (int rc = h16 ? launch_hydro_list<true>(a, n, S.s, S.list_shape)
+                       : launch_hydro_list<false>(a, n, S.s, S.list_shape))
+        return rc;
       ++L;
     } else if (S.opt.precision == WCSPH_PREC_TILED) {
       if (int rc = launch_hydro_tiled<false>(a, n, S.s, S.tile_shape)) return rc;
@@ -297,9 +300,9 @@ static int enqueue_reuse(SimImpl& S, StepArgs a, bool density, int* launches, cu
     }
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[2], S.s));
     if (S.opt.precision == WCSPH_PREC_HALF2) {
-      if (int rc = launch_hydro_list<true>(a, n, S.s)) return rc;
+      if (int rc = launch_hydro_list<true>(a, n, S.s, S.list_shape)) return rc;
     } else {
-      if (int rc = launch_hydro_list<false>(a, n, S.s)) return rc;
+      if (int rc = launch_hydro_list<false>(a, n, S.s, S.list_shape)) return rc;
     }
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[3], S.s));  // the dead tail stays in place
@@ -371,6 +374,29 @@ static int autotune(SimImpl& S) {
     if (ms < best) best = ms, best_shape = v;
   }
   S.tile_shape = best_shape;
+  if (S.opt.list_interval > 0) {
+    // The list pass: a probe build pass makes lists of the current state
+    // (they serve the steps that follow), then every launch shape is timed
+    // on them with probe launches (diagnostics only, state untouched).
+    if (int rc = enqueue_pass(S, a, false, false, nullptr, nullptr, true)) return rc;
+    S.lists_valid = true;
+    S.since_build = 0;
+    S.last_disp = 0.f;
+    StepArgs b = make_args(S);
+    b.list_reuse = 1;
+    b.x0 = S.x0;
+    b.alt = b.main;
+    float best_list = 1e30f;
+    int best_list_shape = 0;
+    for (int v = 0; v < kListShapes; ++v) {
+      int rc = time_launches(S, 3, [&]() {
+        return h16 ? launch_hydro_list<true>(b, n, S.s, v) : launch_hydro_list<false>(b, n, S.s, v);
+      }, &ms);
+      if (rc) return rc;
+      if (ms < best_list) best_list = ms, best_list_shape = v;
+    }
+    S.list_shape = best_list_shape;
+  }
   S.tuned_bucket = bucket;
   S.graph_dirty = true;
   return set_all_phases(S, PH_STEP);
@@ -1273,7 +1299,9 @@ static int enqueue_probe_lists(SimImpl& S, int density_pass) {
       k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
     }
     const bool h16 = S.opt.precision == WCSPH_PREC_HALF2;
-    if (int rc = h16 ? launch_hydro_list<true>(a, n, S.s) : launch_hydro_list<false>(a, n, S.s)) return rc;
+    if (int rc = h16 ? launch_hydro_list<true>(a, n, S.s, S.list_shape)
+                     : launch_hydro_list<false>(a, n, S.s, S.list_shape))
+      return rc;
   }
   WCSPH_CUDA(cudaGetLastError());
   return 0;
@@ -1399,7 +1427,7 @@ void* wcsph_sim_stream(wcsph_sim* sim) { return sim ? (void*)sim->impl.s : nullp
 int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out3) {
   if (!sim || !out3) return WCSPH_E_INVALID;
   out3[0] = sim->impl.tile_shape;
-  out3[1] = 0;  // the density pass always uses the per-thread kernel
+  out3[1] = sim->impl.list_shape;
   out3[2] = sim->impl.tuned_bucket;
   return 0;
 }

@@ -131,29 +131,40 @@ __device__ __forceinline__ f2 snds7_2(f2 RHO, f2 RHO0, f2 IRHO0, f2 C0) {
   return pk(fmaxf(fabsf(lo(T)), 1.0e-8f), fmaxf(fabsf(hi(T)), 1.0e-8f));
 }
 
-// The list pass with one thread per particle slot below the build's live
-// count (the particles of the build's cell table; the dead tail is
-// k_copy_dead's), on list steps and right after the scan of a build step:
-// each thread walks its own list row four entries per 16-byte load and sums
-// two entries at a time in the f32x2 halves of pair2, support tested per
-// entry; no shared memory, no cross-lane reduction.  For gamma = 7 the sound
-// speed of j is recomputed from its density (snds7_2, the stored value bit
-// for bit) instead of gathered: one gather per entry fewer.
-template <bool H16>
-__global__ void __launch_bounds__(128, 5) k_hydro_list(StepArgs a) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+// The list pass over particle slots below the build's live count (the
+// particles of the build's cell table; the dead tail is k_copy_dead's), on
+// list steps and right after the scan of a build step: TPI threads per
+// particle walk its list row, each taking every TPI-th group of four entries
+// (one 16-byte load), and sum two entries at a time in the f32x2 halves of
+// pair2, support tested per entry; the TPI partial sums are combined with
+// shuffles, and no shared memory is used.  For gamma = 7 the sound speed of j
+// is recomputed from its density (snds7_2, the stored value bit for bit)
+// instead of gathered: one gather per entry fewer.  MINB is the launch
+// bound's blocks per SM (it sets the register budget).  With TPI = 1 every
+// sum runs in list order; TPI = 2 changes the summation order (the results
+// agree to FP32 rounding).
+template <bool H16, int TPI, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_hydro_list(StepArgs a) {
+  const unsigned full = 0xffffffffu;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = t / TPI, sub = t % TPI;
   float dt_cand = 0.f;
   bool dt_valid = false;
   int inst = 0;
   unsigned owned = 0;
+  bool work = false;
+  uint32_t fp = 0;
+  float sx = 0.f, sy = 0.f, sz = 0.f, sd = 0.f, sv = 0.f;
+  unsigned scnt = 0;
   if (p < *a.n_alive) {
-    const uint32_t fp = a.alt.flags[p];
+    fp = a.alt.flags[p];
     inst = fp & kInstMask;
     const InstParams& P = a.params[inst];
     const int ph = a.phase[inst];
     if ((fp & kDeadBit) || !wants_force(P, a.dyn[inst], ph)) {
-      copy_state(a, p);
+      if (sub == 0) copy_state(a, p);
     } else {
+      work = true;
       const JRec R = a.jr[p];
       PairI I;
       I.X = dup(R.a.x), I.Y = dup(R.a.y), I.Z = dup(R.a.z), I.PO = dup(R.a.w);
@@ -169,7 +180,7 @@ __global__ void __launch_bounds__(128, 5) k_hydro_list(StepArgs a) {
       f2 AX = 0ull, AY = 0ull, AZ = 0ull, DS = 0ull;
       float vsa = 0.f, vsb = 0.f;
       unsigned ca = 0, cb = 0;
-      if (cnt_build > a.list_max) {
+      if (cnt_build > a.list_max && sub == 0) {
         // The list overflowed at this step's build (the host rebuilds at the
         // next step, so no list step ever sees it): sum over the cell search
         // of the build's cell table instead, one j at a time.
@@ -182,7 +193,7 @@ __global__ void __launch_bounds__(128, 5) k_hydro_list(StepArgs a) {
                             ++ca;
                           });
       }
-      for (int k = 0; k < n; k += 4) {
+      for (int k = 4 * sub; k < n; k += 4 * TPI) {
         const uint4 e = __ldg(&row[k >> 2]);
         const uint32_t e0 = e.x, e1 = k + 1 < n ? e.y : self, e2 = k + 2 < n ? e.z : self, e3 = k + 3 < n ? e.w : self;
         const int g0 = e0 & kSlotMask, g1 = e1 & kSlotMask, g2 = e2 & kSlotMask, g3 = e3 & kSlotMask;
@@ -199,21 +210,48 @@ __global__ void __launch_bounds__(128, 5) k_hydro_list(StepArgs a) {
         pair2<H16, true>(P, C, I, R2, R3, e2 >> 27, e3 >> 27, C23, k + 2 < n, k + 3 < n, AX, AY, AZ, DS, vsa, vsb,
                          ca, cb);
       }
-      const unsigned cnt = ca + cb;
-      if (!(fp & kGhostBit)) owned = cnt;  // owned particles only
-      finish_hydro(a, p, P, inst, ph, fp, lo(AX) + hi(AX), lo(AY) + hi(AY), lo(AZ) + hi(AZ), lo(DS) + hi(DS),
-                   fmaxf(vsa, vsb), cnt, dt_cand, dt_valid);
+      sx = lo(AX) + hi(AX), sy = lo(AY) + hi(AY), sz = lo(AZ) + hi(AZ), sd = lo(DS) + hi(DS);
+      sv = fmaxf(vsa, vsb);
+      scnt = ca + cb;
     }
   }
+#pragma unroll
+  for (int o = 1; o < TPI; o <<= 1) {  // every lane takes part; a particle's TPI lanes are adjacent
+    sx += __shfl_xor_sync(full, sx, o);
+    sy += __shfl_xor_sync(full, sy, o);
+    sz += __shfl_xor_sync(full, sz, o);
+    sd += __shfl_xor_sync(full, sd, o);
+    sv = fmaxf(sv, __shfl_xor_sync(full, sv, o));
+    scnt += __shfl_xor_sync(full, scnt, o);
+  }
+  if (work && sub == 0) {
+    const InstParams& P = a.params[inst];
+    if (!(fp & kGhostBit)) owned = scnt;  // owned particles only
+    finish_hydro(a, p, P, inst, a.phase[inst], fp, sx, sy, sz, sd, sv, scnt, dt_cand, dt_valid);
+  }
   dt_min(a.dyn, inst, dt_cand, dt_valid);
-  const unsigned tot = __reduce_add_sync(0xffffffffu, owned);
+  const unsigned tot = __reduce_add_sync(full, owned);
   if ((threadIdx.x & 31) == 0 && tot) atomicAdd(a.pair_count, (unsigned long long)tot);
 }
 
+// Launch shapes of the list pass the autotuner chooses among: (threads per
+// particle, blocks per SM of the launch bound).  Shapes 0 and 2 sum in one
+// order (bit-identical results), shapes 1 and 3 in another.
+constexpr int kListShapes = 4;
+constexpr int kListShapeTPI[kListShapes] = {1, 2, 1, 2};
+constexpr int kListShapeMINB[kListShapes] = {5, 4, 4, 5};
+
 template <bool H16>
-inline int launch_hydro_list(const StepArgs& a, int n, cudaStream_t s) {
+inline int launch_hydro_list(const StepArgs& a, int n, cudaStream_t s, int shape = 0) {
   if (n <= 0) return 0;
-  k_hydro_list<H16><<<(n + 127) / 128, 128, 0, s>>>(a);
+  const long long threads = (long long)n * kListShapeTPI[shape < 0 || shape >= kListShapes ? 0 : shape];
+  const int grid = (int)((threads + 127) / 128);
+  switch (shape) {
+    case 1: k_hydro_list<H16, 2, 4><<<grid, 128, 0, s>>>(a); break;
+    case 2: k_hydro_list<H16, 1, 4><<<grid, 128, 0, s>>>(a); break;
+    case 3: k_hydro_list<H16, 2, 5><<<grid, 128, 0, s>>>(a); break;
+    default: k_hydro_list<H16, 1, 5><<<grid, 128, 0, s>>>(a); break;
+  }
   WCSPH_CUDA(cudaGetLastError());
   return 0;
 }

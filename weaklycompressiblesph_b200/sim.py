@@ -206,10 +206,10 @@ class Solver:
         return int(N.lib().wcsph_sim_kernels_per_step(self._h))
 
     def tuning(self):
-        """Autotuner decision: tile shape, density kernel (0 per-thread, 1 tiled), tuned bucket."""
+        """Autotuner decision: tiled-kernel block shape, list-pass launch shape, tuned bucket."""
         out = np.zeros(3, np.int32)
         N.call("wcsph_sim_tuning", self._h, N.ptr(out, C.c_int32))
-        return dict(tile_shape=int(out[0]), density_tiled=bool(out[1]), bucket=int(out[2]))
+        return dict(tile_shape=int(out[0]), list_shape=int(out[1]), bucket=int(out[2]))
 
     def stream(self):
         """The solver's cudaStream_t as an integer handle."""
