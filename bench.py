@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--e2e-only", action="store_true",
                     help="time only the FDPS drop-in pass (dispatch + retrieve from host records), --steps passes")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison run")
+    ap.add_argument("--no-other-precision", action="store_true",
+                    help="skip the run of the other list-mode precision (half2 beside FP32, or the reverse)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble and serving samples")
     ap.add_argument("--ensemble-steps", type=int, default=60)
     ap.add_argument("--no-cpu", action="store_true")
@@ -535,6 +537,17 @@ def main():
             q = run_device(case, prec, args.steps, args.warmup, local)
             search = {"value": q["pairs_per_step"] / (q["ms_per_step"] * 1e-3), "steps_per_s": 1e3 / q["ms_per_step"],
                       "ms_per_step": q["ms_per_step"], "hydro_ms": q["phase_ms"][2]}
+    other = None
+    if not args.no_other_precision and not slab_mode and prec in ("tiled", "half2"):
+        oprec = "half2" if prec == "tiled" else "tiled"
+        o = run_device(case, oprec, args.steps, args.warmup, local, list_interval=args.list_interval,
+                       list_skin=args.list_skin)
+        other = {"precision": oprec, "value": o["pairs_per_step"] / (o["ms_per_step"] * 1e-3),
+                 "steps_per_s": 1e3 / o["ms_per_step"], "ms_per_step": o["ms_per_step"],
+                 "hydro_ms": o["phase_ms"][2], "lists": o.get("lists"), "tuning": o.get("tuning")}
+        if plain:
+            other["speedup_vs_plain_fp32"] = other["steps_per_s"] / plain["steps_per_s"]
+        other["error_vs_fp64"] = validation_errors(args.workload, oprec)
     peak, peak_kind = load_peaks()
     hydro_ms = dev["phase_ms"][2]
     bpp = BYTES_PER_PAIR[prec]
@@ -546,6 +559,7 @@ def main():
             t = json.load(f)
         key = f"{args.workload}/{prec}" + ("/lists" if dev.get("lists") else "")
         traffic = t.get(key, {}).get("bytes_per_launch")
+    l1 = l1_roofline(args.workload, prec, dev)
     e2e = None
     cpu = None
     if rank == 0 and not args.no_e2e and args.workload != "periodic8m":
@@ -575,7 +589,9 @@ def main():
         "steps_per_s": steps_per_s * 1.0,
         "pairs_per_step": dev["pairs_per_step"],
         "plain_fp32": plain,
+        "speedup_vs_plain_fp32": (steps_per_s / plain["steps_per_s"]) if plain else None,
         "search_every_step": search,
+        ("half2" if other and other["precision"] == "half2" else "fp32_tiled"): other,
         "phase_ms": {"bin_sort_permute": dev["phase_ms"][0], "density": dev["phase_ms"][1],
                      "hydro": dev["phase_ms"][2], "total": dev["phase_ms"][3]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -583,6 +599,8 @@ def main():
                      "model": f"{bpp} B per true pair (j-record) / hydro kernel time"
                               + (" (build and list steps averaged)" if dev.get("lists") else ""),
                      "peak_kind": peak_kind},
+        "roofline_l1": l1,
+        "error_vs_fp64": validation_errors(args.workload, prec),
         "cpu_baseline": cpu,
         "e2e": e2e,
         "autotune": dev.get("tuning"),
@@ -600,6 +618,47 @@ def main():
     barrier(pg)
     finish(pg)
     return 0
+
+
+def _profile_json(name):
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f)
+
+
+def validation_errors(workload, prec):
+    """Relative L2 errors against the FP64 oracle of the same path, from the
+    committed summary of tests/validate_dam_break.py (largest over its
+    checkpoints), or None when that path was not validated on this workload."""
+    v = _profile_json("validation_dam1m.json")
+    if not v or workload != "dam1m":
+        return None
+    path = {"tiled": "tiled_lists", "half2": "half2_lists", "fp32": None}.get(prec)
+    r = v.get("paths", {}).get(path)
+    if not r:
+        return None
+    return {"acc": r["max_acc"], "div_v": r["max_div_v"], "drho_dt": r["max_drho_dt"], "checkpoints": r["checkpoints"],
+            "steps": v["steps"], "source": "tests/validate_dam_break.py (profiles/validation_dam1m.md)"}
+
+
+def l1_roofline(workload, prec, dev):
+    """The list pass is bound by the L1 data pipe that delivers its j-record
+    gathers: L1 wavefronts per true pair from one ncu capture of the pass,
+    against the minimum its record and list-entry bytes need at 128 B per
+    wavefront (profiles/hydro_list_l1.json)."""
+    t = _profile_json("hydro_list_l1.json")
+    if not t or not dev.get("lists"):
+        return None
+    r = t.get(f"{workload}/{prec}")
+    if not r:
+        return None
+    return {"bound": "l1", "wavefronts_per_pair": r["wavefronts"] / r["pairs"],
+            "min_wavefronts_per_pair": r["entries"] * r["bytes_per_entry"] / 128.0 / r["pairs"],
+            "frac": (r["entries"] * r["bytes_per_entry"] / 128.0) / r["wavefronts"],
+            "l1_pipe_util": r.get("l1_pipe_util"), "bytes_per_entry": r["bytes_per_entry"],
+            "source": "ncu capture summarised in profiles/hydro_list_l1.json"}
 
 
 def bench_config(args, case, prec, world):

@@ -122,6 +122,15 @@ int wcsph_hydro_dispatch(int32_t tag, int32_t n_walk, const void* const* epi, co
  * writes acc, dt and div_v of n_i[w] RESULT records at force[w]. */
 int wcsph_hydro_retrieve(int32_t tag, int32_t n_walk, const int32_t* n_i, void* const* force);
 
+/* Transfer figures of the last dispatch with this tag (no counterpart in the
+ * reference; src/kernel.cu:370-373,388 copy fixed-size half records):
+ * out[0] bytes copied host to device (walk records, displacements, work
+ * list), out[1] bytes copied device to host (results), out[2] pieces of the
+ * batch staged compactly (36-byte records: every record of the piece carried
+ * the same h, nu and m, which then travel once, as src/kernel.cu:303-304
+ * hoists them), out[3] pieces in all (the rest used 48-byte records). */
+int wcsph_fdps_stats(int32_t tag, int64_t* out4);
+
 /* Allocation-free walk pair sum.  No counterpart in the reference: it is for
  * callers that cannot allocate device memory, such as an application that owns
  * all device memory through its own pool allocator or runs under a fixed

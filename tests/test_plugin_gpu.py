@@ -124,3 +124,41 @@ def test_error_behaviour(native):
     _, _, out_l = fdps.split_walks(w, epi, epj, out)
     fdps.HydrRetrieveKernel(0, w.n_walk, np.diff(w.i_off), out_l)
     assert np.all(np.isfinite(out["acc"]))
+
+
+def fdps_stats(tag=0):
+    import ctypes as C
+    out = (C.c_int64 * 4)()
+    N.call("wcsph_fdps_stats", tag, out)
+    return dict(h2d=int(out[0]), d2h=int(out[1]), compact=int(out[2]), pieces=int(out[3]))
+
+
+def test_compact_staging(native, oracle_lib):
+    """A piece of the batch whose records all carry the same h, nu and m is
+    staged in 36-byte records, the others in 48-byte ones: both give the
+    oracle's sums, and the compact pieces give the same bits as when every
+    piece is compact."""
+    case = small_dam(dx=0.04, seed=13)
+    w, epi, epj = walk_setup(case, group_size=16)
+    assert w.n_walk >= 256  # four pieces
+    pair = fdps.pair_params("reference_gpu")
+    ref_pair = oracle_pair(oracle_lib, pair)
+    a = run_plugin(w, epi, epj, pair)
+    sa = fdps_stats()
+    assert sa["pieces"] == 4 and sa["compact"] == 4
+    ref = oracle_lib.hydro_walks(w.i_off, epi, w.j_off, epj, ref_pair)
+    assert rel_l2(a["acc"], ref["acc"]) < TOL and rel_l2(a["div_v"], ref["div_v"]) < TOL
+    np.testing.assert_allclose(a["dt"], ref["dt"], rtol=TOL)
+    # one j-record of the last walk with another viscosity: its piece (the
+    # last quarter of the walks) goes back to 48-byte records
+    epj2 = epj.copy()
+    epj2["visc"][w.j_off[-2]] *= 1.5
+    b = run_plugin(w, epi, epj2, pair)
+    sb = fdps_stats()
+    assert sb["pieces"] == 4 and sb["compact"] == 3
+    assert sb["h2d"] > sa["h2d"]
+    ref2 = oracle_lib.hydro_walks(w.i_off, epi, w.j_off, epj2, ref_pair)
+    assert rel_l2(b["acc"], ref2["acc"]) < TOL and rel_l2(b["div_v"], ref2["div_v"]) < TOL
+    first = w.i_off[(w.n_walk * 3) // 4]  # the i-records of the three compact pieces
+    np.testing.assert_array_equal(a["acc"][:first], b["acc"][:first])
+    np.testing.assert_array_equal(a["dt"][:first], b["dt"][:first])

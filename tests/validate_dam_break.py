@@ -92,6 +92,7 @@ def main():
                     help="also run the tiled and half2 paths with neighbour lists rebuilt at least every K steps "
                          "(0: skip)")
     ap.add_argument("--paths", default="", help="comma-separated subset of the paths (fp32_tiled always runs)")
+    ap.add_argument("--summary", default="", help="also write the largest error of every path as JSON here")
     args = ap.parse_args()
     case = cases.dam_break(dx=args.dx)
     out = {"case": case.name, "particles": case.n, "steps": args.steps}
@@ -120,6 +121,15 @@ def main():
             "max_abs_diff_m": float(np.abs(oi - f32[:, 1]).max()),
             "max_rel_diff_vs_travel": float(np.abs(oi - f32[:, 1]).max() / max(f32[:, 1].max() - col, 1e-9))}
     print(json.dumps(out))
+    if args.summary:
+        summ = {"case": case.name, "particles": case.n, "steps": args.steps, "every": args.every, "paths": {}}
+        for name in res:
+            ch = out[name]["checks"]
+            summ["paths"][name] = {"max_acc": max(c["acc"] for c in ch), "max_div_v": max(c["div_v"] for c in ch),
+                                   "max_drho_dt": max(c["drho_dt"] for c in ch), "checkpoints": len(ch),
+                                   "neighbors_exact": all(c["neighbors_exact"] for c in ch)}
+        with open(args.summary, "w") as f:
+            json.dump(summ, f, indent=1)
 
 
 if __name__ == "__main__":

@@ -56,10 +56,16 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
 // ---------------------------------------------------------- walk kernels
 // Staged records (FP32, 48 B): A = (x, y, z, h) relative to the walk origin,
 // B = (vx, vy, vz, rho), C = (P/rho^2, c, nu, m).  i-records use the same
-// shape (m unused).
+// shape (m unused).  Compact staging (36 B), used for a piece of the batch
+// whose records all carry the same h, nu and m (the reference hoists them
+// from the first particle, src/kernel.cu:303-304,400-401): A = (x, y, z,
+// P/rho^2), B as above, and c alone in the C block; h, nu, m travel in
+// WalkPair.  The kernels rebuild the full records, so both stagings give the
+// same results bit for bit.
 struct WalkPair {
   float alpha, beta, c_cfl, eps;
   int vsig_mode, grad_mode;
+  float h, nu, m;  // compact staging: the piece's uniform h, nu, m
 };
 
 constexpr int kWalkThreads = 128;  // one thread per i; FDPS Ngroup = 128 (param.h:9)
@@ -191,14 +197,30 @@ __device__ __forceinline__ void wq_append2(uint16_t* q, int& n, bool he, bool ho
   n += __popc(me) + __popc(mo);
 }
 
-template <int VSIG, int GRAD>
-__global__ void __launch_bounds__(kWQWarps * 32) k_walk_hydro(const float4* __restrict__ iA, const float4* __restrict__ iB,
+// Full (A, C) records of staged record q under either staging.
+template <bool COMPACT>
+__device__ __forceinline__ float4 walk_rec_a(const float4* __restrict__ A, int q, const WalkPair& pp) {
+  float4 r = A[q];
+  if (COMPACT) r.w = pp.h;
+  return r;
+}
+template <bool COMPACT>
+__device__ __forceinline__ float4 walk_rec_c(const float4* __restrict__ A, const float4* __restrict__ C,
+                                             const float* __restrict__ c, int q, const WalkPair& pp) {
+  if (COMPACT) return make_float4(A[q].w, c[q], pp.nu, pp.m);
+  return C[q];
+}
+
+template <int VSIG, int GRAD, bool COMPACT>
+__global__ void __launch_bounds__(kWQWarps * 32, 4) k_walk_hydro(const float4* __restrict__ iA, const float4* __restrict__ iB,
                                                               const float4* __restrict__ iC, const float4* __restrict__ jA,
                                                               const float4* __restrict__ jB, const float4* __restrict__ jC,
                                                               const int* __restrict__ ni_displ,
                                                               const int* __restrict__ nj_displ,
                                                               const int2* __restrict__ items, WalkPair pp,
-                                                              float4* __restrict__ out4, float* __restrict__ out_dt) {
+                                                              float4* __restrict__ out4, float* __restrict__ out_dt,
+                                                              const float* __restrict__ ic,
+                                                              const float* __restrict__ jc) {
   using Lay = WalkQLayout<VSIG>;
   extern __shared__ __align__(16) unsigned char wq_smem[];
   float* tx = reinterpret_cast<float*>(wq_smem + Lay::soa);
@@ -228,7 +250,7 @@ __global__ void __launch_bounds__(kWQWarps * 32) k_walk_hydro(const float4* __re
     for (int t = threadIdx.x; t < kWQChunk * 5; t += blockDim.x) (&res[0][0])[t] = 0.0f;
     // largest h of the batch's i (h > 0: its bits order like the values)
     float hm = 0.0f;
-    for (int t = threadIdx.x; t < nb; t += blockDim.x) hm = fmaxf(hm, iA[ib + t].w);
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) hm = fmaxf(hm, walk_rec_a<COMPACT>(iA, ib + t, pp).w);
     for (int jb = j0; jb < j1; jb += kWQTile) {
       const int nt = min(kWQTile, j1 - jb), nt64 = (nt + 63) & ~63;
       __syncthreads();  // the previous tile's readers are done; res zeroed
@@ -237,7 +259,7 @@ __global__ void __launch_bounds__(kWQWarps * 32) k_walk_hydro(const float4* __re
       float hj_max = hm;
       for (int k = threadIdx.x; k < nt64; k += blockDim.x) {
         if (k < nt) {
-          const float4 J = jA[jb + k];
+          const float4 J = walk_rec_a<COMPACT>(jA, jb + k, pp);
           tx[k] = J.x, ty[k] = J.y, tz[k] = J.z, th[k] = J.w;
           hj_max = fmaxf(hj_max, J.w);
           if (VSIG) {
@@ -260,7 +282,7 @@ __global__ void __launch_bounds__(kWQWarps * 32) k_walk_hydro(const float4* __re
         const int ia = ib + ip;
         const bool has_b = ip + 1 < nb;
         const int ibb = has_b ? ia + 1 : ia;
-        const float4 Aa = iA[ia], Ab = iA[ibb];
+        const float4 Aa = walk_rec_a<COMPACT>(iA, ia, pp), Ab = walk_rec_a<COMPACT>(iA, ibb, pp);
         const float4 Ba = iB[ia], Bb = iB[ibb];
         const f2 XA = dup(Aa.x), YA = dup(Aa.y), ZA = dup(Aa.z);
         const f2 XB = dup(Ab.x), YB = dup(Ab.y), ZB = dup(Ab.z);
@@ -292,7 +314,7 @@ __global__ void __launch_bounds__(kWQWarps * 32) k_walk_hydro(const float4* __re
           }
         }
         __syncwarp();
-        const float4 Ca = iC[ia], Cb = iC[ibb];
+        const float4 Ca = walk_rec_c<COMPACT>(iA, iC, ic, ia, pp), Cb = walk_rec_c<COMPACT>(iA, iC, ic, ibb, pp);
         float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         const int n = max(na, nq);
         for (int k = lane; k < n; k += 32) {
@@ -300,13 +322,13 @@ __global__ void __launch_bounds__(kWQWarps * 32) k_walk_hydro(const float4* __re
             const int u = qa[k];
             const float4 J = make_float4(tx[u], ty[u], tz[u], th[u]);
             const float4 V = VSIG ? make_float4(tvx[u], tvy[u], tvz[u], trho[u]) : jB[jb + u];
-            walk_pair<GRAD>(Aa, Ba, Ca, J, V, jC[jb + u], pp, acc);
+            walk_pair<GRAD>(Aa, Ba, Ca, J, V, walk_rec_c<COMPACT>(jA, jC, jc, jb + u, pp), pp, acc);
           }
           if (k < nq) {
             const int u = qb[k];
             const float4 J = make_float4(tx[u], ty[u], tz[u], th[u]);
             const float4 V = VSIG ? make_float4(tvx[u], tvy[u], tvz[u], trho[u]) : jB[jb + u];
-            walk_pair<GRAD>(Ab, Bb, Cb, J, V, jC[jb + u], pp, acc + 4);
+            walk_pair<GRAD>(Ab, Bb, Cb, J, V, walk_rec_c<COMPACT>(jA, jC, jc, jb + u, pp), pp, acc + 4);
           }
         }
         const float y = wq_butterfly8(acc, lane);
@@ -332,7 +354,8 @@ __global__ void __launch_bounds__(kWQWarps * 32) k_walk_hydro(const float4* __re
       const int i = ib + t;
       const float* r = res[t];
       out4[i] = make_float4(r[0], r[1], r[2], r[3] / iB[i].w);
-      out_dt[i] = pp.c_cfl * iA[i].w / (iC[i].y + r[4]);  // force.h:56 / kernel.cu:279
+      out_dt[i] = pp.c_cfl * walk_rec_a<COMPACT>(iA, i, pp).w /
+                  (walk_rec_c<COMPACT>(iA, iC, ic, i, pp).y + r[4]);  // force.h:56 / kernel.cu:279
     }
     __syncthreads();
   }
@@ -416,6 +439,8 @@ struct TagState {
   int kind = K_NONE;  // what the last dispatch enqueued
   int n_walk = 0;
   long long ni_total = 0;
+  long long h2d_bytes = 0, d2h_bytes = 0;  // of the last dispatch
+  int pieces = 0, pieces_compact = 0;
   PinnedBuf h_i, h_j, h_off, h_out;
   DevBuf d_i, d_j, d_off, d_out;
 };
@@ -592,6 +617,79 @@ static int check_walk_args(const char* fn, int32_t tag, int32_t n_walk, const vo
   return 0;
 }
 
+// Where the hydro records of one dispatch are staged (SoA blocks of the
+// pinned buffers) and what one piece of it is packed with.
+struct HydroPack {
+  const wcsph_fdps_layout* L;
+  const void* const* epi;
+  const void* const* epj;
+  const int32_t* n_epi;
+  const int32_t* n_epj;
+  const long long* ni_d;
+  const long long* nj_d;
+  float4 *hiA, *hiB, *hiC, *hjA, *hjB, *hjC;
+  bool compact;
+  double h0, nu0, m0;  // compact: the piece's uniform values
+  float *hic, *hjc;    // compact: c of record q at hic[q] / hjc[q], inside the piece's own part of the C blocks
+};
+
+// Pack walk w: positions relative to its first i-particle (or j when it has
+// no i).  Full staging: A = (x, y, z, h), B = (v, rho), C = (P/rho^2, c, nu, m).
+// Compact: A = (x, y, z, P/rho^2), B, c alone; returns false when a record's
+// h, nu or m differs from the piece's (the piece is then packed again in full).
+static bool pack_hydro_walk(const HydroPack& K, int w) {
+  const wcsph_fdps_layout& L = *K.L;
+  const char* pi = (const char*)K.epi[w];
+  const char* pj = (const char*)K.epj[w];
+  double o[3] = {0, 0, 0};
+  if (K.n_epi[w] > 0) {
+    for (int k = 0; k < 3; ++k) o[k] = rd(pi, L.epi_pos + 8 * k);
+  } else if (K.n_epj[w] > 0) {
+    for (int k = 0; k < 3; ++k) o[k] = rd(pj, L.epj_pos + 8 * k);
+  }
+  bool uniform = true;
+  float* hic = K.hic;
+  float* hjc = K.hjc;
+  for (int i = 0; i < K.n_epi[w]; ++i) {
+    const char* r = pi + (size_t)i * L.epi_size;
+    const long long q = K.ni_d[w] + i;
+    const double dens = rd(r, L.epi_dens);
+    const float po = (float)(rd(r, L.epi_pres) / (dens * dens));
+    const float x = (float)(rd(r, L.epi_pos) - o[0]), y = (float)(rd(r, L.epi_pos + 8) - o[1]),
+                z = (float)(rd(r, L.epi_pos + 16) - o[2]);
+    st_stage(&K.hiB[q], (float)rd(r, L.epi_vel), (float)rd(r, L.epi_vel + 8), (float)rd(r, L.epi_vel + 16),
+             (float)dens);
+    if (K.compact) {
+      uniform &= rd(r, L.epi_smth) == K.h0 && rd(r, L.epi_visc) == K.nu0;
+      st_stage(&K.hiA[q], x, y, z, po);
+      hic[q] = (float)rd(r, L.epi_snds);
+    } else {
+      st_stage(&K.hiA[q], x, y, z, (float)rd(r, L.epi_smth));
+      st_stage(&K.hiC[q], po, (float)rd(r, L.epi_snds), (float)rd(r, L.epi_visc), 0.f);
+    }
+  }
+  for (int j = 0; j < K.n_epj[w]; ++j) {
+    const char* r = pj + (size_t)j * L.epj_size;
+    const long long q = K.nj_d[w] + j;
+    const double dens = rd(r, L.epj_dens);
+    const float po = (float)(rd(r, L.epj_pres) / (dens * dens));
+    const float x = (float)(rd(r, L.epj_pos) - o[0]), y = (float)(rd(r, L.epj_pos + 8) - o[1]),
+                z = (float)(rd(r, L.epj_pos + 16) - o[2]);
+    st_stage(&K.hjB[q], (float)rd(r, L.epj_vel), (float)rd(r, L.epj_vel + 8), (float)rd(r, L.epj_vel + 16),
+             (float)dens);
+    if (K.compact) {
+      uniform &= rd(r, L.epj_smth) == K.h0 && rd(r, L.epj_visc) == K.nu0 && rd(r, L.epj_mass) == K.m0;
+      st_stage(&K.hjA[q], x, y, z, po);
+      hjc[q] = (float)rd(r, L.epj_snds);
+    } else {
+      st_stage(&K.hjA[q], x, y, z, (float)rd(r, L.epj_smth));
+      st_stage(&K.hjC[q], po, (float)rd(r, L.epj_snds), (float)rd(r, L.epj_visc), (float)rd(r, L.epj_mass));
+    }
+  }
+  stage_fence();
+  return uniform;
+}
+
 // Shared dispatch body.  kind selects the record shapes and the kernel.
 static int dispatch_common(int kind, int32_t tag, int32_t n_walk, const void* const* epi, const int32_t* n_epi,
                            const void* const* epj, const int32_t* n_epj) {
@@ -665,6 +763,9 @@ static int dispatch_common(int kind, int32_t tag, int32_t n_walk, const void* co
     }
   }
   WCSPH_CUDA(cudaMemcpyAsync(d_ni, h_ni, off_bytes, cudaMemcpyHostToDevice, T.stream));
+  T.h2d_bytes = (long long)off_bytes;
+  T.d2h_bytes = 0;
+  T.pieces = T.pieces_compact = 0;
   const int2* d_items = reinterpret_cast<const int2*>(d_nj + (n_walk + 1));
 
   // SoA sub-arrays inside the staging buffers.
@@ -681,42 +782,42 @@ static int dispatch_common(int kind, int32_t tag, int32_t n_walk, const void* co
   for (int ch = 0; ch < chunks; ++ch) {
     const int w0 = (int)((long long)n_walk * ch / chunks), w1 = (int)((long long)n_walk * (ch + 1) / chunks);
     if (w0 == w1) continue;
+    bool compact = false;
+    WalkPair pp{(float)g_plugin.pair.alpha, (float)g_plugin.pair.beta, (float)g_plugin.pair.c_cfl,
+                (float)g_plugin.pair.eps, g_plugin.pair.vsig_mode, g_plugin.pair.grad_mode, 0.f, 0.f, 0.f};
+    if (kind == K_HYDRO) {
+      // A compact piece keeps c of record q at float 3 a0 + q of the C block:
+      // bytes [16 a0, 16 a0 + 4 (a1 - a0)), inside the piece's own part
+      // [16 a0, 16 a1) (the copies of earlier pieces may still be reading
+      // theirs).
+      HydroPack K{&L, epi, epj, n_epi, n_epj, ni_d.data(), nj_d.data(), hiA, hiB, hiC, hjA, hjB, hjC, false, 0, 0, 0,
+                  reinterpret_cast<float*>(hiC) + 3 * ni_d[w0], reinterpret_cast<float*>(hjC) + 3 * nj_d[w0]};
+      // Compact staging when every record of the piece carries the h, nu and
+      // m of its first j-record (checked while packing).
+      for (int w = w0; w < w1 && !K.compact; ++w)
+        if (n_epj[w] > 0) {
+          const char* r = (const char*)epj[w];
+          K.compact = true;
+          K.h0 = rd(r, L.epj_smth), K.nu0 = rd(r, L.epj_visc), K.m0 = rd(r, L.epj_mass);
+        }
+      int mixed = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : mixed)
+      for (int w = w0; w < w1; ++w) mixed |= pack_hydro_walk(K, w) ? 0 : 1;
+      if (K.compact && mixed) {
+        K.compact = false;
 #pragma omp parallel for schedule(dynamic, 16)
-    for (int w = w0; w < w1; ++w) {
-      const char* pi = (const char*)epi[w];
-      const char* pj = (const char*)epj[w];
-      // Walk origin: the first i-particle (or j if the walk has no i).
-      double o[3] = {0, 0, 0};
-      if (kind == K_HYDRO) {
-        if (n_epi[w] > 0) {
-          for (int k = 0; k < 3; ++k) o[k] = rd(pi, L.epi_pos + 8 * k);
-        } else if (n_epj[w] > 0) {
-          for (int k = 0; k < 3; ++k) o[k] = rd(pj, L.epj_pos + 8 * k);
-        }
-        for (int i = 0; i < n_epi[w]; ++i) {
-          const char* r = pi + (size_t)i * L.epi_size;
-          const long long q = ni_d[w] + i;
-          const double dens = rd(r, L.epi_dens);
-          st_stage(&hiA[q], (float)(rd(r, L.epi_pos) - o[0]), (float)(rd(r, L.epi_pos + 8) - o[1]),
-                   (float)(rd(r, L.epi_pos + 16) - o[2]), (float)rd(r, L.epi_smth));
-          st_stage(&hiB[q], (float)rd(r, L.epi_vel), (float)rd(r, L.epi_vel + 8), (float)rd(r, L.epi_vel + 16),
-                   (float)dens);
-          st_stage(&hiC[q], (float)(rd(r, L.epi_pres) / (dens * dens)), (float)rd(r, L.epi_snds),
-                   (float)rd(r, L.epi_visc), 0.f);
-        }
-        for (int j = 0; j < n_epj[w]; ++j) {
-          const char* r = pj + (size_t)j * L.epj_size;
-          const long long q = nj_d[w] + j;
-          const double dens = rd(r, L.epj_dens);
-          st_stage(&hjA[q], (float)(rd(r, L.epj_pos) - o[0]), (float)(rd(r, L.epj_pos + 8) - o[1]),
-                   (float)(rd(r, L.epj_pos + 16) - o[2]), (float)rd(r, L.epj_smth));
-          st_stage(&hjB[q], (float)rd(r, L.epj_vel), (float)rd(r, L.epj_vel + 8), (float)rd(r, L.epj_vel + 16),
-                   (float)dens);
-          st_stage(&hjC[q], (float)(rd(r, L.epj_pres) / (dens * dens)), (float)rd(r, L.epj_snds),
-                   (float)rd(r, L.epj_visc), (float)rd(r, L.epj_mass));
-        }
-        stage_fence();
-      } else {
+        for (int w = w0; w < w1; ++w) pack_hydro_walk(K, w);
+      }
+      compact = K.compact;
+      if (compact) pp.h = (float)K.h0, pp.nu = (float)K.nu0, pp.m = (float)K.m0;
+      ++T.pieces;
+      T.pieces_compact += compact ? 1 : 0;
+    } else {
+#pragma omp parallel for schedule(dynamic, 16)
+      for (int w = w0; w < w1; ++w) {
+        const char* pi = (const char*)epi[w];
+        const char* pj = (const char*)epj[w];
+        double o[3] = {0, 0, 0};
         if (n_epi[w] > 0) {
           for (int k = 0; k < 3; ++k) o[k] = rd(pi, L.fepi_pos + 8 * k);
         } else if (n_epj[w] > 0) {
@@ -738,36 +839,51 @@ static int dispatch_common(int kind, int32_t tag, int32_t n_walk, const void* co
     }
     // H2D of this chunk's records (SoA blocks copied piecewise).
     const long long a0 = ni_d[w0], a1 = ni_d[w1], b0 = nj_d[w0], b1 = nj_d[w1];
-    const int nblk_i = kind == K_HYDRO ? 3 : 1;
-    for (int s = 0; s < nblk_i; ++s)
-      if (a1 > a0)
-        WCSPH_CUDA(cudaMemcpyAsync(diA + s * NI + a0, hiA + s * NI + a0, sizeof(float4) * (a1 - a0),
-                                   cudaMemcpyHostToDevice, T.stream));
+    // the third block carries full float4 records, or only c (compact staging,
+    // at the start of the piece's part of the block)
+    auto h2d = [&](void* dst, const void* src, size_t bytes) -> int {
+      if (bytes == 0) return 0;
+      WCSPH_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, T.stream));
+      T.h2d_bytes += (long long)bytes;
+      return 0;
+    };
+    int rc = 0;
     if (kind == K_HYDRO) {
-      for (int s = 0; s < 3; ++s)
-        if (b1 > b0)
-          WCSPH_CUDA(cudaMemcpyAsync(djA + s * NJ + b0, hjA + s * NJ + b0, sizeof(float4) * (b1 - b0),
-                                     cudaMemcpyHostToDevice, T.stream));
-    } else if (b1 > b0) {
-      WCSPH_CUDA(cudaMemcpyAsync(djA + b0, hjA + b0, sizeof(float4) * (b1 - b0), cudaMemcpyHostToDevice, T.stream));
-      WCSPH_CUDA(cudaMemcpyAsync((float*)(djA + NJ) + b0, hjm + b0, sizeof(float) * (b1 - b0), cudaMemcpyHostToDevice,
-                                 T.stream));
+      if (a1 > a0) {
+        rc |= h2d(diA + a0, hiA + a0, sizeof(float4) * (a1 - a0));
+        rc |= h2d(diA + NI + a0, hiB + a0, sizeof(float4) * (a1 - a0));
+        rc |= h2d(diA + 2 * NI + a0, hiC + a0, (compact ? sizeof(float) : sizeof(float4)) * (a1 - a0));
+      }
+      if (b1 > b0) {
+        rc |= h2d(djA + b0, hjA + b0, sizeof(float4) * (b1 - b0));
+        rc |= h2d(djA + NJ + b0, hjB + b0, sizeof(float4) * (b1 - b0));
+        rc |= h2d(djA + 2 * NJ + b0, hjC + b0, (compact ? sizeof(float) : sizeof(float4)) * (b1 - b0));
+      }
+    } else {
+      if (a1 > a0) rc |= h2d(diA + a0, hiA + a0, sizeof(float4) * (a1 - a0));
+      if (b1 > b0) {
+        rc |= h2d(djA + b0, hjA + b0, sizeof(float4) * (b1 - b0));
+        rc |= h2d((float*)(djA + NJ) + b0, hjm + b0, sizeof(float) * (b1 - b0));
+      }
     }
+    if (rc) return rc;
     // One CTA per walk.
     if (kind == K_HYDRO) {
-      const WalkPair pp{(float)g_plugin.pair.alpha, (float)g_plugin.pair.beta, (float)g_plugin.pair.c_cfl,
-                        (float)g_plugin.pair.eps, g_plugin.pair.vsig_mode, g_plugin.pair.grad_mode};
       float4* out4 = (float4*)T.d_out.p;
       float* out_dt = (float*)(out4 + NI);
-      auto kern = pp.vsig_mode ? (pp.grad_mode ? k_walk_hydro<1, 1> : k_walk_hydro<1, 0>)
-                               : (pp.grad_mode ? k_walk_hydro<0, 1> : k_walk_hydro<0, 0>);
+      auto kern = compact ? (pp.vsig_mode ? (pp.grad_mode ? k_walk_hydro<1, 1, true> : k_walk_hydro<1, 0, true>)
+                                          : (pp.grad_mode ? k_walk_hydro<0, 1, true> : k_walk_hydro<0, 0, true>))
+                          : (pp.vsig_mode ? (pp.grad_mode ? k_walk_hydro<1, 1, false> : k_walk_hydro<1, 0, false>)
+                                          : (pp.grad_mode ? k_walk_hydro<0, 1, false> : k_walk_hydro<0, 0, false>));
       const int smem = (int)(pp.vsig_mode ? WalkQLayout<1>::bytes : WalkQLayout<0>::bytes);
       WCSPH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
       const long long nblk = item_off[ch + 1] - item_off[ch];
       if (nblk > 0) {
         kern<<<(unsigned)nblk, kWQWarps * 32, smem, T.stream>>>(diA, diA + NI, diA + 2 * NI, djA, djA + NJ,
                                                                 djA + 2 * NJ, d_ni, d_nj, d_items + item_off[ch], pp,
-                                                                out4, out_dt);
+                                                                out4, out_dt,
+                                                                reinterpret_cast<const float*>(diA + 2 * NI) + 3 * a0,
+                                                                reinterpret_cast<const float*>(djA + 2 * NJ) + 3 * b0);
         WCSPH_CUDA(cudaGetLastError());
       }
       if (a1 > a0) {
@@ -775,14 +891,17 @@ static int dispatch_common(int kind, int32_t tag, int32_t n_walk, const void* co
                                    cudaMemcpyDeviceToHost, T.stream));
         WCSPH_CUDA(cudaMemcpyAsync((float*)((float4*)T.h_out.p + NI) + a0, out_dt + a0, sizeof(float) * (a1 - a0),
                                    cudaMemcpyDeviceToHost, T.stream));
+        T.d2h_bytes += (long long)(sizeof(float4) + sizeof(float)) * (a1 - a0);
       }
     } else {
       float* out = (float*)T.d_out.p;
       k_walk_filter<<<w1 - w0, kWalkThreads, 0, T.stream>>>(diA, djA, (const float*)(djA + NJ), d_ni, d_nj, w0, out);
       WCSPH_CUDA(cudaGetLastError());
-      if (a1 > a0)
+      if (a1 > a0) {
         WCSPH_CUDA(cudaMemcpyAsync((float*)T.h_out.p + a0, out + a0, sizeof(float) * (a1 - a0), cudaMemcpyDeviceToHost,
                                    T.stream));
+        T.d2h_bytes += (long long)sizeof(float) * (a1 - a0);
+      }
     }
   }
   WCSPH_CUDA(cudaEventRecord(T.done, T.stream));
@@ -864,6 +983,19 @@ int wcsph_filter_dispatch(int32_t tag, int32_t n_walk, const void* const* epi, c
 int wcsph_filter_retrieve(int32_t tag, int32_t n_walk, const int32_t* n_i, void* const* result) {
   std::lock_guard<std::mutex> lk(g_plugin_mu);
   return retrieve_common(K_FILTER, tag, n_walk, n_i, result);
+}
+int wcsph_fdps_stats(int32_t tag, int64_t* out4) {
+  if (tag < 0 || tag >= WCSPH_FDPS_MAX_TAGS || !out4) {
+    set_error("wcsph_fdps_stats: bad tag %d or null output", tag);
+    return WCSPH_E_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(g_plugin_mu);
+  const TagState& T = g_plugin.tags[tag];
+  out4[0] = T.h2d_bytes;
+  out4[1] = T.d2h_bytes;
+  out4[2] = T.pieces_compact;
+  out4[3] = T.pieces;
+  return 0;
 }
 }  // extern "C"
 
