@@ -364,6 +364,14 @@ def run_e2e(case, steps, warmup, device):
 
     for _ in range(warmup):
         one_pass()
+    # bytes each pass moves, as the library counts them (wcsph_fdps_stats after each batch)
+    h2d = d2h = pieces = compact = 0
+    st = (C.c_int64 * 4)()
+    for pi, pj, po, ni, nj, nw in batches:
+        N.check("dispatch", L.wcsph_hydro_dispatch(0, nw, pi, N.ptr(ni, C.c_int32), pj, N.ptr(nj, C.c_int32)))
+        N.check("stats", L.wcsph_fdps_stats(0, st))
+        N.check("retrieve", L.wcsph_hydro_retrieve(0, nw, N.ptr(ni, C.c_int32), po))
+        h2d, d2h, compact, pieces = h2d + st[0], d2h + st[1], compact + st[2], pieces + st[3]
     split = [0.0, 0.0]  # dispatch (pack + enqueue), retrieve (wait + unpack)
 
     def timed_pass():
@@ -379,10 +387,9 @@ def run_e2e(case, steps, warmup, device):
     for _ in range(steps):
         timed_pass()
     dt = (time.perf_counter() - t0) / steps
-    h2d = len(epi) * 48 + len(epj) * 48 + 8 * (w.n_walk + len(batches))
-    d2h = len(epi) * 20
-    return dict(s_per_pass=dt, h2d=h2d, d2h=d2h, n_walk=w.n_walk, evaluated=w.n_evaluated, walks=w, epi=epi,
-                epj=epj, dispatch_ms=1e3 * split[0] / steps, retrieve_ms=1e3 * split[1] / steps)
+    return dict(s_per_pass=dt, h2d=int(h2d), d2h=int(d2h), n_walk=w.n_walk, evaluated=w.n_evaluated, walks=w, epi=epi,
+                epj=epj, dispatch_ms=1e3 * split[0] / steps, retrieve_ms=1e3 * split[1] / steps,
+                pieces=int(pieces), pieces_compact=int(compact))
 
 
 def cpu_reference(case, walks, epi, epj, seconds, pairs_total, whole_budget_s=None):
@@ -512,7 +519,8 @@ def main():
                               "warmup": args.warmup, "ms_per_pass": 1e3 * e["s_per_pass"],
                               "dispatch_ms": e["dispatch_ms"], "retrieve_ms": e["retrieve_ms"],
                               "walks": e["n_walk"], "pair_evaluations_per_pass": e["evaluated"],
-                              "h2d_bytes_per_pass": e["h2d"], "d2h_bytes_per_pass": e["d2h"]}))
+                              "h2d_bytes_per_pass": e["h2d"], "d2h_bytes_per_pass": e["d2h"],
+                              "pieces_compact": f"{e['pieces_compact']} of {e['pieces']}"}))
         barrier(pg)
         finish(pg)
         return 0
@@ -566,7 +574,9 @@ def main():
         e = run_e2e(case, max(1, min(3, args.steps // 50)), 1, local)
         e2e = {"value": dev["pairs_per_step"] / e["s_per_pass"], "unit": UNIT, "h2d_bytes_per_step": e["h2d"],
                "d2h_bytes_per_step": e["d2h"], "path": "wcsph_hydro_dispatch/retrieve, FDPS walks of <=128 i",
-               "walks": e["n_walk"], "pair_evaluations_per_pass": e["evaluated"]}
+               "walks": e["n_walk"], "pair_evaluations_per_pass": e["evaluated"],
+               "ms_per_pass": 1e3 * e["s_per_pass"], "dispatch_ms": e["dispatch_ms"], "retrieve_ms": e["retrieve_ms"],
+               "pieces_compact": f"{e['pieces_compact']} of {e['pieces']}"}
         if not args.no_cpu:
             v, desc, cores, _ = cpu_reference(case, e["walks"], e["epi"], e["epj"], args.cpu_seconds,
                                               dev["pairs_per_step"])

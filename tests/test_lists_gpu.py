@@ -32,10 +32,13 @@ def test_lists_match_per_step_search(prec, native):
     assert stats["builds"] + stats["list_steps"] == 60
     assert stats["builds"] >= 60 // 8 and stats["longest"] <= 192
     assert st["steps"] == ref_st["steps"] == 60
-    assert abs(st["time"] - ref_st["time"]) <= 1e-5 * ref_st["time"]
-    assert rel_l2(got["pos"], ref["pos"]) < 1e-6
-    assert rel_l2(got["vel"], ref["vel"]) < 1e-4
-    assert rel_l2(got["dens"], ref["dens"]) < 1e-6
+    # the half2 list pass rebuilds displacements from 16-bit positions (about
+    # 1e-4 relative per pair), the FP32 one only reorders the sums
+    h16 = prec == N.PREC_HALF2
+    assert abs(st["time"] - ref_st["time"]) <= (1e-4 if h16 else 1e-5) * ref_st["time"]
+    assert rel_l2(got["pos"], ref["pos"]) < (1e-5 if h16 else 1e-6)
+    assert rel_l2(got["vel"], ref["vel"]) < (1e-3 if h16 else 1e-4)
+    assert rel_l2(got["dens"], ref["dens"]) < (1e-5 if h16 else 1e-6)
     assert rel_l2(got["acc"], ref["acc"]) < 1e-3
     assert abs(pairs - ref_pairs) <= 1e-3 * ref_pairs
 
@@ -183,7 +186,7 @@ LIST_TOL = {N.PREC_TILED: 1e-5, N.PREC_HALF2: 1e-3}
 
 
 @pytest.mark.parametrize("density_pass", [0, 1, 2], ids=["none", "summation", "shepard"])
-@pytest.mark.parametrize("prec", [N.PREC_TILED], ids=["tiled"])
+@pytest.mark.parametrize("prec", [N.PREC_TILED, N.PREC_HALF2], ids=["tiled", "half2"])
 def test_list_pass_vs_fp64(prec, density_pass, native, oracle_lib):
     """The passes a list step runs (k_density_list, k_hydro_list) on a list
     step after several steps of drift, against the FP64 oracle on the same
@@ -210,14 +213,15 @@ def test_list_pass_vs_fp64(prec, density_pass, native, oracle_lib):
         assert r["dens"] < 1e-5, r
 
 
-def test_list_pass_periodic_vs_fp64(native, oracle_lib):
+@pytest.mark.parametrize("prec", [N.PREC_TILED, N.PREC_HALF2], ids=["tiled", "half2"])
+def test_list_pass_periodic_vs_fp64(prec, native, oracle_lib):
     """Config-3 mode (periodic box, summation density every step) through the
     lists: particles run past the faces between builds (wrapping waits for the
     next build); the oracle sees the wrapped positions."""
     case = cases.periodic_lattice(n_side=20, dx=0.01, seed=21)
     rng = np.random.default_rng(22)
     case.vel = rng.normal(0.0, 1.0, size=case.vel.shape)
-    with Solver(case.n, precision=N.PREC_TILED, list_interval=50, list_skin=0.8) as s:
+    with Solver(case.n, precision=prec, list_interval=50, list_skin=0.8) as s:
         k = s.add(case)
         s.step(6)
         st = s.read(k)
@@ -230,7 +234,8 @@ def test_list_pass_periodic_vs_fp64(native, oracle_lib):
     # unwrapped vs wrapped coordinates round differently in the last bit, which
     # can flip the support test of a pair at r = 2h exactly; none expected here
     assert abs(int(pr["nbr"].sum()) - int(r["tot"])) <= 2
-    assert r["dens"] < 1e-5 and r["acc"] < 1e-5 and r["div_v"] < 1e-5, r
+    tol = LIST_TOL[prec]
+    assert r["dens"] < 1e-5 and r["acc"] < tol and r["div_v"] < tol, r
 
 
 def test_probe_lists_builds_when_stale(native, oracle_lib):
@@ -256,3 +261,28 @@ def test_probe_lists_needs_lists(native):
         k = s.add(case)
         with pytest.raises(N.WcsphError, match="no neighbour lists"):
             s.probe(k, lists=True)
+
+
+def test_half2_list_options(native):
+    with pytest.raises(N.WcsphError, match="list_skin"):
+        Solver(1000, precision=N.PREC_HALF2, list_interval=4, list_skin=2.0)
+
+
+def test_half2_lists_far_particles(native, oracle_lib):
+    """Particles thrown above the cell grid (whose top cells are clamped) are
+    more than a cell edge from their build cell's centre: the half2 list pass
+    reads them from the FP32 records, and the sums stay the oracle's."""
+    case = small_dam(dx=0.05, seed=14, vel_sigma=0.1)
+    fluid = np.nonzero(case.type == N.HYDRO)[0]
+    top = fluid[np.argsort(-case.pos[fluid, 2], kind="stable")[:40]]
+    case.pos[top, 2] += (case.hi[2] - case.pos[top, 2]) + 0.3  # two cells above the grid, inside the kill box
+    with Solver(case.n, precision=N.PREC_HALF2, list_interval=20) as s:
+        k = s.add(case, density_mode=N.DENSITY_CONTINUITY)
+        s.step(3)
+        st = s.read(k)
+        pr = s.probe(k, lists=True)
+    assert (st["alive"] == 1).all()
+    assert (st["pos"][top, 2] > case.hi[2]).all()
+    r = oracle_list_check(oracle_lib, case, st, pr, 0)
+    np.testing.assert_array_equal(pr["nbr"], r["cnt"])
+    assert r["acc"] < 1e-3 and r["div_v"] < 1e-3, r

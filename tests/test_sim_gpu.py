@@ -22,9 +22,10 @@ def prec(request):
 
 
 def force_tol(prec):
-    """FP32 pair arithmetic: 1e-5 relative L2 vs FP64.  The half2 kernel
-    gradient carries ~5e-4 relative error per pair: 3e-3."""
-    return 3e-3 if prec == N.PREC_HALF2 else TOL
+    """FP32 pair arithmetic: 1e-5 relative L2 vs FP64.  Without neighbour
+    lists the half2 precision runs the FP32 tiled kernel (its compact records
+    belong to the list pass), so the same bar holds for every precision here."""
+    return TOL
 
 
 def f32(a):
@@ -125,10 +126,10 @@ def test_trajectory_vs_fp64(prec, native, oracle_lib, mode):
     assert status["steps"] == nsteps
     assert status["time"] == pytest.approx(t, rel=1e-5)
     disp = o["pos"] - f32(case.pos)
-    traj = 1e-2 if prec == N.PREC_HALF2 else 1e-3
+    traj = 1e-3
     assert rel_l2(st["pos"] - f32(case.pos), disp) < traj
     assert rel_l2(st["vel"], o["vel"]) < traj
-    np.testing.assert_allclose(st["dens"], o["dens"], rtol=1e-4 if prec == N.PREC_HALF2 else 1e-5)
+    np.testing.assert_allclose(st["dens"], o["dens"], rtol=1e-5)
 
 
 def test_momentum_conservation_periodic(prec, native):

@@ -82,6 +82,8 @@ struct SimImpl {
   uint32_t* list = nullptr;
   int* list_cnt = nullptr;
   float4* x0 = nullptr;
+  float4* jv = nullptr;  // compact j-records of the half2 list pass
+  uint2* jq = nullptr;
   unsigned* d_lflags = nullptr;       // see StepArgs::list_flags
   unsigned* h_lflags = nullptr;       // pinned copy, written at the end of every list-mode step
   cudaGraphExec_t gexec_reuse = nullptr;
@@ -118,8 +120,11 @@ static size_t per_particle_bytes() {
          + sizeof(int);                                             // non-empty cell list
 }
 
+static bool h16_lists(const wcsph_sim_options& o) { return o.list_interval > 0 && o.precision == WCSPH_PREC_HALF2; }
+
 static int64_t device_bytes(const wcsph_sim_options& o) {
-  const int64_t list_bytes = o.list_interval > 0 ? (int64_t)(kListMax * 4 + 4 + 16) * o.max_particles : 0;
+  const int64_t list_bytes =
+      o.list_interval > 0 ? (int64_t)(kListMax * 4 + 4 + 16 + (h16_lists(o) ? 24 : 0)) * o.max_particles : 0;
   return (int64_t)per_particle_bytes() * o.max_particles + list_bytes + 2 * sizeof(int) * o.max_cells +
          (sizeof(InstParams) + sizeof(InstDyn) + sizeof(int)) * (int64_t)o.max_instances + (int64_t)cub_sort_bytes(o.max_particles) +
          (1 << 20);
@@ -198,6 +203,8 @@ static StepArgs make_args(SimImpl& S) {
     a.list_cnt = S.list_cnt;
     a.list_max = kListMax;
     a.list_flags = S.d_lflags;
+    a.jv = S.jv;
+    a.jq = S.jq;
   }
   return a;
 }
@@ -294,7 +301,7 @@ static int enqueue_reuse(SimImpl& S, StepArgs a, bool density, int* launches, cu
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));
     if (density) {  // the kernels return at once for instances with no density pass due
-      if (int rc = launch_density_list(a, n, S.s)) return rc;
+      if (int rc = launch_density_list(a, n, S.s, h16_lists(S.opt))) return rc;
       k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
       L += 2;
     }
@@ -443,6 +450,7 @@ static int fill_params(const wcsph_instance_desc& d, HostInst& I, InstParams& P)
     I.cell[k] = d.periodic ? ext / (float)nc : std::max(ext / (float)nc, H * 1.0001f);
     if (I.cell[k] < H) I.cell[k] = H * 1.0001f;
     P.lo[k] = d.lo[k];
+    P.cell[k] = I.cell[k];
     P.inv_cell[k] = 1.0f / I.cell[k];
     P.ncell[k] = nc;
     P.L[k] = ext;
@@ -615,6 +623,11 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
     set_error("wcsph_sim_create: neighbour lists need the tiled or half2 precision");
     return WCSPH_E_INVALID;
   }
+  if (h16_lists(*opt) && opt->list_skin > 1.5f) {
+    set_error("wcsph_sim_create: the half2 list pass keeps positions within one cell edge of the build cell's "
+              "centre, which needs list_skin <= 1.5 h (got %g)", (double)opt->list_skin);
+    return WCSPH_E_INVALID;
+  }
   int ndev = 0;
   WCSPH_CUDA(cudaGetDeviceCount(&ndev));
   if (opt->device < 0 || opt->device >= ndev) {
@@ -670,6 +683,10 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
     rc |= alloc(S, (void**)&S.list_cnt, N * sizeof(int));
     rc |= alloc(S, (void**)&S.x0, N * sizeof(float4));
     rc |= alloc(S, (void**)&S.d_lflags, 4 * sizeof(unsigned));
+    if (h16_lists(*opt)) {
+      rc |= alloc(S, (void**)&S.jv, N * sizeof(float4));
+      rc |= alloc(S, (void**)&S.jq, N * sizeof(uint2));
+    }
     if (!rc && cudaHostAlloc((void**)&S.h_lflags, 4 * sizeof(unsigned), cudaHostAllocDefault) != cudaSuccess)
       rc = 1;
   }
@@ -807,6 +824,18 @@ static int append_instance(SimImpl& S, const AppendSpec& A, int32_t* slot) {
     const float skin = list_skin(S.opt) * (float)d.h, R = 2.0f * (float)d.h + skin;
     P.HL2 = R * R;
     P.inv_skin = 1.0f / skin;
+    // Half2 list pass: a rebuilt displacement coordinate is off by at most
+    // half a 2^-15 step of the cell edge plus the rounding of the two FP32
+    // cell centres; doubled for margin, the squared distance near (2h)^2 is
+    // then within band of the exact FP32 value.
+    float delta = 0.f;
+    for (int k = 0; k < 3; ++k) {
+      const float big = std::max(std::fabs(d.lo[k]), std::fabs(d.hi[k])) + 2.0f * I.cell[k];
+      const float ulp = std::nextafter(big, INFINITY) - big;
+      delta = std::max(delta, 2.0f * (I.cell[k] / 65536.0f + 2.0f * ulp));
+    }
+    const float H = 2.0f * (float)d.h, H2 = H * H;
+    P.h16_band = 4.0f * H * 1.7320508f * delta + 3.0f * delta * delta + 16.0f * (std::nextafter(H2, INFINITY) - H2);
   }
   I.used = I.active = true;
   HostInst prev = S.inst[k];
@@ -1295,7 +1324,7 @@ static int enqueue_probe_lists(SimImpl& S, int density_pass) {
   if (n > 0) {
     k_kick_refresh<<<nblk(n), kBlock, 0, S.s>>>(a);
     if (density_pass) {
-      if (int rc = launch_density_list(a, n, S.s)) return rc;
+      if (int rc = launch_density_list(a, n, S.s, h16_lists(S.opt))) return rc;
       k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
     }
     const bool h16 = S.opt.precision == WCSPH_PREC_HALF2;

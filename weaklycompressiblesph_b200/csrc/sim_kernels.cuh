@@ -10,6 +10,8 @@
 //     pair phases with one 256-bit load)
 //   cell table: start/end per linear cell, instance-major.
 #pragma once
+#include <cuda_fp16.h>
+
 #include "wcsph_common.cuh"
 
 namespace wcsph {
@@ -25,6 +27,52 @@ __device__ __forceinline__ JRec ld_jrec(const JRec* p) {
       : "=f"(r.a.x), "=f"(r.a.y), "=f"(r.a.z), "=f"(r.a.w), "=f"(r.b.x), "=f"(r.b.y), "=f"(r.b.z), "=f"(r.b.w)
       : "l"(p));
   return r;
+}
+
+// ---------------------------------------------- compact (half2) j-records
+// The half2 list pass reads, per list entry, jv = (vx, vy, vz, P/rho^2) in
+// FP32 and jq: x, y, z as 16-bit fixed-point offsets from the centre of the
+// particle's cell at the last list build (units of 2^-15 cell edges, biased
+// by 2^15, so one cell edge either side) and (rho - rho0) as a half.  24
+// bytes instead of the 32 of the FP32 record.  A particle more than one cell
+// edge from that centre (above the grid, where the cells are clamped; or
+// removed) is marked far (the half NaN kFarMark), and its entries are read
+// from the FP32 record.
+constexpr uint32_t kFarMark = 0x7e00u;  // half NaN in the high 16 bits of jq.y
+constexpr float kQ16Scale = 32768.0f;
+
+__device__ __forceinline__ float cell_centre(const InstParams& P, int k, int c) {
+  return __fmaf_rn((float)c + 0.5f, P.cell[k], P.lo[k]);
+}
+
+__device__ __forceinline__ uint32_t rho_half_bits(const InstParams& P, float rho) {
+  return (uint32_t)__half_as_ushort(__float2half_rn(rho - P.rho0));
+}
+
+// Write the compact record of slot p: position x, velocity v, P/rho^2 po,
+// density rho, build cell (cx, cy, cz).
+__device__ __forceinline__ void write_h16(float4* jv, uint2* jq, const InstParams& P, int p, const float4& x,
+                                          const float4& v, float po, float rho, int cx, int cy, int cz) {
+  const int c[3] = {cx, cy, cz};
+  const float* xa = &x.x;
+  uint32_t u[3];
+  bool far = false;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float q = (xa[k] - cell_centre(P, k, c[k])) * P.inv_cell[k];
+    const int t = __float2int_rn(q * kQ16Scale) + 32768;  // NaN converts to 0: far below
+    far |= t < 0 || t > 65535;
+    u[k] = (uint32_t)min(max(t, 0), 65535);
+  }
+  jv[p] = make_float4(v.x, v.y, v.z, po);
+  jq[p] = make_uint2(u[0] | (u[1] << 16), u[2] | ((far ? kFarMark : rho_half_bits(P, rho)) << 16));
+}
+
+// A removed particle: far, so that its entries take the FP32 record (whose
+// position is far from everything).
+__device__ __forceinline__ void write_h16_dead(float4* jv, uint2* jq, int p) {
+  jv[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+  jq[p] = make_uint2(0x80008000u, 0x8000u | (kFarMark << 16));
 }
 
 struct SimArrays {
@@ -62,6 +110,9 @@ struct StepArgs {
                           // [2] sticky errors (1 skin exceeded, 2 overflow), [3] largest list
   int list_reuse;         // this step reads the lists: periodic wrapping waits for the next build
   int* dens_any;          // set by k_step_begin when any instance has a density pass in this launch
+  // compact j-records of the half2 list pass (WCSPH_PREC_HALF2 with lists; null otherwise)
+  float4* jv;             // (vx, vy, vz, P/rho^2)
+  uint2* jq;              // 16-bit cell-relative x, y, z and (rho - rho0) as a half (h16_record)
   int probe_density;      // density pass of a probe launch: 0 none, 1 summation, 2 Shepard
   // diagnostics (probe phase)
   float4* diag_acc;
@@ -254,9 +305,11 @@ __global__ void k_permute(StepArgs a) {
   if (a.x0) a.x0[p] = make_float4(x.x, x.y, x.z, 0.f);  // list build: positions the lists refer to
   float pres, snds;
   tait(P, x.w, pres, snds);
-  a.jr[p].a = make_float4(x.x, x.y, x.z, pres / (x.w * x.w));
+  const float po = pres / (x.w * x.w);
+  a.jr[p].a = make_float4(x.x, x.y, x.z, po);
   a.jr[p].b = make_float4(v.x, v.y, v.z, x.w);
   a.jC[p] = snds;
+  if (a.jv) write_h16(a.jv, a.jq, P, p, x, v, po, x.w, cx, cy, cz);
 }
 
 // Does the hydro pass run for an instance in the current launch?
@@ -342,9 +395,15 @@ __global__ void k_eos(StepArgs a) {
   const float rho = a.rho_new[p];
   float pres, snds;
   tait(P, rho, pres, snds);
-  a.jr[p].a.w = pres / (rho * rho);
+  const float po = pres / (rho * rho);
+  a.jr[p].a.w = po;
   a.jr[p].b.w = rho;
   a.jC[p] = snds;
+  if (a.jv) {  // the compact record's P/rho^2 and density (a far mark stays)
+    a.jv[p].w = po;
+    const uint2 q = a.jq[p];
+    if ((q.y >> 16) != kFarMark) a.jq[p].y = (q.y & 0xffffu) | (rho_half_bits(P, rho) << 16);
+  }
   if (ph != PH_PROBE) a.alt.pos[p].w = rho;
 }
 

@@ -49,10 +49,14 @@ __global__ void k_kick_refresh(StepArgs a) {
   if (!dead) {
     float pres, snds;
     tait(P, x.w, pres, snds);
-    a.jr[p].a = make_float4(x.x, x.y, x.z, pres / (x.w * x.w));
+    const float po = pres / (x.w * x.w);
+    a.jr[p].a = make_float4(x.x, x.y, x.z, po);
     a.jr[p].b = make_float4(v.x, v.y, v.z, x.w);
     a.jC[p] = snds;
     const float4 o = a.x0[p];
+    if (a.jv)  // compact record relative to the particle's cell at the build
+      write_h16(a.jv, a.jq, P, p, x, v, po, x.w, cell_of(o.x, P.lo[0], P.inv_cell[0], P.ncell[0]),
+                cell_of(o.y, P.lo[1], P.inv_cell[1], P.ncell[1]), cell_of(o.z, P.lo[2], P.inv_cell[2], P.ncell[2]));
     const float dx = x.x - o.x, dy = x.y - o.y, dz = x.z - o.z;
     const float r = sqrtf(dx * dx + dy * dy + dz * dz) * P.inv_skin;
     disp_bits = __float_as_uint(r);
@@ -61,16 +65,50 @@ __global__ void k_kick_refresh(StepArgs a) {
     a.jr[p].a = make_float4(1.0e30f, 1.0e30f, 1.0e30f, 0.f);
     a.jr[p].b = make_float4(0.f, 0.f, 0.f, 1.f);
     a.jC[p] = 0.f;
+    if (a.jv) write_h16_dead(a.jv, a.jq, p);
   }
   list_flag_max(&a.list_flags[0], disp_bits);
   list_flag_max(&a.list_flags[1], drift_bits);
+}
+
+// The build cell of slot p (its position x0 at the last list build).
+__device__ __forceinline__ void build_cell(const StepArgs& a, const InstParams& P, int p, int c[3]) {
+  const float4 o = a.x0[p];
+  c[0] = cell_of(o.x, P.lo[0], P.inv_cell[0], P.ncell[0]);
+  c[1] = cell_of(o.y, P.lo[1], P.inv_cell[1], P.ncell[1]);
+  c[2] = cell_of(o.z, P.lo[2], P.inv_cell[2], P.ncell[2]);
+}
+
+// Neighbour-cell offsets + 1 of an offset code k = (ox+1) + 3 (oy+1) + 9 (oz+1).
+__device__ __forceinline__ void offset_code(uint32_t k, uint32_t& ox1, uint32_t& oy1, uint32_t& oz1) {
+  const uint32_t t = (k * 11u) >> 5;  // k / 3 for k < 32
+  ox1 = k - 3u * t;
+  oz1 = (t * 11u) >> 5;  // t / 3
+  oy1 = t - 3u * oz1;
+}
+
+// Periodic image shift of an entry with offset code k for a particle in
+// build cell c: the neighbour cell c + o wraps past an edge on an axis exactly
+// where the image code of the FP32 list build would name a shift.
+__device__ __forceinline__ void offset_shift(const InstParams& P, const int c[3], uint32_t k, float& sx, float& sy,
+                                             float& sz) {
+  uint32_t o1[3];
+  offset_code(k, o1[0], o1[1], o1[2]);
+  float sh[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int q = c[d] + (int)o1[d] - 1;
+    sh[d] = q < 0 ? -P.L[d] : (q >= P.ncell[d] ? P.L[d] : 0.0f);
+  }
+  sx = sh[0], sy = sh[1], sz = sh[2];
 }
 
 // Density pass over the lists: k_density_plain's sums (summation, or the
 // Shepard filter of force.h:12-29) over each particle's list entries that are
 // within the support now, one thread per particle walking its own list row
 // four entries per 16-byte load.  Particles removed since the build keep
-// their density.
+// their density.  H16: the entries carry offset codes (half2 list build).
+template <bool H16>
 __global__ void __launch_bounds__(128) k_density_list(StepArgs a) {
   if (a.dens_any && !*a.dens_any) return;  // no density pass in this launch
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -90,6 +128,8 @@ __global__ void __launch_bounds__(128) k_density_list(StepArgs a) {
   const float rho_i = a.jr[p].b.w;
   const int n = min(a.list_cnt[p], a.list_max);
   const uint4* row = reinterpret_cast<const uint4*>(a.list + (size_t)p * a.list_max);
+  int ci[3] = {0, 0, 0};
+  if (H16 && P.periodic) build_cell(a, P, p, ci);
   float sum = 0.f, one = 0.f;
   for (int k = 0; k < n; k += 4) {
     const uint4 e4 = __ldg(&row[k >> 2]);
@@ -100,7 +140,10 @@ __global__ void __launch_bounds__(128) k_density_list(StepArgs a) {
         const int q = ent[u] & kSlotMask;
         const float4 J = __ldg(&a.jr[q].a);
         float sx = 0.f, sy = 0.f, sz = 0.f;
-        if (P.periodic) entry_shift(P, ent[u] >> 27, sx, sy, sz);
+        if (P.periodic) {
+          if (H16) offset_shift(P, ci, ent[u] >> 27, sx, sy, sz);
+          else entry_shift(P, ent[u] >> 27, sx, sy, sz);
+        }
         const float dx = __fsub_rn(I.x, __fadd_rn(J.x, sx));
         const float dy = __fsub_rn(I.y, __fadd_rn(J.y, sy));
         const float dz = __fsub_rn(I.z, __fadd_rn(J.z, sz));
@@ -117,9 +160,10 @@ __global__ void __launch_bounds__(128) k_density_list(StepArgs a) {
   a.rho_new[p] = shep ? t / (0.5f / rho_i + one) : P.mass * P.Kw * t;
 }
 
-inline int launch_density_list(const StepArgs& a, int n, cudaStream_t s) {
+inline int launch_density_list(const StepArgs& a, int n, cudaStream_t s, bool h16) {
   if (n <= 0) return 0;
-  k_density_list<<<(n + 127) / 128, 128, 0, s>>>(a);
+  if (h16) k_density_list<true><<<(n + 127) / 128, 128, 0, s>>>(a);
+  else k_density_list<false><<<(n + 127) / 128, 128, 0, s>>>(a);
   WCSPH_CUDA(cudaGetLastError());
   return 0;
 }
@@ -129,6 +173,83 @@ __device__ __forceinline__ f2 snds7_2(f2 RHO, f2 RHO0, f2 IRHO0, f2 C0) {
   const f2 X = add2(dup(1.0f), mul2(sub2(RHO, RHO0), IRHO0));
   const f2 T = mul2(C0, mul2(mul2(X, X), X));
   return pk(fmaxf(fabsf(lo(T)), 1.0e-8f), fmaxf(fabsf(hi(T)), 1.0e-8f));
+}
+
+// i-side operands of the half2 list pass: i's position relative to the
+// centre of its build cell (FP32, exact: the two are within a factor of two),
+// its build cell, and the scales -cell / 2^15 that turn the 16-bit offsets
+// into lengths.
+struct H16I {
+  f2 QX, QY, QZ, SX, SY, SZ;
+  int c[3];
+  float band;
+};
+
+// Two list entries (halves a, b) of the half2 list pass.  The displacement of
+// j from i is rebuilt from the 16-bit offsets: x_i - x_j = q_i - (o + q_j)
+// cell, with o the neighbour-cell offset of the entry; the biased offset and
+// o are added as integers below the float mantissa's top (0x4B000000 is
+// 2^23), so one packed subtraction turns them into an exact (q_j + o) 2^15.
+// An entry takes the FP32 record instead (the displacement exactly as the
+// FP32 path and the oracle round it) when its squared distance lies within
+// the band where the 16-bit positions cannot decide 0 < r^2 < (2h)^2, or when
+// j is marked far: the pairs summed, and the neighbour counts, are exactly
+// those of the FP32 support test.
+__device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P, const PairC& C, const PairI& I,
+                                          const H16I& H, const float4& Va, const float4& Vb, uint2 Qa, uint2 Qb,
+                                          uint32_t ea, uint32_t eb, bool qva, bool qvb, bool g7, f2& AX, f2& AY,
+                                          f2& AZ, f2& DS, float& vsa, float& vsb, unsigned& na, unsigned& nb) {
+  const f2 MAG = dup(8388608.0f + 65536.0f);
+  uint32_t oxa, oya, oza, oxb, oyb, ozb;
+  offset_code(ea >> 27, oxa, oya, oza);
+  offset_code(eb >> 27, oxb, oyb, ozb);
+  auto fb = [](uint32_t u16, uint32_t o1) { return __uint_as_float(0x4B000000u + u16 + (o1 << 15)); };
+  const f2 TX = sub2(pk(fb(Qa.x & 0xffffu, oxa), fb(Qb.x & 0xffffu, oxb)), MAG);
+  const f2 TY = sub2(pk(fb(Qa.x >> 16, oya), fb(Qb.x >> 16, oyb)), MAG);
+  const f2 TZ = sub2(pk(fb(Qa.y & 0xffffu, oza), fb(Qb.y & 0xffffu, ozb)), MAG);
+  f2 DX = fma2(TX, H.SX, H.QX), DY = fma2(TY, H.SY, H.QY), DZ = fma2(TZ, H.SZ, H.QZ);
+  f2 R2raw = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
+  const uint32_t ha = Qa.y >> 16, hb = Qb.y >> 16;
+  float r2a = lo(R2raw), r2b = hi(R2raw);
+  const bool xa = qva && (ha == kFarMark || r2a < H.band || fabsf(r2a - C.H2) < H.band);
+  const bool xb = qvb && (hb == kFarMark || r2b < H.band || fabsf(r2b - C.H2) < H.band);
+  float rja = P.rho0 + __half2float(__ushort_as_half((unsigned short)ha));
+  float rjb = P.rho0 + __half2float(__ushort_as_half((unsigned short)hb));
+  if (xa || xb) {  // rare: the exact FP32 displacement of the FP32 path
+    float dx[2] = {lo(DX), hi(DX)}, dy[2] = {lo(DY), hi(DY)}, dz[2] = {lo(DZ), hi(DZ)}, r2[2] = {r2a, r2b};
+    float rj[2] = {rja, rjb};
+    const bool ex[2] = {xa, xb};
+    const uint32_t e[2] = {ea, eb};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (!ex[h]) continue;
+      const JRec R = ld_jrec(&a.jr[e[h] & kSlotMask]);
+      float sx = 0.f, sy = 0.f, sz = 0.f;
+      if (P.periodic) offset_shift(P, H.c, e[h] >> 27, sx, sy, sz);
+      const float ix = h ? hi(I.X) : lo(I.X), iy = h ? hi(I.Y) : lo(I.Y), iz = h ? hi(I.Z) : lo(I.Z);
+      dx[h] = __fsub_rn(ix, __fadd_rn(R.a.x, sx));
+      dy[h] = __fsub_rn(iy, __fadd_rn(R.a.y, sy));
+      dz[h] = __fsub_rn(iz, __fadd_rn(R.a.z, sz));
+      r2[h] = dist2(dx[h], dy[h], dz[h]);
+      rj[h] = R.b.w;
+    }
+    DX = pk(dx[0], dx[1]), DY = pk(dy[0], dy[1]), DZ = pk(dz[0], dz[1]);
+    R2raw = pk(r2[0], r2[1]);
+    r2a = r2[0], r2b = r2[1];
+    rja = rj[0], rjb = rj[1];
+  }
+  const bool va = qva && r2a > 0.0f && r2a < C.H2;
+  const bool vb = qvb && r2b > 0.0f && r2b < C.H2;
+  na += va, nb += vb;
+  const f2 RHOJ = pk(rja, rjb);
+  f2 CJ;
+  if (g7) {
+    CJ = snds7_2(RHOJ, dup(P.rho0), dup(P.inv_rho0), dup(P.c0));
+  } else {
+    CJ = pk(__ldg(&a.jC[ea & kSlotMask]), __ldg(&a.jC[eb & kSlotMask]));
+  }
+  pair_terms2(C, I, DX, DY, DZ, R2raw, va, vb, pk(Va.x, Vb.x), pk(Va.y, Vb.y), pk(Va.z, Vb.z), pk(Va.w, Vb.w), RHOJ,
+              CJ, AX, AY, AZ, DS, vsa, vsb);
 }
 
 // The list pass over particle slots below the build's live count (the
@@ -188,27 +309,49 @@ __global__ void __launch_bounds__(128, MINB) k_hydro_list(StepArgs a) {
                           [&](int q, const float4&, float, float, float, float, uint32_t code) {
                             const JRec Rq = ld_jrec(&a.jr[q]);
                             const float cq = g7 ? lo(snds7_2(dup(Rq.b.w), RHO0, IRHO0, C0)) : __ldg(&a.jC[q]);
-                            pair2<H16, false>(P, C, I, Rq, R, code, 13u, dup(cq), true, false, AX, AY, AZ, DS, vsa,
-                                              vsb, ca, cb);
+                            pair2<false>(P, C, I, Rq, R, code, 13u, dup(cq), true, false, AX, AY, AZ, DS, vsa, vsb,
+                                         ca, cb);
                             ++ca;
                           });
       }
-      for (int k = 4 * sub; k < n; k += 4 * TPI) {
-        const uint4 e = __ldg(&row[k >> 2]);
-        const uint32_t e0 = e.x, e1 = k + 1 < n ? e.y : self, e2 = k + 2 < n ? e.z : self, e3 = k + 3 < n ? e.w : self;
-        const int g0 = e0 & kSlotMask, g1 = e1 & kSlotMask, g2 = e2 & kSlotMask, g3 = e3 & kSlotMask;
-        const JRec R0 = ld_jrec(&a.jr[g0]), R1 = ld_jrec(&a.jr[g1]);
-        const JRec R2 = ld_jrec(&a.jr[g2]), R3 = ld_jrec(&a.jr[g3]);
-        f2 C01, C23;
-        if (g7) {  // c_j from rho_j: no gather of c
-          C01 = snds7_2(pk(R0.b.w, R1.b.w), RHO0, IRHO0, C0);
-          C23 = snds7_2(pk(R2.b.w, R3.b.w), RHO0, IRHO0, C0);
-        } else {
-          C01 = pk(__ldg(&a.jC[g0]), __ldg(&a.jC[g1])), C23 = pk(__ldg(&a.jC[g2]), __ldg(&a.jC[g3]));
+      if (H16) {  // compact records
+        H16I H;
+        build_cell(a, P, p, H.c);
+        H.QX = dup(R.a.x - cell_centre(P, 0, H.c[0]));
+        H.QY = dup(R.a.y - cell_centre(P, 1, H.c[1]));
+        H.QZ = dup(R.a.z - cell_centre(P, 2, H.c[2]));
+        H.SX = dup(-P.cell[0] / kQ16Scale), H.SY = dup(-P.cell[1] / kQ16Scale), H.SZ = dup(-P.cell[2] / kQ16Scale);
+        H.band = P.h16_band;
+        for (int k = 4 * sub; k < n; k += 4 * TPI) {
+          const uint4 e = __ldg(&row[k >> 2]);
+          const uint32_t e0 = e.x, e1 = k + 1 < n ? e.y : self, e2 = k + 2 < n ? e.z : self,
+                         e3 = k + 3 < n ? e.w : self;
+          const int g0 = e0 & kSlotMask, g1 = e1 & kSlotMask, g2 = e2 & kSlotMask, g3 = e3 & kSlotMask;
+          const float4 V0 = __ldg(&a.jv[g0]), V1 = __ldg(&a.jv[g1]), V2 = __ldg(&a.jv[g2]), V3 = __ldg(&a.jv[g3]);
+          const uint2 Q0 = __ldg(&a.jq[g0]), Q1 = __ldg(&a.jq[g1]), Q2 = __ldg(&a.jq[g2]), Q3 = __ldg(&a.jq[g3]);
+          h16_pair2(a, P, C, I, H, V0, V1, Q0, Q1, e0, e1, true, k + 1 < n, g7, AX, AY, AZ, DS, vsa, vsb, ca, cb);
+          h16_pair2(a, P, C, I, H, V2, V3, Q2, Q3, e2, e3, k + 2 < n, k + 3 < n, g7, AX, AY, AZ, DS, vsa, vsb, ca,
+                    cb);
         }
-        pair2<H16, true>(P, C, I, R0, R1, e0 >> 27, e1 >> 27, C01, true, k + 1 < n, AX, AY, AZ, DS, vsa, vsb, ca, cb);
-        pair2<H16, true>(P, C, I, R2, R3, e2 >> 27, e3 >> 27, C23, k + 2 < n, k + 3 < n, AX, AY, AZ, DS, vsa, vsb,
-                         ca, cb);
+      } else {
+        for (int k = 4 * sub; k < n; k += 4 * TPI) {
+          const uint4 e = __ldg(&row[k >> 2]);
+          const uint32_t e0 = e.x, e1 = k + 1 < n ? e.y : self, e2 = k + 2 < n ? e.z : self,
+                         e3 = k + 3 < n ? e.w : self;
+          const int g0 = e0 & kSlotMask, g1 = e1 & kSlotMask, g2 = e2 & kSlotMask, g3 = e3 & kSlotMask;
+          const JRec R0 = ld_jrec(&a.jr[g0]), R1 = ld_jrec(&a.jr[g1]);
+          const JRec R2 = ld_jrec(&a.jr[g2]), R3 = ld_jrec(&a.jr[g3]);
+          f2 C01, C23;
+          if (g7) {  // c_j from rho_j: no gather of c
+            C01 = snds7_2(pk(R0.b.w, R1.b.w), RHO0, IRHO0, C0);
+            C23 = snds7_2(pk(R2.b.w, R3.b.w), RHO0, IRHO0, C0);
+          } else {
+            C01 = pk(__ldg(&a.jC[g0]), __ldg(&a.jC[g1])), C23 = pk(__ldg(&a.jC[g2]), __ldg(&a.jC[g3]));
+          }
+          pair2<true>(P, C, I, R0, R1, e0 >> 27, e1 >> 27, C01, true, k + 1 < n, AX, AY, AZ, DS, vsa, vsb, ca, cb);
+          pair2<true>(P, C, I, R2, R3, e2 >> 27, e3 >> 27, C23, k + 2 < n, k + 3 < n, AX, AY, AZ, DS, vsa, vsb, ca,
+                      cb);
+        }
       }
       sx = lo(AX) + hi(AX), sy = lo(AY) + hi(AY), sz = lo(AZ) + hi(AZ), sd = lo(DS) + hi(DS);
       sv = fmaxf(vsa, vsb);

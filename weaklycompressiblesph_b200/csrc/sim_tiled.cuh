@@ -1,9 +1,11 @@
-// Tiled hydro kernel (WCSPH_PREC_TILED, WCSPH_PREC_HALF2): one warp per non-empty cell.
+// Tiled hydro kernel (WCSPH_PREC_TILED, WCSPH_PREC_HALF2; the two differ only
+// in the entries a list build writes): one warp per non-empty cell.
 //
 //   1. The 27 neighbour cells of the warp's cell are flattened into one
 //      candidate list and staged into the warp's shared-memory tile as
 //      structure-of-arrays x[], y[], z[] (pre-shifted by the periodic image)
-//      and e[] (global slot | image code << 27), with coalesced loads (a
+//      and e[] (global slot | image code << 27; the half2 list build writes
+//      the neighbour-cell offset code instead), with coalesced loads (a
 //      cell's particles are contiguous after the sort).
 //   2. The cell's i-particles are taken two at a time.  Each lane tests two
 //      adjacent candidates against both i: one 64-bit shared load yields the
@@ -114,21 +116,55 @@ __device__ __forceinline__ PairC pair_consts(const InstParams& P) {
 }
 
 // Pair terms of two (i, j) pairs at once, one per f32x2 half (force.h:38-57
-// for uniform h, m, nu within an instance): j-records Ra, Rb with image codes
-// ea, eb (entry >> 27) and sound speeds CJ; qva, qvb say whether a half holds
-// a pair (idle halves must still name a valid record; they add exactly zero).
-// Accumulates a_x, a_y, a_z, sum g dr.dv and the v_sig maximum per half.
-// CHECK: halves outside 0 < r^2 < (2h)^2 add exactly zero, and na, nb count
-// the halves summed.
-// H16: the kernel gradient (|dr|^2, 1/|dr|, s, F(s), F/|dr|) is evaluated in
-// packed half2 on displacements in units of the support 2h; everything else
-// stays FP32 (WCSPH_PREC_HALF2).
-template <bool H16, bool CHECK>
+// for uniform h, m, nu within an instance), from the displacements DX, DY,
+// DZ = x_i - x_j with R2raw their squared length, j's velocity VJX..VJZ,
+// P_j/rho_j^2 POJ, density RHOJ and sound speed CJ; va, vb say whether a half
+// holds an in-support pair (idle halves add exactly zero).  Accumulates a_x,
+// a_y, a_z, sum g dr.dv and the v_sig maximum per half.
+__device__ __forceinline__ void pair_terms2(const PairC& C, const PairI& I, f2 DX, f2 DY, f2 DZ, f2 R2raw, bool va,
+                                            bool vb, f2 VJX, f2 VJY, f2 VJZ, f2 POJ, f2 RHOJ, f2 CJ, f2& AX, f2& AY,
+                                            f2& AZ, f2& DS, float& vsa, float& vsb) {
+  const f2 ONE = dup(1.0f), HALF = dup(0.5f), TWELVE = dup(12.0f), MTHREE = dup(-3.0f), TWO = dup(2.0f);
+  const f2 MONE = dup(-1.0f);
+  const f2 R2 = pk(va ? lo(R2raw) : C.H2, vb ? hi(R2raw) : C.H2);  // finite stand-in for idle halves
+  const f2 W = pk(va ? 1.0f : 0.0f, vb ? 1.0f : 0.0f);
+  // gradW = G * dr
+  const f2 RINV = rsqrt2(R2);
+  const f2 S = mul2(mul2(R2, RINV), C.IH);
+  const f2 A = max0_2(sub2(ONE, S)), B = max0_2(sub2(HALF, S));
+  const f2 F = fma2(TWELVE, mul2(B, B), mul2(MTHREE, mul2(A, A)));  // 12 (1/2-s)+^2 - 3 (1-s)+^2
+  const f2 G = mul2(mul2(F, C.KG), mul2(RINV, W));
+  const f2 DVX = sub2(I.VX, VJX), DVY = sub2(I.VY, VJY), DVZ = sub2(I.VZ, VJZ);
+  const f2 DRDV = fma2(DZ, DVZ, fma2(DY, DVY, mul2(DX, DVX)));
+  const f2 RDEN = rcp2(add2(R2, C.EH2));
+  const f2 MUr = mul2(mul2(DRDV, RDEN), C.HH);
+  const f2 MU = pk(va && lo(DRDV) < 0.0f ? lo(MUr) : 0.0f, vb && hi(DRDV) < 0.0f ? hi(MUr) : 0.0f);
+  const f2 RS = rcp2(add2(I.RHO, RHOJ));
+  const f2 AV = mul2(mul2(fma2(C.BETA, MU, mul2(C.MHALPHA, add2(I.CI, CJ))), MU), mul2(RS, TWO));
+  if (C.vs) {
+    vsa = fmaxf(vsa, -lo(MU));
+    vsb = fmaxf(vsb, -hi(MU));
+  } else {
+    vsa = fmaxf(vsa, lo(MU));
+    vsb = fmaxf(vsb, hi(MU));
+  }
+  const f2 NPG = mul2(mul2(add2(add2(I.PO, POJ), AV), G), MONE);
+  const f2 VISC = mul2(mul2(mul2(C.NU4, G), R2), mul2(RS, RDEN));
+  AX = fma2(NPG, DX, fma2(VISC, DVX, AX));
+  AY = fma2(NPG, DY, fma2(VISC, DVY, AY));
+  AZ = fma2(NPG, DZ, fma2(VISC, DVZ, AZ));
+  DS = fma2(G, DRDV, DS);
+}
+
+// Pair terms of two (i, j) pairs at once from FP32 j-records Ra, Rb with
+// image codes ea, eb (entry >> 27) and sound speeds CJ; qva, qvb say whether a
+// half holds a pair (idle halves must still name a valid record; they add
+// exactly zero).  CHECK: halves outside 0 < r^2 < (2h)^2 add exactly zero,
+// and na, nb count the halves summed.
+template <bool CHECK>
 __device__ __forceinline__ void pair2(const InstParams& P, const PairC& C, const PairI& I, const JRec& Ra,
                                       const JRec& Rb, uint32_t ea, uint32_t eb, f2 CJ, bool qva, bool qvb, f2& AX,
                                       f2& AY, f2& AZ, f2& DS, float& vsa, float& vsb, unsigned& na, unsigned& nb) {
-  const f2 ONE = dup(1.0f), HALF = dup(0.5f), TWELVE = dup(12.0f), MTHREE = dup(-3.0f), TWO = dup(2.0f);
-  const f2 MONE = dup(-1.0f);
   const float4 &Ja = Ra.a, &Jb = Rb.a, &JBa = Ra.b, &JBb = Rb.b;
   float jxa = Ja.x, jya = Ja.y, jza = Ja.z, jxb = Jb.x, jyb = Jb.y, jzb = Jb.z;
   if (C.per) {  // the same rounded image position the scan tested
@@ -143,57 +179,13 @@ __device__ __forceinline__ void pair2(const InstParams& P, const PairC& C, const
   const bool va = CHECK ? qva && lo(R2raw) > 0.0f && lo(R2raw) < C.H2 : qva;
   const bool vb = CHECK ? qvb && hi(R2raw) > 0.0f && hi(R2raw) < C.H2 : qvb;
   if (CHECK) na += va, nb += vb;
-  const f2 R2 = pk(va ? lo(R2raw) : C.H2, vb ? hi(R2raw) : C.H2);  // finite stand-in for idle halves
-  const f2 W = pk(va ? 1.0f : 0.0f, vb ? 1.0f : 0.0f);
-  f2 G;  // gradW = G * dr
-  if (H16) {
-    const float iH = C.iH;
-    // q = dr / 2h; idle halves get a harmless |q| = 1/2
-    const __half2 qx = __floats2half2_rn(va ? lo(DX) * iH : 0.5f, vb ? hi(DX) * iH : 0.5f);
-    const __half2 qy = __floats2half2_rn(va ? lo(DY) * iH : 0.0f, vb ? hi(DY) * iH : 0.0f);
-    const __half2 qz = __floats2half2_rn(va ? lo(DZ) * iH : 0.0f, vb ? hi(DZ) * iH : 0.0f);
-    const __half2 r2h = __hmax2(__hfma2(qz, qz, __hfma2(qy, qy, __hmul2(qx, qx))), __float2half2_rn(1.0e-4f));
-    const __half2 rih = h2rsqrt(r2h);
-    const __half2 sh = __hmul2(r2h, rih);  // s = |dr| / 2h
-    const __half2 ah = __hmax2(__hsub2(__float2half2_rn(1.0f), sh), __float2half2_rn(0.0f));
-    const __half2 bh = __hmax2(__hsub2(__float2half2_rn(0.5f), sh), __float2half2_rn(0.0f));
-    const __half2 Fh = __hfma2(__float2half2_rn(12.0f), __hmul2(bh, bh),
-                               __hmul2(__float2half2_rn(-3.0f), __hmul2(ah, ah)));
-    const float2 gq = __half22float2(__hmul2(Fh, rih));  // F(s) / |q|
-    G = mul2(pk(gq.x, gq.y), mul2(dup(C.KgiH), W));       // g = F Kg / |dr| = (F/|q|) Kg / 2h
-  } else {
-    const f2 RINV = rsqrt2(R2);
-    const f2 S = mul2(mul2(R2, RINV), C.IH);
-    const f2 A = max0_2(sub2(ONE, S)), B = max0_2(sub2(HALF, S));
-    const f2 F = fma2(TWELVE, mul2(B, B), mul2(MTHREE, mul2(A, A)));  // 12 (1/2-s)+^2 - 3 (1-s)+^2
-    G = mul2(mul2(F, C.KG), mul2(RINV, W));
-  }
-  const f2 DVX = sub2(I.VX, pk(JBa.x, JBb.x)), DVY = sub2(I.VY, pk(JBa.y, JBb.y)), DVZ = sub2(I.VZ, pk(JBa.z, JBb.z));
-  const f2 DRDV = fma2(DZ, DVZ, fma2(DY, DVY, mul2(DX, DVX)));
-  const f2 RDEN = rcp2(add2(R2, C.EH2));
-  const f2 MUr = mul2(mul2(DRDV, RDEN), C.HH);
-  const f2 MU = pk(va && lo(DRDV) < 0.0f ? lo(MUr) : 0.0f, vb && hi(DRDV) < 0.0f ? hi(MUr) : 0.0f);
-  const f2 RS = rcp2(add2(I.RHO, pk(JBa.w, JBb.w)));
-  const f2 AV = mul2(mul2(fma2(C.BETA, MU, mul2(C.MHALPHA, add2(I.CI, CJ))), MU), mul2(RS, TWO));
-  if (C.vs) {
-    vsa = fmaxf(vsa, -lo(MU));
-    vsb = fmaxf(vsb, -hi(MU));
-  } else {
-    vsa = fmaxf(vsa, lo(MU));
-    vsb = fmaxf(vsb, hi(MU));
-  }
-  const f2 NPG = mul2(mul2(add2(add2(I.PO, pk(Ja.w, Jb.w)), AV), G), MONE);
-  const f2 VISC = mul2(mul2(mul2(C.NU4, G), R2), mul2(RS, RDEN));
-  AX = fma2(NPG, DX, fma2(VISC, DVX, AX));
-  AY = fma2(NPG, DY, fma2(VISC, DVY, AY));
-  AZ = fma2(NPG, DZ, fma2(VISC, DVZ, AZ));
-  DS = fma2(G, DRDV, DS);
+  pair_terms2(C, I, DX, DY, DZ, R2raw, va, vb, pk(JBa.x, JBb.x), pk(JBa.y, JBb.y), pk(JBa.z, JBb.z), pk(Ja.w, Jb.w),
+              pk(JBa.w, JBb.w), CJ, AX, AY, AZ, DS, vsa, vsb);
 }
 
 // Pair terms of i_a (low half) and i_b (high half) over their queues; adds
 // the warp totals into res[0] (i_a) and res[1] (i_b): ax, ay, az, sum g drdv,
 // v_sig, count.  Lanes past a queue's end contribute exactly zero.
-template <bool H16>
 __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParams& P, int ia, int ib, bool has_b,
                                               const float4& IA, const float4& IBp, const uint32_t* qa, int na,
                                               const uint32_t* qb, int nb, float (*res)[6], int lane) {
@@ -217,7 +209,7 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
     const int ga = ea & kSlotMask, gb = eb & kSlotMask;
     const JRec Ra = ld_jrec(&a.jr[ga]), Rb = ld_jrec(&a.jr[gb]);
     const f2 CJ = pk(__ldg(&a.jC[ga]), __ldg(&a.jC[gb]));
-    pair2<H16, false>(P, C, I, Ra, Rb, ea >> 27, eb >> 27, CJ, qva, qvb, AX, AY, AZ, DS, vsa, vsb, ca, cb);
+    pair2<false>(P, C, I, Ra, Rb, ea >> 27, eb >> 27, CJ, qva, qvb, AX, AY, AZ, DS, vsa, vsb, ca, cb);
   }
   const float v8[8] = {lo(AX), lo(AY), lo(AZ), lo(DS), hi(AX), hi(AY), hi(AZ), hi(DS)};
   const float y = butterfly8(v8, lane);
@@ -355,7 +347,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
             const int u = ub + 32 * r + lane;
             const int k = kk[r];
             const float sx = __shfl_sync(full, shx, k), sy = __shfl_sync(full, shy, k), sz = __shfl_sync(full, shz, k);
-            const uint32_t ck27 = __shfl_sync(full, code, k) << 27;
+            // entries carry the image code, or for the half2 list pass the
+            // neighbour-cell offset code k (its compact records are relative
+            // to the cells of the build)
+            const uint32_t ck27 = (H16 && LB ? (uint32_t)k : __shfl_sync(full, code, k)) << 27;
             if (u < t0 + tn) {
               tx[u - t0] = __fadd_rn(J[r].x, sx);
               ty[u - t0] = __fadd_rn(J[r].y, sy);
@@ -412,7 +407,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
             if (lane == ii) lcount += na;
             if (has_b && lane == ii + 1) lcount += nb;
           }
-          if (!LB) hydro_queues2<H16>(a, P, ia, ibb, has_b, IA, IB, qa, na, qb, nb, &res[ii], lane);
+          if (!LB) hydro_queues2(a, P, ia, ibb, has_b, IA, IB, qa, na, qb, nb, &res[ii], lane);
           __syncwarp();
         }
       }

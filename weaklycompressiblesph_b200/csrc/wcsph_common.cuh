@@ -91,6 +91,9 @@ struct InstParams {
   float dt_nu;            // 0.125 h^2 / nu (or +inf)
   float kill_lo[3], kill_hi[3];
   float slab_margin2;     // slab instances: squared largest drift a step may make (0: not a slab)
+  float cell[3];          // cell edge per axis
+  float h16_band;         // half2 list pass: squared-distance band around (2h)^2 and 0 within which the
+                          // 16-bit positions cannot decide the support test (exact FP32 test there)
   float HL2;              // neighbour lists: squared list radius (2h + skin)^2
   float inv_skin;         // neighbour lists: 1 / skin (0: lists off)
   double t_end;
