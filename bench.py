@@ -60,6 +60,11 @@ def parse():
                     help="skip the run of the other list-mode precision (half2 beside FP32, or the reverse)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble and serving samples")
     ap.add_argument("--ensemble-steps", type=int, default=60)
+    ap.add_argument("--ensemble-precision", default="half2", choices=["tiled", "half2"],
+                    help="precision of the batched ensemble and served requests (config: half2 pairs)")
+    ap.add_argument("--serving-requests", type=int, default=16)
+    ap.add_argument("--serving-nmax", type=float, default=2e5, help="largest request (config: 2e6 particles)")
+    ap.add_argument("--serving-tend", type=float, default=0.1, help="physical end time (config: 1.0 s)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
@@ -453,13 +458,16 @@ def measure_ensemble(device, steps=None):
     from weaklycompressiblesph_b200 import cases, ensemble
     steps = steps or ARGS.ensemble_steps
     ens = cases.ensemble_cases(count=64, seed=2024)
-    b = ensemble.run_batched(ens, steps=steps, warmup=3, device=device, list_interval=ARGS.list_interval)
+    b = ensemble.run_batched(ens, steps=steps, warmup=3, device=device, list_interval=ARGS.list_interval,
+                             precision=ARGS.ensemble_precision)
     s = ensemble.run_serial(ens, steps=steps, warmup=3, precision="fp32", device=device)
     return {"instances": len(ens), "particles": b["particles"], "steps": steps,
+            "precision": ARGS.ensemble_precision,
             "batched_particle_steps_per_s": b["particle_steps_per_s"],
             "serial_plain_particle_steps_per_s": s["particle_steps_per_s"],
             "speedup_vs_serial_plain": b["particle_steps_per_s"] / s["particle_steps_per_s"],
-            "sample": f"{steps} timed steps per instance (config: 2000)",
+            "tuning": b.get("tuning"),
+            "sample": f"{steps} timed steps per instance" + ("" if steps >= 2000 else " (config: 2000)"),
             "neighbour_search": (f"lists, rebuilt at least every {ARGS.list_interval} steps" if ARGS.list_interval
                                  else "every step") + "; serial baseline: plain FP32, search every step"}
 
@@ -473,10 +481,11 @@ def measure_serving(device):
     from weaklycompressiblesph_b200 import _native as N
     from weaklycompressiblesph_b200 import cases
     from weaklycompressiblesph_b200.serving import Server, run_alone
-    reqs = cases.serving_requests(count=16, rate=20.0, seed=7, n_min=2e4, n_max=2e5, t_end=0.1)
+    reqs = cases.serving_requests(count=ARGS.serving_requests, rate=20.0, seed=7, n_min=2e4,
+                                  n_max=ARGS.serving_nmax, t_end=ARGS.serving_tend)
     total = sum(c.n for _, c in reqs)
     with Server(budget_bytes=150e9, max_particles=total + 1024, device=device, read_results=False,
-                list_interval=ARGS.list_interval) as srv:
+                list_interval=ARGS.list_interval, precision=precision_code(ARGS.ensemble_precision)) as srv:
         out = srv.run(reqs)
     el = 0.0
     ps = 0
@@ -490,8 +499,11 @@ def measure_serving(device):
             "speedup_vs_serial_plain": out["particle_steps_per_s"] / (ps / el),
             "neighbour_search": (f"lists, rebuilt at least every {ARGS.list_interval} steps" if ARGS.list_interval
                                  else "every step") + "; serial baseline: plain FP32, search every step",
-            "sample": "16 requests, counts log-uniform [2e4, 2e5], t_end 0.1 s, Poisson 20/s, budget 150 GB "
-                      "(config: counts to 2e6, t_end 1.0 s)"}
+            "precision": ARGS.ensemble_precision,
+            "sample": f"{len(reqs)} requests, counts log-uniform [2e4, {ARGS.serving_nmax:.0e}], "
+                      f"t_end {ARGS.serving_tend:g} s, Poisson 20/s, budget 150 GB"
+                      + ("" if ARGS.serving_nmax >= 2e6 and ARGS.serving_tend >= 1.0
+                         else " (config: counts to 2e6, t_end 1.0 s)")}
 
 
 ARGS = None

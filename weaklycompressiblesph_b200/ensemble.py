@@ -36,8 +36,9 @@ def run_batched(cases, steps, precision="tiled", warmup=3, device=0, list_interv
         st = [s.status(k) for k in slots]
         states = [s.read(k) for k in slots] if read else None
         lists = s.list_stats() if list_interval else None
+        tuning = s.tuning()
     return dict(seconds=el, steps=steps, particles=total, particle_steps_per_s=total * steps / el,
-                status=st, states=states, lists=lists)
+                status=st, states=states, lists=lists, tuning=tuning)
 
 
 def run_serial(cases, steps, precision="fp32", warmup=3, device=0, list_interval=0, read=False):
