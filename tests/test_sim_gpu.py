@@ -230,14 +230,15 @@ def test_conservation_sums_fp64(prec, native, lists):
         st = s.read(k)
         c = s.conservation(k)
     alive = st["alive"] == 1
-    m = case.mass
+    m = float(np.float32(case.mass))  # the device holds the mass in FP32 and sums in FP64
     v = st["vel"][alive].astype(np.float64)
     a = st["acc"][alive].astype(np.float64)
     assert c[0] == pytest.approx(m * alive.sum(), rel=1e-12)
     np.testing.assert_allclose(c[1:4], m * v.sum(axis=0), rtol=1e-9, atol=1e-12 * m * np.abs(v).sum())
     assert c[4] == pytest.approx(0.5 * m * (v * v).sum(), rel=1e-9)
-    ref5 = m * (a[:, 2] + case.phys.g).sum()
+    g = float(np.float32(case.phys.g))  # gravity as the device holds it
+    ref5 = m * (a[:, 2] + g).sum()
     assert c[5] == pytest.approx(ref5, rel=1e-9, abs=1e-12 * m * np.abs(a[:, 2]).sum())
     # the pair forces cancel: their vertical total is rounding noise next to the
     # sum of their magnitudes
-    assert abs(c[5]) < 1e-5 * m * np.abs(a[:, 2] + case.phys.g).sum()
+    assert abs(c[5]) < 1e-5 * m * np.abs(a[:, 2] + g).sum()

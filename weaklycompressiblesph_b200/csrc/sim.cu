@@ -382,13 +382,12 @@ static int autotune(SimImpl& S) {
   }
   S.tile_shape = best_shape;
   if (S.opt.list_interval > 0) {
-    // The list pass: a probe build pass makes lists of the current state
-    // (they serve the steps that follow), then every launch shape is timed
-    // on them with probe launches (diagnostics only, state untouched).
+    // The list pass: a probe build pass makes lists of the current state,
+    // then every launch shape is timed on them with probe launches
+    // (diagnostics only, state untouched).  The lists are dropped afterwards:
+    // the first step builds its own, with the overflow and drift checks of a
+    // step's build.
     if (int rc = enqueue_pass(S, a, false, false, nullptr, nullptr, true)) return rc;
-    S.lists_valid = true;
-    S.since_build = 0;
-    S.last_disp = 0.f;
     StepArgs b = make_args(S);
     b.list_reuse = 1;
     b.x0 = S.x0;
@@ -403,6 +402,7 @@ static int autotune(SimImpl& S) {
       if (ms < best_list) best_list = ms, best_list_shape = v;
     }
     S.list_shape = best_list_shape;
+    S.lists_valid = false;
   }
   S.tuned_bucket = bucket;
   S.graph_dirty = true;

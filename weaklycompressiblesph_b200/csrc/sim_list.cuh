@@ -213,8 +213,11 @@ __device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P
   float r2a = lo(R2raw), r2b = hi(R2raw);
   const bool xa = qva && (ha == kFarMark || r2a < H.band || fabsf(r2a - C.H2) < H.band);
   const bool xb = qvb && (hb == kFarMark || r2b < H.band || fabsf(r2b - C.H2) < H.band);
-  float rja = P.rho0 + __half2float(__ushort_as_half((unsigned short)ha));
-  float rjb = P.rho0 + __half2float(__ushort_as_half((unsigned short)hb));
+  // a far record's density comes from its FP32 record (exact path); an idle
+  // half naming one still needs a finite stand-in (its terms are multiplied
+  // by zero, and NaN times zero is NaN)
+  float rja = ha == kFarMark ? P.rho0 : P.rho0 + __half2float(__ushort_as_half((unsigned short)ha));
+  float rjb = hb == kFarMark ? P.rho0 : P.rho0 + __half2float(__ushort_as_half((unsigned short)hb));
   if (xa || xb) {  // rare: the exact FP32 displacement of the FP32 path
     float dx[2] = {lo(DX), hi(DX)}, dy[2] = {lo(DY), hi(DY)}, dz[2] = {lo(DZ), hi(DZ)}, r2[2] = {r2a, r2b};
     float rj[2] = {rja, rjb};
