@@ -290,7 +290,8 @@ def run_device(case, prec_name, steps, warmup, device, clocks=False, list_interv
             b, r = ls1["builds"] - ls0["builds"], ls1["list_steps"] - ls0["list_steps"]
             res["kernels_per_step"] = (b * ls1["kernels_build"] + r * ls1["kernels_list"]) / max(1, b + r)
             res["lists"] = {"interval": list_interval, "skin_h": list_skin or 0.3, "timed_builds": b,
-                            "timed_list_steps": r, "overflows": ls1["overflows"], "longest": ls1["longest"]}
+                            "timed_list_steps": r, "overflows": ls1["overflows"], "longest": ls1["longest"],
+                            "entries": s.list_entries()}
         # per-phase kernel times (eager launches, CUDA events on the solver stream)
         prof_steps = max(3, min(20, steps // 5))
         ph = s.profile_steps(prof_steps)
@@ -666,21 +667,26 @@ def validation_errors(workload, prec):
 
 
 def l1_roofline(workload, prec, dev):
-    """The list pass is bound by the L1 data pipe that delivers its j-record
-    gathers: L1 wavefronts per true pair from one ncu capture of the pass,
-    against the minimum its record and list-entry bytes need at 128 B per
-    wavefront (profiles/hydro_list_l1.json)."""
+    """The list pass is bound by the L1 data pipe that delivers its gathers.
+    Per list entry it needs one list word and one j-record: at 128 B per L1
+    wavefront that is (4 + record bytes) / 128 wavefronts at least.  The
+    measured L1 load wavefronts of one launch come from the ncu capture
+    summarised in profiles/hydro_list_l1.json; entries and true pairs are this
+    run's."""
     t = _profile_json("hydro_list_l1.json")
-    if not t or not dev.get("lists"):
+    lists = dev.get("lists")
+    if not t or not lists or not lists.get("entries"):
         return None
     r = t.get(f"{workload}/{prec}")
     if not r:
         return None
-    return {"bound": "l1", "wavefronts_per_pair": r["wavefronts"] / r["pairs"],
-            "min_wavefronts_per_pair": r["entries"] * r["bytes_per_entry"] / 128.0 / r["pairs"],
-            "frac": (r["entries"] * r["bytes_per_entry"] / 128.0) / r["wavefronts"],
-            "l1_pipe_util": r.get("l1_pipe_util"), "bytes_per_entry": r["bytes_per_entry"],
-            "source": "ncu capture summarised in profiles/hydro_list_l1.json"}
+    entries, pairs = lists["entries"], dev["pairs_per_step"]
+    need = entries * (4 + r["record_bytes"]) / 128.0
+    return {"bound": "l1", "wavefronts_per_launch": r["wavefronts"], "min_wavefronts_per_launch": need,
+            "frac": need / r["wavefronts"], "wavefronts_per_pair": r["wavefronts"] / pairs,
+            "entries_per_pair": entries / pairs, "record_bytes": r["record_bytes"],
+            "l1_pipe_util_pct": r.get("l1_pipe_util_pct"),
+            "source": "ncu capture of one list-pass launch, profiles/hydro_list_l1.json"}
 
 
 def bench_config(args, case, prec, world):

@@ -366,6 +366,10 @@ int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out3);
  * step builds again), out[3] largest list built so far, out[4] kernel
  * launches of a build step, out[5] kernel launches of a list step. */
 int wcsph_sim_list_stats(wcsph_sim* sim, int64_t* out6);
+/* Entries of the current neighbour lists over all particles (what one list
+ * pass reads: each entry a list word and a j-record), 0 without current
+ * lists, -1 on error. */
+int64_t wcsph_sim_list_entries(wcsph_sim* sim);
 /* Drop the current neighbour lists (list_interval > 0): the next step builds
  * them again, as after a change of the instance set.  For callers that edit
  * state outside the solver, and for timing a build-inclusive sequence of

@@ -124,6 +124,7 @@ _SIGS = {
     "wcsph_sim_tuning": (C.c_int, [P, I32P]),
     "wcsph_fdps_stats": (C.c_int, [C.c_int32, C.POINTER(C.c_int64)]),
     "wcsph_sim_invalidate_lists": (C.c_int, [P]),
+    "wcsph_sim_list_entries": (C.c_int64, [P]),
     "wcsph_sim_profile_steps": (C.c_int, [P, C.c_int32, F64P]),
 }
 

@@ -1477,6 +1477,21 @@ int wcsph_sim_list_stats(wcsph_sim* sim, int64_t* out6) {
   return 0;
 }
 
+int64_t wcsph_sim_list_entries(wcsph_sim* sim) {
+  if (!sim) return -1;
+  SimImpl& S = sim->impl;
+  if (S.opt.list_interval <= 0 || !S.lists_valid) return 0;
+  if (cudaSetDevice(S.opt.device) != cudaSuccess || cudaStreamSynchronize(S.s) != cudaSuccess) return -1;
+  int n_alive = 0;
+  if (cudaMemcpy(&n_alive, S.d_n_alive, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  std::vector<int> cnt(std::max(0, n_alive));
+  if (n_alive > 0 && cudaMemcpy(cnt.data(), S.list_cnt, sizeof(int) * n_alive, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  int64_t tot = 0;
+  for (int c : cnt) tot += std::min(c, kListMax);
+  return tot;
+}
+
 int wcsph_sim_invalidate_lists(wcsph_sim* sim) {
   if (!sim) return WCSPH_E_INVALID;
   sim->impl.lists_valid = false;

@@ -221,6 +221,13 @@ class Solver:
         return dict(builds=int(out[0]), list_steps=int(out[1]), overflows=int(out[2]), longest=int(out[3]),
                     kernels_build=int(out[4]), kernels_list=int(out[5]))
 
+    def list_entries(self):
+        """Entries of the current neighbour lists (0 without current lists)."""
+        v = int(N.lib().wcsph_sim_list_entries(self._h))
+        if v < 0:
+            raise N.WcsphError("wcsph_sim_list_entries", -1, "CUDA error")
+        return v
+
     def invalidate_lists(self):
         """The next step rebuilds the neighbour lists (wcsph_sim_invalidate_lists)."""
         N.call("wcsph_sim_invalidate_lists", self._h)
