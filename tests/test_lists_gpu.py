@@ -220,11 +220,16 @@ def test_list_pass_periodic_vs_fp64(prec, native, oracle_lib):
     next build); the oracle sees the wrapped positions."""
     case = cases.periodic_lattice(n_side=20, dx=0.01, seed=21)
     rng = np.random.default_rng(22)
-    case.vel = rng.normal(0.0, 0.7, size=case.vel.shape)
+    case.vel = rng.normal(0.0, 0.1, size=case.vel.shape)
+    # shift the lattice so that a layer sits just inside the +x face, and send
+    # it outward: it crosses the face on the list steps after the first build
+    side = case.hi[0] - case.lo[0]
+    case.pos[:, 0] = np.mod(case.pos[:, 0] + 0.0048, side)
+    case.vel[case.pos[:, 0] > side - 0.0006, 0] = 3.0
     # the default skin: 2.3 h holds about 110 lattice neighbours (a list holds 192)
     with Solver(case.n, precision=prec, list_interval=50) as s:
         k = s.add(case)
-        s.step(6)
+        s.step(3)
         st = s.read(k)
         pr = s.probe(k, density_pass=1, lists=True)
         stats = s.list_stats()
