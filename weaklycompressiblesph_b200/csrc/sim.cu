@@ -84,16 +84,13 @@ struct SimImpl {
   float4* x0 = nullptr;
   float4* jv = nullptr;  // compact j-records of the half2 list pass
   uint2* jq = nullptr;
-  unsigned* d_lflags = nullptr;       // see StepArgs::list_flags
+  unsigned* d_lflags = nullptr;       // kLfWords words, see ListFlag
+  unsigned* d_motion = nullptr;       // 3 words per instance, see StepArgs::inst_motion
   unsigned* h_lflags = nullptr;       // pinned copy, written at the end of every list-mode step
-  cudaGraphExec_t gexec_reuse = nullptr;
   cudaEvent_t step_ev[2] = {nullptr, nullptr};
-  bool lists_valid = false;
-  int since_build = 0;
+  bool lists_valid = false;           // false: the next step is asked to build (kLfForce)
   int kernels_reuse = 0;
-  long long steps_launched = 0, last_build = -1;
-  long long n_builds = 0, n_reuse = 0, n_overflow = 0;
-  float last_disp = 0.f, last_drift = 0.f;  // from the latest completed step, in units of the skin
+  long long steps_launched = 0;
 };
 
 constexpr int kListMax = kListMaxEntries;  // entries per particle list (2h + 0.3 h holds ~100-115 at h = 1.3 dx)
@@ -203,6 +200,7 @@ static StepArgs make_args(SimImpl& S) {
     a.list_cnt = S.list_cnt;
     a.list_max = kListMax;
     a.list_flags = S.d_lflags;
+    a.inst_motion = S.d_motion;
     a.jv = S.jv;
     a.jq = S.jq;
   }
@@ -220,15 +218,30 @@ static inline int nblk(long long n) { return (int)std::max<long long>(1, (n + kB
 
 // Enqueue one pass of the pipeline.  init_filter adds the initial Shepard
 // filter after the hydro pass (main.cpp:75).  Returns the kernel-launch count.
+// After k_step_begin ran with list_reuse set (the list-step prologue): the
+// ranges the binning sets again, and the slot count of a binning pass.
+__global__ void k_begin_build(StepArgs a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < a.n_inst) {
+    a.dyn[k].range_lo = 0x7fffffff;
+    a.dyn[k].range_hi = 0;
+  }
+  if (k == 0) *a.n_alive = a.n_host;
+}
+
 static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, int* launches,
-                        cudaEvent_t* ev = nullptr, bool build_lists = false) {
+                        cudaEvent_t* ev = nullptr, bool build_lists = false, bool after_prologue = false) {
   int L = 0;
   const int n = S.n_host;
   if (build_lists) a.x0 = S.x0;
   else S.lists_valid = false;  // any other pass re-sorts or changes what the lists refer to
-  if (ev) WCSPH_CUDA(cudaEventRecord(ev[0], S.s));
-  WCSPH_CUDA(cudaMemsetAsync(S.d_counters + 4, 0, sizeof(int), S.s));
-  k_step_begin<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
+  if (after_prologue) {  // a list-mode build branch: the step has begun
+    k_begin_build<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
+  } else {
+    if (ev) WCSPH_CUDA(cudaEventRecord(ev[0], S.s));
+    WCSPH_CUDA(cudaMemsetAsync(S.d_counters + 4, 0, sizeof(int), S.s));
+    k_step_begin<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
+  }
   ++L;
   if (n > 0) {
     k_kick_bin<<<nblk(n), kBlock, 0, S.s>>>(a);
@@ -287,15 +300,13 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
 }
 
 // A step that reads the neighbour lists (sim_list.cuh): no sort, no scan.
+// The list-step branch (the step has begun in the prologue).
 static int enqueue_reuse(SimImpl& S, StepArgs a, bool density, int* launches, cudaEvent_t* ev = nullptr) {
   const int n = S.n_host;
   a.list_reuse = 1;
   a.x0 = S.x0;    // read by k_kick_refresh (the displacement since the build)
   a.alt = a.main;  // in place: no re-sort, each particle's state is its own thread's
-  if (ev) WCSPH_CUDA(cudaEventRecord(ev[0], S.s));
-  WCSPH_CUDA(cudaMemsetAsync(S.d_counters + 4, 0, sizeof(int), S.s));
-  k_step_begin<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
-  int L = 1;
+  int L = 0;
   if (n > 0) {
     k_kick_refresh<<<nblk(n), kBlock, 0, S.s>>>(a);
     ++L;
@@ -403,6 +414,7 @@ static int autotune(SimImpl& S) {
     }
     S.list_shape = best_list_shape;
     S.lists_valid = false;
+    WCSPH_CUDA(cudaMemsetAsync(S.d_lflags + kLfOverflowPending, 0, sizeof(unsigned), S.s));
   }
   S.tuned_bucket = bucket;
   S.graph_dirty = true;
@@ -498,65 +510,64 @@ static int fill_params(const wcsph_instance_desc& d, HostInst& I, InstParams& P)
 }
 
 // ------------------------------------------------------- neighbour lists
-// Flags of the latest completed step.  Sticky errors are handled after
-// draining the stream, so that they are seen and cleared exactly once.
+// Sticky errors of the latest completed step, handled after draining the
+// stream, so that they are seen and cleared exactly once.
 static int read_list_flags(SimImpl& S) {
   volatile unsigned* h = S.h_lflags;
-  if (h[2]) {
+  if (h[kLfErr]) {
     WCSPH_CUDA(cudaStreamSynchronize(S.s));
-    const unsigned e = h[2];
-    h[2] = 0u;
-    WCSPH_CUDA(cudaMemsetAsync(S.d_lflags + 2, 0, sizeof(unsigned), S.s));
+    h[kLfErr] = 0u;
+    WCSPH_CUDA(cudaMemsetAsync(S.d_lflags + kLfErr, 0, sizeof(unsigned), S.s));
     WCSPH_CUDA(cudaStreamSynchronize(S.s));
     S.lists_valid = false;
-    if (e & 2u) ++S.n_overflow;
-    if (e & 1u) {
-      set_error("wcsph_sim_step: a particle moved more than half the neighbour-list skin between list builds; "
-                "the step's pair sums may be incomplete (raise list_skin or lower list_interval)");
-      return WCSPH_E_STATE;
-    }
+    set_error("wcsph_sim_step: a particle moved more than half the neighbour-list skin between list builds; "
+              "the step's pair sums may be incomplete (raise list_skin or lower list_interval)");
+    return WCSPH_E_STATE;
   }
-  const unsigned u0 = h[0], u1 = h[1];
-  memcpy(&S.last_disp, &u0, sizeof(float));
-  memcpy(&S.last_drift, &u1, sizeof(float));
   return 0;
 }
 
-// One step in list mode.  Build when the lists are stale, K steps old, or
-// the displacement since the build plus 2.5 steps of
-// the latest drift would pass half the skin (the decision sees the step
-// before the one in flight).  At most two steps are in flight; a build is
-// waited for, since its lists may have overflowed.
+// The prologue of a list-mode step: dt rotation (k_step_begin, keeping the
+// build's order), then the device's build decision (k_list_set), which sets
+// the condition `cond` when use_cond.
+static int enqueue_list_prologue(SimImpl& S, const StepArgs& a0, cudaGraphConditionalHandle cond, bool use_cond,
+                                 cudaEvent_t* ev) {
+  StepArgs a = a0;
+  a.list_reuse = 1;
+  a.x0 = S.x0;
+  if (ev) WCSPH_CUDA(cudaEventRecord(ev[0], S.s));
+  WCSPH_CUDA(cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s));
+  WCSPH_CUDA(cudaMemsetAsync(S.d_counters + 4, 0, sizeof(int), S.s));
+  k_step_begin<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
+  k_list_set<<<1, 1, 0, S.s>>>(a, S.opt.list_interval, cond, use_cond ? 1 : 0);
+  WCSPH_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// One step in list mode.  Stale lists are marked for the device (kLfForce);
+// the device decides whether the step builds.  At most two steps are in
+// flight; the flags are read one step behind.
 static int list_step(SimImpl& S, bool graph, cudaEvent_t* ev) {
-  const bool build = !S.lists_valid || S.since_build >= S.opt.list_interval ||
-                     S.last_disp + 2.5f * S.last_drift > 0.5f;
+  if (!S.lists_valid) {
+    WCSPH_CUDA(cudaMemsetAsync(S.d_lflags + kLfForce, 0x01, sizeof(unsigned), S.s));
+    S.lists_valid = true;
+  }
   if (graph) {
-    WCSPH_CUDA(cudaGraphLaunch(build ? S.gexec : S.gexec_reuse, S.s));
+    WCSPH_CUDA(cudaGraphLaunch(S.gexec, S.s));
   } else {
     StepArgs a = make_args(S);
-    WCSPH_CUDA(cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s));
-    WCSPH_CUDA(cudaMemsetAsync(S.d_lflags, 0, 2 * sizeof(unsigned), S.s));
-    const int rc = build ? enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step, ev, true)
+    if (int rc = enqueue_list_prologue(S, a, 0, false, ev)) return rc;
+    unsigned build = 0;
+    WCSPH_CUDA(cudaMemcpyAsync(&build, S.d_lflags + kLfDecision, sizeof(unsigned), cudaMemcpyDeviceToHost, S.s));
+    WCSPH_CUDA(cudaStreamSynchronize(S.s));
+    const int rc = build ? enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step, ev, true, true)
                          : enqueue_reuse(S, a, S.any_density, &S.kernels_reuse, ev);
     if (rc) return rc;
-    WCSPH_CUDA(cudaMemcpyAsync(S.h_lflags, S.d_lflags, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, S.s));
-  }
-  if (build) {
-    S.lists_valid = true;
-    S.since_build = 1;
-    S.last_disp = 0.f;
-    ++S.n_builds;
-  } else {
-    ++S.since_build;
-    ++S.n_reuse;
+    WCSPH_CUDA(cudaMemcpyAsync(S.h_lflags, S.d_lflags, kLfWords * sizeof(unsigned), cudaMemcpyDeviceToHost, S.s));
   }
   const int par = (int)(S.steps_launched & 1);
   WCSPH_CUDA(cudaEventRecord(S.step_ev[par], S.s));
   ++S.steps_launched;
-  if (build) {
-    WCSPH_CUDA(cudaEventSynchronize(S.step_ev[par]));
-    return read_list_flags(S);
-  }
   if (S.steps_launched >= 2) {
     WCSPH_CUDA(cudaEventSynchronize(S.step_ev[par ^ 1]));
     return read_list_flags(S);
@@ -564,38 +575,67 @@ static int list_step(SimImpl& S, bool graph, cudaEvent_t* ev) {
   return 0;
 }
 
-// Capture the build-step and list-step graphs.
-static int capture_list_graphs(SimImpl& S) {
-  StepArgs a = make_args(S);
-  for (int kind = 0; kind < 2; ++kind) {
-    cudaGraphExec_t& X = kind == 0 ? S.gexec : S.gexec_reuse;
-    if (X) {
-      cudaGraphExecDestroy(X);
-      X = nullptr;
-    }
-    cudaGraph_t g;
-    WCSPH_CUDA(cudaStreamBeginCapture(S.s, cudaStreamCaptureModeThreadLocal));
-    int rc = 0;
-    if (cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s) != cudaSuccess ||
-        cudaMemsetAsync(S.d_lflags, 0, 2 * sizeof(unsigned), S.s) != cudaSuccess)
-      rc = WCSPH_E_CUDA;
-    if (!rc)
-      rc = kind == 0 ? enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step, nullptr, true)
-                     : enqueue_reuse(S, a, S.any_density, &S.kernels_reuse);
-    if (!rc && cudaMemcpyAsync(S.h_lflags, S.d_lflags, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, S.s) !=
-                   cudaSuccess)
-      rc = WCSPH_E_CUDA;
-    cudaError_t e = cudaStreamEndCapture(S.s, &g);
-    if (rc) {
-      if (e == cudaSuccess) cudaGraphDestroy(g);
-      set_error("capturing the neighbour-list step graphs failed");
-      return rc;
-    }
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
-    e = cudaGraphInstantiate(&X, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+// The list-mode step graph: the prologue, then a conditional node whose IF
+// branch is a build step (binning, sort, scan-only tiled pass, list pass) and
+// whose ELSE branch is a list step (kick and refresh in place, list passes),
+// then the copy of the flags to the host.
+static int capture_list_graph(SimImpl& S) {
+  if (S.gexec) {
+    cudaGraphExecDestroy(S.gexec);
+    S.gexec = nullptr;
   }
+  StepArgs a = make_args(S);
+  cudaGraph_t g = nullptr;
+  WCSPH_CUDA(cudaGraphCreate(&g, 0));
+  auto fail = [&](int rc, const char* what) {
+    cudaGraphDestroy(g);
+    if (rc == WCSPH_E_CUDA || rc == 0) set_error("capturing the neighbour-list step graph failed (%s)", what);
+    return rc ? rc : WCSPH_E_CUDA;
+  };
+  cudaGraphConditionalHandle cond;
+  if (cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault) != cudaSuccess)
+    return fail(WCSPH_E_CUDA, "conditional handle");
+  const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+  if (cudaStreamBeginCaptureToGraph(S.s, g, nullptr, nullptr, 0, mode) != cudaSuccess)
+    return fail(WCSPH_E_CUDA, "begin capture");
+  int rc = enqueue_list_prologue(S, a, cond, true, nullptr);
+  cudaGraphNodeParams cp = {};
+  cudaGraphNode_t cnode = nullptr;
+  if (!rc) {
+    cudaStreamCaptureStatus st;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 2;  // IF: build; ELSE: list step
+    if (cudaStreamGetCaptureInfo(S.s, &st, nullptr, &cg, &deps, &ndeps) != cudaSuccess ||
+        cudaGraphAddNode(&cnode, cg, deps, ndeps, &cp) != cudaSuccess ||
+        cudaStreamUpdateCaptureDependencies(S.s, &cnode, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+      rc = WCSPH_E_CUDA;
+  }
+  if (!rc && cudaMemcpyAsync(S.h_lflags, S.d_lflags, kLfWords * sizeof(unsigned), cudaMemcpyDeviceToHost, S.s) !=
+                 cudaSuccess)
+    rc = WCSPH_E_CUDA;
+  cudaGraph_t out = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(S.s, &out);
+  if (rc || e != cudaSuccess) return fail(rc, "prologue");
+  for (int branch = 0; branch < 2; ++branch) {
+    if (cudaStreamBeginCaptureToGraph(S.s, cp.conditional.phGraph_out[branch], nullptr, nullptr, 0, mode) !=
+        cudaSuccess)
+      return fail(WCSPH_E_CUDA, "begin branch capture");
+    rc = branch == 0 ? enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step, nullptr, true, true)
+                     : enqueue_reuse(S, a, S.any_density, &S.kernels_reuse);
+    cudaGraph_t bo = nullptr;
+    const cudaError_t eb = cudaStreamEndCapture(S.s, &bo);
+    if (rc || eb != cudaSuccess) return fail(rc, branch == 0 ? "build branch" : "list-step branch");
+  }
+  const cudaError_t ei = cudaGraphInstantiate(&S.gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) return cuda_fail(ei, "cudaGraphInstantiate (list step)", __FILE__, __LINE__);
+  S.kernels_per_step += 2;  // the prologue's kernels
+  S.kernels_reuse += 2;
   S.graph_dirty = false;
   return 0;
 }
@@ -682,12 +722,13 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
     rc |= alloc(S, (void**)&S.list, N * kListMax * sizeof(uint32_t));
     rc |= alloc(S, (void**)&S.list_cnt, N * sizeof(int));
     rc |= alloc(S, (void**)&S.x0, N * sizeof(float4));
-    rc |= alloc(S, (void**)&S.d_lflags, 4 * sizeof(unsigned));
+    rc |= alloc(S, (void**)&S.d_lflags, kLfWords * sizeof(unsigned));
+    rc |= alloc(S, (void**)&S.d_motion, 3 * (size_t)opt->max_instances * sizeof(unsigned));
     if (h16_lists(*opt)) {
       rc |= alloc(S, (void**)&S.jv, N * sizeof(float4));
       rc |= alloc(S, (void**)&S.jq, N * sizeof(uint2));
     }
-    if (!rc && cudaHostAlloc((void**)&S.h_lflags, 4 * sizeof(unsigned), cudaHostAllocDefault) != cudaSuccess)
+    if (!rc && cudaHostAlloc((void**)&S.h_lflags, kLfWords * sizeof(unsigned), cudaHostAllocDefault) != cudaSuccess)
       rc = 1;
   }
   if (rc) {
@@ -702,8 +743,10 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
       cudaEventCreateWithFlags(&S.step_ev[1], cudaEventDisableTiming) != cudaSuccess)
     return fail(WCSPH_E_CUDA);
   if (S.d_lflags) {
-    memset(S.h_lflags, 0, 4 * sizeof(unsigned));
-    if (cudaMemsetAsync(S.d_lflags, 0, 4 * sizeof(unsigned), S.s) != cudaSuccess) return fail(WCSPH_E_CUDA);
+    memset(S.h_lflags, 0, kLfWords * sizeof(unsigned));
+    if (cudaMemsetAsync(S.d_lflags, 0, kLfWords * sizeof(unsigned), S.s) != cudaSuccess ||
+        cudaMemsetAsync(S.d_motion, 0, 3 * (size_t)opt->max_instances * sizeof(unsigned), S.s) != cudaSuccess)
+      return fail(WCSPH_E_CUDA);
   }
   *out = sim;
   return 0;
@@ -715,7 +758,6 @@ int wcsph_sim_destroy(wcsph_sim* sim) {
   cudaSetDevice(S.opt.device);
   cudaStreamSynchronize(S.s);
   if (S.gexec) cudaGraphExecDestroy(S.gexec);
-  if (S.gexec_reuse) cudaGraphExecDestroy(S.gexec_reuse);
   for (void* p : S.allocs) cudaFree(p);
   if (S.h_lflags) cudaFreeHost(S.h_lflags);
   for (cudaEvent_t e : S.step_ev)
@@ -1132,9 +1174,9 @@ int wcsph_sim_step(wcsph_sim* sim, int32_t nsteps) {
   WCSPH_CUDA(cudaSetDevice(S.opt.device));
   if (nsteps == 0) return 0;
   if (S.opt.list_interval > 0) {
-    if (S.opt.use_graph && (S.graph_dirty || !S.gexec || !S.gexec_reuse)) {
+    if (S.opt.use_graph && (S.graph_dirty || !S.gexec)) {
       if (int rc = autotune(S)) return rc;
-      if (int rc = capture_list_graphs(S)) return rc;
+      if (int rc = capture_list_graph(S)) return rc;
     }
     for (int t = 0; t < nsteps; ++t)
       if (int rc = list_step(S, S.opt.use_graph != 0, nullptr)) return rc;
@@ -1392,11 +1434,11 @@ int wcsph_sim_probe_lists(wcsph_sim* sim, int32_t slot, int32_t density_pass, fl
     StepArgs a = make_args(S);
     a.probe_density = density_pass;
     rc = enqueue_pass(S, a, density_pass != 0, false, nullptr, nullptr, true);
-    if (!rc) {
+    if (!rc) {  // the device's schedule starts from these lists
       S.lists_valid = true;
-      S.since_build = 0;
-      S.last_disp = 0.f;
-      S.graph_dirty = true;
+      if (cudaMemsetAsync(S.d_lflags + kLfSince, 0, sizeof(unsigned), S.s) != cudaSuccess ||
+          cudaMemsetAsync(S.d_lflags + kLfForce, 0, sizeof(unsigned), S.s) != cudaSuccess)
+        rc = WCSPH_E_CUDA;
     }
   }
   int rc2 = set_all_phases(S, PH_STEP);
@@ -1466,12 +1508,12 @@ int wcsph_sim_list_stats(wcsph_sim* sim, int64_t* out6) {
   SimImpl& S = sim->impl;
   WCSPH_CUDA(cudaSetDevice(S.opt.device));
   WCSPH_CUDA(cudaStreamSynchronize(S.s));
-  unsigned mx = 0;
-  if (S.d_lflags) WCSPH_CUDA(cudaMemcpy(&mx, S.d_lflags + 3, sizeof(mx), cudaMemcpyDeviceToHost));
-  out6[0] = S.n_builds;
-  out6[1] = S.n_reuse;
-  out6[2] = S.n_overflow;
-  out6[3] = (int64_t)mx;
+  unsigned lf[kLfWords] = {};
+  if (S.d_lflags) WCSPH_CUDA(cudaMemcpy(lf, S.d_lflags, sizeof(lf), cudaMemcpyDeviceToHost));
+  out6[0] = lf[kLfBuilds];
+  out6[1] = lf[kLfListSteps];
+  out6[2] = lf[kLfOverflows] + (lf[kLfOverflowPending] ? 1 : 0);
+  out6[3] = (int64_t)lf[kLfLongest];
   out6[4] = S.kernels_per_step;
   out6[5] = S.kernels_reuse;
   return 0;

@@ -106,10 +106,12 @@ struct StepArgs {
   int* list_cnt;          // entries per slot
   int list_max;
   float4* x0;             // build steps: record the positions the lists were built at
-  unsigned* list_flags;   // [0] max |x - x0| / skin, [1] max step drift / skin (float bits),
-                          // [2] sticky errors (1 skin exceeded, 2 overflow), [3] largest list
+  unsigned* list_flags;   // kLf* words (sim_list.cuh): displacement and drift maxima, sticky errors,
+                          // largest list, the device's rebuild decision and its counters
   int list_reuse;         // this step reads the lists: periodic wrapping waits for the next build
   int* dens_any;          // set by k_step_begin when any instance has a density pass in this launch
+  unsigned* inst_motion;  // neighbour lists: per instance, the largest |x - x0|, |v| and |a| over its moving
+                          // particles at the end of the step, in units of its skin (float bits)
   // compact j-records of the half2 list pass (WCSPH_PREC_HALF2 with lists; null otherwise)
   float4* jv;             // (vx, vy, vz, P/rho^2)
   uint2* jq;              // 16-bit cell-relative x, y, z and (rho - rho0) as a half (h16_record)
@@ -189,10 +191,9 @@ __device__ __forceinline__ bool wrap_periodic(const InstParams& P, float4& x) {
 // KDK first half of one live particle p of a stepping instance
 // (class.h:146-159 as main.cpp:98-103 runs it), periodic wrap (not on list
 // steps), escapee removal (Dam2.h:117-122).  Returns true when the state
-// changed; dead is set when the particle left the kill box; drift_bits
-// receives this step's drift in units of the neighbour-list skin.
+// changed; dead is set when the particle left the kill box.
 __device__ __forceinline__ bool kick_particle(const StepArgs& a, const InstParams& P, int inst, int p, uint32_t f,
-                                              float4& x, float4& v, float4& vh, bool& dead, unsigned& drift_bits) {
+                                              float4& x, float4& v, float4& vh, bool& dead) {
   const int ph = a.phase[inst];
   const float dt = a.dyn[inst].dt_cur;
   if (!(ph == PH_STEP && dt > 0.0f)) return false;
@@ -206,8 +207,6 @@ __device__ __forceinline__ bool kick_particle(const StepArgs& a, const InstParam
     x.z += dt * vh.z;
     if (P.slab_margin2 > 0.0f && dt * dt * (vh.x * vh.x + vh.y * vh.y + vh.z * vh.z) > P.slab_margin2)
       atomicOr(&a.dyn[inst].errors, kErrDrift);  // the ghost layer no longer covers this drift
-    if (a.list_flags && P.inv_skin > 0.0f)
-      drift_bits = __float_as_uint(dt * sqrtf(vh.x * vh.x + vh.y * vh.y + vh.z * vh.z) * P.inv_skin);
     v = make_float4(v.x + dt * acc.x, v.y + dt * acc.y, v.z + dt * acc.z, 0.f);
     if (P.periodic && !a.list_reuse) wrap_periodic(P, x);  // between list builds positions run on continuously
     if (P.kill_on) {
@@ -218,13 +217,6 @@ __device__ __forceinline__ bool kick_particle(const StepArgs& a, const InstParam
     }
   }
   return true;
-}
-
-// Warp-aggregated maximum of a ratio (float bits) into a list flag word.
-__device__ __forceinline__ void list_flag_max(unsigned* word, unsigned bits) {
-  const unsigned m = __activemask();
-  const unsigned mx = __reduce_max_sync(m, bits);
-  if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && mx) atomicMax(word, mx);
 }
 
 // The kick, the periodic wrap (every binning pass: positions run on
@@ -240,8 +232,7 @@ __global__ void k_kick_bin(StepArgs a) {
   float4 x = a.main.pos[p];
   float4 v = a.main.vel[p];
   float4 vh = v;
-  unsigned drift_bits = 0u;
-  bool changed = !dead && kick_particle(a, P, inst, p, f, x, v, vh, dead, drift_bits);
+  bool changed = !dead && kick_particle(a, P, inst, p, f, x, v, vh, dead);
   // passes without a kick (probe, initial and binning passes) wrap too, so
   // that positions left outside the box by list steps are binned correctly
   if (!dead && !changed && P.periodic && wrap_periodic(P, x)) changed = true;
@@ -261,7 +252,6 @@ __global__ void k_kick_bin(StepArgs a) {
   }
   a.keys_in[p] = key;
   a.vals_in[p] = p;
-  if (a.list_flags) list_flag_max(&a.list_flags[1], drift_bits);
 }
 
 // ------------------------------------------------- permutation + tables
@@ -428,9 +418,17 @@ __device__ __forceinline__ void dt_min(InstDyn* dyn, int inst, float v, bool val
 // Adds gravity to every particle (Dam2.h:104-108), does the final kick of
 // HYDRO particles (class.h:160-163), the density floor (Dam2.h:111), and
 // folds the CFL limits of integral.h:2-12 into dt_cand.  Writes main[p].
+// Motion of a particle at the end of a step, in units of its instance's skin:
+// |x - x0| (x0: its position at the last list build), |v| and |a|.  The next
+// step's drift is dt (v + dt/2 a), so its displacement from x0 is at most
+// d + dt s + dt^2/2 acc (k_list_set).
+struct Motion {
+  float d = 0.f, s = 0.f, acc = 0.f;
+};
+
 __device__ __forceinline__ void finish_hydro(const StepArgs& a, int p, const InstParams& P, int inst, int ph,
                                              uint32_t f, float ax, float ay, float az, float dsum, float vsig,
-                                             unsigned cnt, float& dt_cand, bool& dt_valid) {
+                                             unsigned cnt, float& dt_cand, bool& dt_valid, Motion* mo = nullptr) {
   float4 x = a.alt.pos[p];
   float4 v = a.alt.vel[p];
   float4 acc;
@@ -464,6 +462,13 @@ __device__ __forceinline__ void finish_hydro(const StepArgs& a, int p, const Ins
     }
     acc = make_float4(ax, ay, az, divv);
     x.w = fmaxf(x.w, P.rho_floor);
+    if (mo && !(f & kFreezeBit) && ph == PH_STEP) {
+      const float4 o = a.x0[p];
+      const float dx = x.x - o.x, dy = x.y - o.y, dz = x.z - o.z;
+      mo->d = sqrtf(dx * dx + dy * dy + dz * dz) * P.inv_skin;
+      mo->s = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) * P.inv_skin;
+      mo->acc = sqrtf(ax * ax + ay * ay + az * az) * P.inv_skin;
+    }
   }
   a.main.pos[p] = x;
   a.main.vel[p] = v;

@@ -14,16 +14,92 @@
 //                 current positions, then the shared epilogue
 // A pair within the support now was within 2h + |dx_i| + |dx_j| at the
 // build, so the lists hold every pair the support test can accept while no
-// particle has moved more than skin / 2 since the build.  The host rebuilds
-// before that (k_kick_refresh reports each step's largest drift and the
-// largest displacement); a displacement beyond skin / 2 sets a sticky error
-// that the next wcsph_sim_step reports.
+// particle has moved more than skin / 2 since the build.  Whether a step
+// builds is decided on the device at the start of the step (k_list_set): a
+// build is due when the lists are stale (the host asks), the last build
+// overflowed, list_interval steps have passed, or a particle could end this
+// step's drift 0.45 skin or more from where the lists were built (bounded
+// from the motion the last list pass recorded and the step's dt).  In the
+// step's CUDA graph the decision selects one branch of a conditional node;
+// without a graph the host reads it.  A displacement beyond skin / 2 at a list
+// step would still set a sticky error that the next wcsph_sim_step reports.
 #pragma once
 #include "sim_tiled.cuh"
 
 namespace wcsph {
 
 constexpr int kListMaxEntries = 192;  // entries per list (the solver's list_max; the dam break needs up to ~140)
+
+// Words of StepArgs::list_flags.
+enum ListFlag {
+  kLfReserved0 = 0,
+  kLfReserved1 = 1,
+  kLfErr = 2,              // sticky errors: bit 0 a displacement passed skin / 2 on a list step
+  kLfLongest = 3,          // largest list built
+  kLfOverflowPending = 4,  // the last build overflowed a list: the next step builds
+  kLfBuilds = 5,           // builds so far
+  kLfListSteps = 6,        // list steps so far
+  kLfOverflows = 7,        // builds whose lists overflowed
+  kLfSince = 8,            // steps since the last build (the build counts 1)
+  kLfUnused9 = 9,
+  kLfForce = 10,           // the host asks for a build (lists stale)
+  kLfDecision = 11,        // this step builds (1) or reads the lists (0)
+  kLfWords = 16
+};
+constexpr float kListRebuildAt = 0.45f;  // predicted displacement / skin that makes a step build
+
+// Warp-aggregated maxima of a particle's motion into its instance's words.
+__device__ __forceinline__ void motion_max(unsigned* w, int inst, const Motion& m) {
+  const unsigned full = 0xffffffffu;
+  const unsigned bd = __float_as_uint(m.d), bs = __float_as_uint(m.s), ba = __float_as_uint(m.acc);
+  const int inst0 = __shfl_sync(full, inst, 0);
+  if (__all_sync(full, inst == inst0 || (bd | bs | ba) == 0u)) {
+    const unsigned md = __reduce_max_sync(full, bd), ms = __reduce_max_sync(full, bs), ma = __reduce_max_sync(full, ba);
+    if ((threadIdx.x & 31) == 0 && (md | ms | ma)) {
+      atomicMax(&w[3 * inst0], md);
+      atomicMax(&w[3 * inst0 + 1], ms);
+      atomicMax(&w[3 * inst0 + 2], ma);
+    }
+  } else if (bd | bs | ba) {
+    atomicMax(&w[3 * inst], bd);
+    atomicMax(&w[3 * inst + 1], bs);
+    atomicMax(&w[3 * inst + 2], ba);
+  }
+}
+
+// One thread, after k_step_begin: the step's build decision, the counters,
+// and (in a graph) the condition of the node that selects the build or the
+// list-step branch.  An instance needs a build when the largest displacement
+// its particles can reach in this step, d + dt s + dt^2/2 acc from the motion
+// the last list pass recorded, reaches kListRebuildAt skins.
+__global__ void k_list_set(StepArgs a, int interval, cudaGraphConditionalHandle cond, int use_cond) {
+  unsigned* lf = a.list_flags;
+  bool moved = false;
+  for (int k = 0; k < a.n_inst; ++k) {
+    const InstParams& P = a.params[k];
+    const float dt = a.dyn[k].dt_cur;
+    unsigned* w = a.inst_motion + 3 * k;
+    if (P.active && P.inv_skin > 0.0f && a.phase[k] == PH_STEP && dt > 0.0f) {
+      const float reach = __uint_as_float(w[0]) + dt * __uint_as_float(w[1]) + 0.5f * dt * dt * __uint_as_float(w[2]);
+      moved |= reach >= kListRebuildAt;
+    }
+    w[0] = w[1] = w[2] = 0u;  // refilled by this step's list pass
+  }
+  const bool overflowed = lf[kLfOverflowPending] != 0u;
+  const bool build = lf[kLfForce] != 0u || overflowed || (int)lf[kLfSince] >= interval || moved;
+  if (overflowed) ++lf[kLfOverflows];
+  if (build) {
+    ++lf[kLfBuilds];
+    lf[kLfSince] = 1u;
+    lf[kLfForce] = 0u;
+    lf[kLfOverflowPending] = 0u;
+  } else {
+    ++lf[kLfListSteps];
+    ++lf[kLfSince];
+  }
+  lf[kLfDecision] = build ? 1u : 0u;
+  if (use_cond) cudaGraphSetConditional(cond, build ? 1u : 0u);
+}
 
 // A list step's kick (kick_particle, no wrapping), in place in the build's
 // order, with the EoS j-records refreshed and |x - x0| checked.  List steps
@@ -39,8 +115,7 @@ __global__ void k_kick_refresh(StepArgs a) {
   float4 x = a.main.pos[p];
   float4 v = a.main.vel[p];
   float4 vh = v;
-  unsigned drift_bits = 0u, disp_bits = 0u;
-  if (!dead && kick_particle(a, P, inst, p, f, x, v, vh, dead, drift_bits)) {
+  if (!dead && kick_particle(a, P, inst, p, f, x, v, vh, dead)) {
     a.main.pos[p] = x;
     a.main.vel[p] = v;
   }
@@ -59,16 +134,13 @@ __global__ void k_kick_refresh(StepArgs a) {
                 cell_of(o.y, P.lo[1], P.inv_cell[1], P.ncell[1]), cell_of(o.z, P.lo[2], P.inv_cell[2], P.ncell[2]));
     const float dx = x.x - o.x, dy = x.y - o.y, dz = x.z - o.z;
     const float r = sqrtf(dx * dx + dy * dy + dz * dz) * P.inv_skin;
-    disp_bits = __float_as_uint(r);
-    if (r > 0.5f) atomicOr(&a.list_flags[2], 1u);  // a pair may be missing from the lists
+    if (r > 0.5f) atomicOr(&a.list_flags[kLfErr], 1u);  // a pair may be missing from the lists
   } else {  // removed: never in anyone's support again
     a.jr[p].a = make_float4(1.0e30f, 1.0e30f, 1.0e30f, 0.f);
     a.jr[p].b = make_float4(0.f, 0.f, 0.f, 1.f);
     a.jC[p] = 0.f;
     if (a.jv) write_h16_dead(a.jv, a.jq, p);
   }
-  list_flag_max(&a.list_flags[0], disp_bits);
-  list_flag_max(&a.list_flags[1], drift_bits);
 }
 
 // The build cell of slot p (its position x0 at the last list build).
@@ -370,12 +442,14 @@ __global__ void __launch_bounds__(128, MINB) k_hydro_list(StepArgs a) {
     sv = fmaxf(sv, __shfl_xor_sync(full, sv, o));
     scnt += __shfl_xor_sync(full, scnt, o);
   }
+  Motion mo;
   if (work && sub == 0) {
     const InstParams& P = a.params[inst];
     if (!(fp & kGhostBit)) owned = scnt;  // owned particles only
-    finish_hydro(a, p, P, inst, a.phase[inst], fp, sx, sy, sz, sd, sv, scnt, dt_cand, dt_valid);
+    finish_hydro(a, p, P, inst, a.phase[inst], fp, sx, sy, sz, sd, sv, scnt, dt_cand, dt_valid, &mo);
   }
   dt_min(a.dyn, inst, dt_cand, dt_valid);
+  motion_max(a.inst_motion, inst, mo);
   const unsigned tot = __reduce_add_sync(full, owned);
   if ((threadIdx.x & 31) == 0 && tot) atomicAdd(a.pair_count, (unsigned long long)tot);
 }

@@ -415,10 +415,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
       if (LB) {
         if (lane < nbat) {
           a.list_cnt[ib + lane] = lcount;
-          if (lcount > a.list_max) atomicOr(&a.list_flags[2], 2u);  // overflow: rebuild next step
+          if (lcount > a.list_max) a.list_flags[4] = 1u;  // kLfOverflowPending: the next step rebuilds
         }
         const int mx = __reduce_max_sync(full, lane < nbat ? lcount : 0);
-        if (lane == 0) atomicMax(&a.list_flags[3], (unsigned)mx);
+        if (lane == 0) atomicMax(&a.list_flags[3], (unsigned)mx);  // kLfLongest
       }
       if (!LB && lane < nbat) {
         const int p = ib + lane;
