@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define WCSPH_ABI_VERSION 1
+#define WCSPH_ABI_VERSION 2
 
 typedef enum {
   WCSPH_OK = 0,
@@ -359,8 +359,9 @@ int32_t wcsph_sim_kernels_per_step(wcsph_sim* sim);
  * thread per particle, 4 blocks per SM; 3: two threads per particle, 5 blocks
  * per SM.  Shapes 0 and 2 sum in one order, 1 and 3 in another: results
  * agree to FP32 rounding), out[2] log2 particle bucket it was tuned for (-1:
- * defaults, not tuned). */
-int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out3);
+ * defaults, not tuned), out[3] shape of the list build's scan (0-2 as out[0];
+ * 3, 4: 4 or 8 warps per block with 256-candidate tiles). */
+int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out4);
 /* Neighbour-list counters (list_interval > 0): out[0] list builds, out[1]
  * steps that read the lists, out[2] builds whose lists overflowed (the next
  * step builds again), out[3] largest list built so far, out[4] kernel

@@ -38,7 +38,7 @@ def test_default_layout_and_pair_params(native):
     assert (g.alpha, g.beta, g.c_cfl, g.vsig_mode, g.grad_mode) == (0.01, 0.02, 0.3, N.VSIG_SIGNAL, N.GRAD_SYM)
     c = fdps.pair_params("reference_cpu")
     assert (c.alpha, c.beta, c.c_cfl, c.vsig_mode, c.grad_mode) == (0.01, 0.0, 0.3, N.VSIG_REF_CPU, N.GRAD_HBAR)
-    assert N.lib().wcsph_abi_version() == 1
+    assert N.lib().wcsph_abi_version() == 2
 
 
 def test_configure_rejects_bad_params(native):
@@ -46,7 +46,7 @@ def test_configure_rejects_bad_params(native):
     p.vsig_mode = 7
     with pytest.raises(N.WcsphError) as e:
         fdps.configure(p)
-    assert e.value.code == N.lib().wcsph_abi_version()  # WCSPH_E_INVALID == 1
+    assert e.value.code == 1  # WCSPH_E_INVALID
     fdps.configure("reference_gpu")
 
 

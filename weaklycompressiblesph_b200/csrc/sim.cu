@@ -73,6 +73,7 @@ struct SimImpl {
   bool any_density = false;
   int tile_shape = 0;          // tiled pair-kernel shape, chosen by the autotuner
   int list_shape = 0;          // list-pass launch shape (kListShapes), chosen by the autotuner
+  int build_shape = 0;         // list build's scan shape (kBuildShapes), chosen by the autotuner
   int tuned_bucket = -1;       // log2 particle bucket of the last tuning
   cudaGraphExec_t gexec = nullptr;
   bool graph_dirty = true;
@@ -268,8 +269,8 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
       k_hydro_plain<true><<<nblk(n), kBlock, 0, S.s>>>(a);
     } else if (build_lists) {  // the scan writes the lists, the list pass sums them
       const bool h16 = S.opt.precision == WCSPH_PREC_HALF2;
-      if (int rc = h16 ? launch_hydro_tiled<true, true>(a, n, S.s, S.tile_shape)
-                       : launch_hydro_tiled<false, true>(a, n, S.s, S.tile_shape))
+      if (int rc = h16 ? launch_hydro_tiled<true, true>(a, n, S.s, S.build_shape)
+                       : launch_hydro_tiled<false, true>(a, n, S.s, S.build_shape))
         return rc;
       if (int rc = h16 ? launch_hydro_list<true>(a, n, S.s, S.list_shape)
                        : launch_hydro_list<false>(a, n, S.s, S.list_shape))
@@ -413,6 +414,19 @@ static int autotune(SimImpl& S) {
       if (ms < best_list) best_list = ms, best_list_shape = v;
     }
     S.list_shape = best_list_shape;
+    // the build's scan on the same sorted state (it rewrites the same lists)
+    StepArgs c = a;
+    c.x0 = S.x0;
+    float best_build = 1e30f;
+    int best_build_shape = 0;
+    for (int v = 0; v < kBuildShapes; ++v) {
+      int rc = time_launches(S, 3, [&]() {
+        return h16 ? launch_hydro_tiled<true, true>(c, n, S.s, v) : launch_hydro_tiled<false, true>(c, n, S.s, v);
+      }, &ms);
+      if (rc) return rc;
+      if (ms < best_build) best_build = ms, best_build_shape = v;
+    }
+    S.build_shape = best_build_shape;
     S.lists_valid = false;
     WCSPH_CUDA(cudaMemsetAsync(S.d_lflags + kLfOverflowPending, 0, sizeof(unsigned), S.s));
   }
@@ -1495,11 +1509,12 @@ int32_t wcsph_sim_kernels_per_step(wcsph_sim* sim) { return sim ? sim->impl.kern
 
 void* wcsph_sim_stream(wcsph_sim* sim) { return sim ? (void*)sim->impl.s : nullptr; }
 
-int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out3) {
-  if (!sim || !out3) return WCSPH_E_INVALID;
-  out3[0] = sim->impl.tile_shape;
-  out3[1] = sim->impl.list_shape;
-  out3[2] = sim->impl.tuned_bucket;
+int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out4) {
+  if (!sim || !out4) return WCSPH_E_INVALID;
+  out4[0] = sim->impl.tile_shape;
+  out4[1] = sim->impl.list_shape;
+  out4[2] = sim->impl.tuned_bucket;
+  out4[3] = sim->impl.build_shape;
   return 0;
 }
 

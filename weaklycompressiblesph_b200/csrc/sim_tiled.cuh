@@ -472,11 +472,21 @@ inline int launch_hydro_tiled(const StepArgs& a, int n, cudaStream_t s, int shap
     set_error("the tiled path holds at most %d particles per solver (got %d)", kMaxTiledParticles, n);
     return WCSPH_E_CAPACITY;
   }
+  if constexpr (LB) {  // list builds only: smaller tiles, more warps per SM (the scan writes no sums)
+    if (shape == 3) return launch_pair_tiled_v<H16, 4, 256, LB>(a, s);
+    if (shape == 4) return launch_pair_tiled_v<H16, 8, 256, LB>(a, s);
+  }
   switch (shape) {
     case 1: return launch_pair_tiled_v<H16, 2, 512, LB>(a, s);
     case 2: return launch_pair_tiled_v<H16, 8, 512, LB>(a, s);
     default: return launch_pair_tiled_v<H16, 4, 512, LB>(a, s);
   }
 }
+
+// Shapes of the list build's scan-only pass: the three above and two with
+// 256-candidate tiles (half the shared memory a warp, so up to twice the
+// warps per SM; a cell's candidates then take two tile passes, which changes
+// only the order in which its list entries are found within each pass).
+constexpr int kBuildShapes = 5;
 
 }  // namespace wcsph

@@ -206,10 +206,11 @@ class Solver:
         return int(N.lib().wcsph_sim_kernels_per_step(self._h))
 
     def tuning(self):
-        """Autotuner decision: tiled-kernel block shape, list-pass launch shape, tuned bucket."""
-        out = np.zeros(3, np.int32)
+        """Autotuner decision: tiled-kernel block shape, list-pass launch shape,
+        tuned bucket, list-build scan shape."""
+        out = np.zeros(4, np.int32)
         N.call("wcsph_sim_tuning", self._h, N.ptr(out, C.c_int32))
-        return dict(tile_shape=int(out[0]), list_shape=int(out[1]), bucket=int(out[2]))
+        return dict(tile_shape=int(out[0]), list_shape=int(out[1]), bucket=int(out[2]), build_shape=int(out[3]))
 
     def stream(self):
         """The solver's cudaStream_t as an integer handle."""
