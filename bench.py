@@ -292,10 +292,18 @@ def run_device(case, prec_name, steps, warmup, device, clocks=False, list_interv
             res["lists"] = {"interval": list_interval, "skin_h": list_skin or 0.3, "timed_builds": b,
                             "timed_list_steps": r, "overflows": ls1["overflows"], "longest": ls1["longest"],
                             "entries": s.list_entries()}
-        # per-phase kernel times (eager launches, CUDA events on the solver stream)
-        prof_steps = max(3, min(20, steps // 5))
-        ph = s.profile_steps(prof_steps)
-        res["phase_ms"] = (ph / prof_steps).tolist()
+        # per-phase kernel times (eager launches, CUDA events on the solver
+        # stream), split into steps that searched or built and steps that read
+        # the lists; with lists the profile starts with a build and spans two
+        # rebuild periods, so it carries builds in the timed region's share
+        if lists:
+            s.invalidate_lists()
+            prof_steps = max(3, min(steps, 2 * list_interval))
+        else:
+            prof_steps = max(3, min(20, steps // 5))
+        sp = s.profile_split(prof_steps)
+        res["phase_ms"] = ((sp["build"] + sp["list"]) / prof_steps).tolist()
+        res["profile"] = sp
         res["status"] = s.status(k)
         res["tuning"] = s.tuning()
     return res
@@ -570,16 +578,10 @@ def main():
             other["speedup_vs_plain_fp32"] = other["steps_per_s"] / plain["steps_per_s"]
         other["error_vs_fp64"] = validation_errors(args.workload, oprec)
     peak, peak_kind = load_peaks()
-    hydro_ms = dev["phase_ms"][2]
-    bpp = BYTES_PER_PAIR[prec]
-    achieved = dev["pairs_per_step"] * bpp / (hydro_ms * 1e-3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "hydro_traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as f:
-            t = json.load(f)
-        key = f"{args.workload}/{prec}" + ("/lists" if dev.get("lists") else "")
-        traffic = t.get(key, {}).get("bytes_per_launch")
+    if other:
+        other["roofline"] = hbm_roofline(args.workload, other["precision"], case.n, o, peak, peak_kind)
+        other["roofline_l1"] = l1_roofline(args.workload, other["precision"], o)
+    roof = hbm_roofline(args.workload, prec, case.n, dev, peak, peak_kind)
     l1 = l1_roofline(args.workload, prec, dev)
     e2e = None
     cpu = None
@@ -617,11 +619,7 @@ def main():
         ("half2" if other and other["precision"] == "half2" else "fp32_tiled"): other,
         "phase_ms": {"bin_sort_permute": dev["phase_ms"][0], "density": dev["phase_ms"][1],
                      "hydro": dev["phase_ms"][2], "total": dev["phase_ms"][3]},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "kernel": "hydro pass",
-                     "model": f"{bpp} B per true pair (j-record) / hydro kernel time"
-                              + (" (build and list steps averaged)" if dev.get("lists") else ""),
-                     "peak_kind": peak_kind},
+        "roofline": roof,
         "roofline_l1": l1,
         "error_vs_fp64": validation_errors(args.workload, prec),
         "cpu_baseline": cpu,
@@ -664,6 +662,65 @@ def validation_errors(workload, prec):
         return None
     return {"acc": r["max_acc"], "div_v": r["max_div_v"], "drho_dt": r["max_drho_dt"], "checkpoints": r["checkpoints"],
             "steps": v["steps"], "source": "tests/validate_dam_break.py (profiles/validation_dam1m.md)"}
+
+
+# Bytes a hydro pass must move per particle besides the j-records it gathers:
+# the epilogue reads position, velocity, half-step velocity, flags and id and
+# writes position, velocity, acceleration (+ div v), flags and id (112 B, the
+# final kick and the dt candidate are fused into the pass); the particle's own
+# FP32 j-record and c (36 B); with lists its entry count (4 B).
+PASS_STATE_BYTES = 112
+OWN_RECORD_BYTES = 36
+COMPACT_RECORD_BYTES = 24   # half2 lists: the particle's compact record, fetched once as a j operand
+SURVEY_I_BYTES = 64         # the per-particle i read and write of the per-pair record model
+
+
+def hbm_roofline(workload, prec, n, dev, peak, peak_kind):
+    """The hydro pass against HBM.  Algorithmic bytes per launch = what the
+    pass must move at least: every particle's state and own record once, and
+    with lists every list word once (4 B per entry); a j-record that a
+    particle's neighbours gather again comes from L1 or L2, so it is counted
+    once.  Duration = the pass's average launch time over the profiled steps
+    (CUDA events on the solver stream): on list steps exactly one list-pass
+    launch.  `traffic` is the DRAM bytes of one launch from an ncu capture.
+    `pair_record_model` is the per-pair model (36 B per true pair + 64 B per
+    particle), an operand rate: the records it counts reach the pair terms
+    from L1 and L2, so it is not a DRAM figure and can exceed the HBM peak."""
+    sp = dev.get("profile")
+    lists = dev.get("lists")
+    bpp = BYTES_PER_PAIR[prec]
+    if lists and sp and sp["list_steps"] > 0:
+        kernel = {"tiled": "k_hydro_list<0> (list pass, FP32 records)",
+                  "half2": "k_hydro_list<1> (list pass, half2 compact records)"}[prec]
+        launch_ms = sp["list"][2] / sp["list_steps"]
+        per_particle = PASS_STATE_BYTES + OWN_RECORD_BYTES + 4 + (COMPACT_RECORD_BYTES if prec == "half2" else 0)
+        alg = n * per_particle + 4.0 * lists["entries"]
+        units = (f"{per_particle} B per particle (state {PASS_STATE_BYTES}, own record {OWN_RECORD_BYTES}, "
+                 f"list count 4" + (f", compact record {COMPACT_RECORD_BYTES}" if prec == "half2" else "")
+                 + ") + 4 B per list entry")
+        key = f"{workload}/{prec}/lists"
+    else:
+        kernel = {"tiled": "k_hydro_tiled (search every step)", "half2": "k_hydro_tiled (search every step)",
+                  "fp32": "k_hydro_plain (search every step)"}[prec]
+        tot = (sp["build"][2] + sp["list"][2]) if sp else dev["phase_ms"][2]
+        launch_ms = tot / max(1, (sp["build_steps"] + sp["list_steps"]) if sp else 1)
+        per_particle = PASS_STATE_BYTES + OWN_RECORD_BYTES
+        alg = n * per_particle
+        units = f"{per_particle} B per particle (state {PASS_STATE_BYTES}, own record {OWN_RECORD_BYTES})"
+        key = f"{workload}/{prec}"
+    achieved = alg / (launch_ms * 1e-3) / 1e9
+    traffic = None
+    tp = _profile_json("hydro_traffic.json")
+    if tp:
+        traffic = tp.get(key, {}).get("bytes_per_launch")
+    pair_rate = (dev["pairs_per_step"] * bpp + n * SURVEY_I_BYTES) / (launch_ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "kernel": kernel, "launch_ms": launch_ms, "algorithmic_bytes": alg,
+            "model": units, "peak_kind": peak_kind,
+            "limiter": "L1 data pipe (roofline_l1)" if lists else "instruction issue",
+            "pair_record_model": {"bytes_per_pair": bpp, "bytes_per_particle": SURVEY_I_BYTES,
+                                  "operand_rate_gbs": pair_rate,
+                                  "note": "j-records delivered to the pair terms, mostly from L1; not DRAM"}}
 
 
 def l1_roofline(workload, prec, dev):

@@ -383,6 +383,14 @@ void* wcsph_sim_stream(wcsph_sim* sim);
  * permutation, ms[1] density pass + EoS refresh, ms[2] hydro pass, ms[3] whole
  * steps.  Advances the simulation like wcsph_sim_step. */
 int wcsph_sim_profile_steps(wcsph_sim* sim, int32_t nsteps, double* ms4);
+/* The same eager steps, their phase times split by kind: ms[0..3] summed over
+ * the steps that searched (list_interval = 0) or built the neighbour lists,
+ * ms[4..7] over the steps that read the lists, ms[8] the builds' list scans
+ * alone (a build's hydro phase is its scan plus one list pass, so a list
+ * step's ms[6] is one list-pass launch); steps[0], steps[1] count the two
+ * kinds.  Times of the per-kernel roofline; no counterpart in the reference
+ * (its Timer, class.h:3-17, times whole steps). */
+int wcsph_sim_profile_split(wcsph_sim* sim, int32_t nsteps, double* ms9, int32_t* steps2);
 
 #ifdef __cplusplus
 }

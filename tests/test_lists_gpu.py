@@ -292,3 +292,30 @@ def test_half2_lists_far_particles(native, oracle_lib):
     r = oracle_list_check(oracle_lib, case, st, pr, 0)
     np.testing.assert_array_equal(pr["nbr"], r["cnt"])
     assert r["acc"] < 1e-3 and r["div_v"] < 1e-3, r
+
+
+def test_profile_split_follows_the_schedule(native):
+    """wcsph_sim_profile_split: steps split into builds and list steps as the
+    device decided them; a build's scan is part of its hydro phase; the
+    steps advance the run like wcsph_sim_step."""
+    case = small_dam(dx=0.04, seed=8)
+    with Solver(case.n, precision=N.PREC_TILED, list_interval=5) as s:
+        k = s.add(case)
+        s.step(3)
+        s.synchronize()
+        s.invalidate_lists()
+        l0 = s.list_stats()
+        sp = s.profile_split(12)
+        l1 = s.list_stats()
+        assert s.status(k)["steps"] == 15
+    assert sp["build_steps"] + sp["list_steps"] == 12
+    assert sp["build_steps"] == l1["builds"] - l0["builds"] >= 3  # the invalidated step, then every 5 steps
+    assert sp["list_steps"] == l1["list_steps"] - l0["list_steps"] > 0
+    for kind in ("build", "list"):
+        ph = sp[kind]
+        assert (ph[:3] >= 0).all() and ph[2] > 0 and abs(ph[3] - ph[:3].sum()) < 1e-6 * max(1.0, ph[3])
+    assert 0 < sp["scan_ms"] < sp["build"][2]
+    with Solver(case.n, precision=N.PREC_TILED) as s:  # searching every step: all steps are of the first kind
+        s.add(case)
+        sp = s.profile_split(4)
+    assert sp["build_steps"] == 4 and sp["list_steps"] == 0 and sp["scan_ms"] == 0.0

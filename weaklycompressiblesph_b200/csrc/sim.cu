@@ -89,6 +89,7 @@ struct SimImpl {
   unsigned* d_motion = nullptr;       // 3 words per instance, see StepArgs::inst_motion
   unsigned* h_lflags = nullptr;       // pinned copy, written at the end of every list-mode step
   cudaEvent_t step_ev[2] = {nullptr, nullptr};
+  cudaEvent_t scan_ev = nullptr;  // set while profiling: recorded between a build's scan and its list pass
   bool lists_valid = false;           // false: the next step is asked to build (kLfForce)
   int kernels_reuse = 0;
   long long steps_launched = 0;
@@ -272,6 +273,7 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
       if (int rc = h16 ? launch_hydro_tiled<true, true>(a, n, S.s, S.build_shape)
                        : launch_hydro_tiled<false, true>(a, n, S.s, S.build_shape))
         return rc;
+      if (ev && S.scan_ev) WCSPH_CUDA(cudaEventRecord(S.scan_ev, S.s));
       if (int rc = h16 ? launch_hydro_list<true>(a, n, S.s, S.list_shape)
                        : launch_hydro_list<false>(a, n, S.s, S.list_shape))
         return rc;
@@ -561,7 +563,7 @@ static int enqueue_list_prologue(SimImpl& S, const StepArgs& a0, cudaGraphCondit
 // One step in list mode.  Stale lists are marked for the device (kLfForce);
 // the device decides whether the step builds.  At most two steps are in
 // flight; the flags are read one step behind.
-static int list_step(SimImpl& S, bool graph, cudaEvent_t* ev) {
+static int list_step(SimImpl& S, bool graph, cudaEvent_t* ev, bool* built = nullptr) {
   if (!S.lists_valid) {
     WCSPH_CUDA(cudaMemsetAsync(S.d_lflags + kLfForce, 0x01, sizeof(unsigned), S.s));
     S.lists_valid = true;
@@ -570,10 +572,12 @@ static int list_step(SimImpl& S, bool graph, cudaEvent_t* ev) {
     WCSPH_CUDA(cudaGraphLaunch(S.gexec, S.s));
   } else {
     StepArgs a = make_args(S);
-    if (int rc = enqueue_list_prologue(S, a, 0, false, ev)) return rc;
+    if (int rc = enqueue_list_prologue(S, a, 0, false, nullptr)) return rc;
     unsigned build = 0;
     WCSPH_CUDA(cudaMemcpyAsync(&build, S.d_lflags + kLfDecision, sizeof(unsigned), cudaMemcpyDeviceToHost, S.s));
     WCSPH_CUDA(cudaStreamSynchronize(S.s));
+    if (built) *built = build != 0;
+    if (ev) WCSPH_CUDA(cudaEventRecord(ev[0], S.s));  // after the host read of the decision
     const int rc = build ? enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step, ev, true, true)
                          : enqueue_reuse(S, a, S.any_density, &S.kernels_reuse, ev);
     if (rc) return rc;
@@ -1555,37 +1559,62 @@ int wcsph_sim_invalidate_lists(wcsph_sim* sim) {
   return 0;
 }
 
-int wcsph_sim_profile_steps(wcsph_sim* sim, int32_t nsteps, double* ms4) {
-  if (!sim || !ms4 || nsteps < 0) return WCSPH_E_INVALID;
-  SimImpl& S = sim->impl;
+// Eager steps with CUDA events around each phase; ms[0..3] summed over the
+// steps that searched or built, ms[4..7] over the steps that read the lists,
+// ms[8] the builds' scans; steps[0..1] how many of each.
+static int profile_impl(SimImpl& S, int nsteps, double* ms, int32_t* steps) {
   WCSPH_CUDA(cudaSetDevice(S.opt.device));
   cudaEvent_t ev[4];
   for (auto& e : ev) WCSPH_CUDA(cudaEventCreate(&e));
-  for (int k = 0; k < 4; ++k) ms4[k] = 0.0;
+  WCSPH_CUDA(cudaEventCreate(&S.scan_ev));
+  for (int k = 0; k < 9; ++k) ms[k] = 0.0;
+  steps[0] = steps[1] = 0;
   StepArgs a = make_args(S);
   int rc = 0;
   for (int t = 0; t < nsteps && !rc; ++t) {
+    bool built = true;
     if (S.opt.list_interval > 0) {
-      rc = list_step(S, false, ev);  // the same build / list-step schedule as wcsph_sim_step
+      rc = list_step(S, false, ev, &built);  // the same build / list-step schedule as wcsph_sim_step
     } else {
       if (cudaMemsetAsync(S.d_pairs, 0, sizeof(unsigned long long), S.s) != cudaSuccess) rc = WCSPH_E_CUDA;
       if (!rc) rc = enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step, ev);
     }
     if (!rc && cudaEventSynchronize(ev[3]) != cudaSuccess) rc = WCSPH_E_CUDA;
-    float x[3];
     if (!rc) {
+      float x[3];
       cudaEventElapsedTime(&x[0], ev[0], ev[1]);
       cudaEventElapsedTime(&x[1], ev[1], ev[2]);
       cudaEventElapsedTime(&x[2], ev[2], ev[3]);
-      ms4[0] += x[0];
-      ms4[1] += x[1];
-      ms4[2] += x[2];
-      ms4[3] += x[0] + x[1] + x[2];
+      double* m = ms + (built ? 0 : 4);
+      for (int k = 0; k < 3; ++k) m[k] += x[k];
+      m[3] += x[0] + x[1] + x[2];
+      ++steps[built ? 0 : 1];
+      if (built && S.opt.list_interval > 0) {
+        float sc = 0.f;
+        cudaEventElapsedTime(&sc, ev[2], S.scan_ev);
+        ms[8] += sc;
+      }
     }
   }
   for (auto& e : ev) cudaEventDestroy(e);
-  if (rc == WCSPH_E_CUDA) set_error("wcsph_sim_profile_steps: CUDA error %s", cudaGetErrorString(cudaGetLastError()));
+  cudaEventDestroy(S.scan_ev);
+  S.scan_ev = nullptr;
+  if (rc == WCSPH_E_CUDA) set_error("profiling steps: CUDA error %s", cudaGetErrorString(cudaGetLastError()));
   return rc;
+}
+
+int wcsph_sim_profile_steps(wcsph_sim* sim, int32_t nsteps, double* ms4) {
+  if (!sim || !ms4 || nsteps < 0) return WCSPH_E_INVALID;
+  double ms[9];
+  int32_t steps[2];
+  const int rc = profile_impl(sim->impl, nsteps, ms, steps);
+  for (int k = 0; k < 4; ++k) ms4[k] = rc ? 0.0 : ms[k] + ms[4 + k];
+  return rc;
+}
+
+int wcsph_sim_profile_split(wcsph_sim* sim, int32_t nsteps, double* ms9, int32_t* steps2) {
+  if (!sim || !ms9 || !steps2 || nsteps < 0) return WCSPH_E_INVALID;
+  return profile_impl(sim->impl, nsteps, ms9, steps2);
 }
 
 }  // extern "C"

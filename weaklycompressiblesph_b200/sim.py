@@ -239,3 +239,14 @@ class Solver:
         ms = np.zeros(4, np.float64)
         N.call("wcsph_sim_profile_steps", self._h, int(nsteps), N.ptr(ms, C.c_double))
         return ms
+
+    def profile_split(self, nsteps):
+        """Like profile_steps, split by kind of step: returns a dict with the
+        phase milliseconds summed over the steps that searched or built
+        ("build"), over the steps that read the lists ("list"), the builds'
+        scans alone ("scan_ms") and the step counts."""
+        ms = np.zeros(9, np.float64)
+        cnt = np.zeros(2, np.int32)
+        N.call("wcsph_sim_profile_split", self._h, int(nsteps), N.ptr(ms, C.c_double), N.ptr(cnt, C.c_int32))
+        return {"build": ms[0:4].copy(), "list": ms[4:8].copy(), "scan_ms": float(ms[8]),
+                "build_steps": int(cnt[0]), "list_steps": int(cnt[1])}
