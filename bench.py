@@ -476,6 +476,7 @@ def measure_ensemble(device, steps=None):
             "serial_plain_particle_steps_per_s": s["particle_steps_per_s"],
             "speedup_vs_serial_plain": b["particle_steps_per_s"] / s["particle_steps_per_s"],
             "tuning": b.get("tuning"),
+            "lists": _list_summary(b.get("lists")),
             "sample": f"{steps} timed steps per instance" + ("" if steps >= 2000 else " (config: 2000)"),
             "neighbour_search": (f"lists, rebuilt at least every {ARGS.list_interval} steps" if ARGS.list_interval
                                  else "every step") + "; serial baseline: plain FP32, search every step"}
@@ -509,10 +510,19 @@ def measure_serving(device):
             "neighbour_search": (f"lists, rebuilt at least every {ARGS.list_interval} steps" if ARGS.list_interval
                                  else "every step") + "; serial baseline: plain FP32, search every step",
             "precision": ARGS.ensemble_precision,
+            "lists": _list_summary(out.get("lists")),
             "sample": f"{len(reqs)} requests, counts log-uniform [2e4, {ARGS.serving_nmax:.0e}], "
                       f"t_end {ARGS.serving_tend:g} s, Poisson 20/s, budget 150 GB"
                       + ("" if ARGS.serving_nmax >= 2e6 and ARGS.serving_tend >= 1.0
                          else " (config: counts to 2e6, t_end 1.0 s)")}
+
+
+def _list_summary(ls):
+    if not ls:
+        return None
+    steps = ls["builds"] + ls["list_steps"]
+    return {"builds": ls["builds"], "list_steps": ls["list_steps"], "overflows": ls["overflows"],
+            "steps_per_build": steps / max(1, ls["builds"])}
 
 
 ARGS = None
