@@ -681,7 +681,7 @@ def validation_errors(workload, prec):
 # FP32 j-record and c (36 B); with lists its entry count (4 B).
 PASS_STATE_BYTES = 112
 OWN_RECORD_BYTES = 36
-COMPACT_RECORD_BYTES = 24   # half2 lists: the particle's compact record, fetched once as a j operand
+COMPACT_RECORD_BYTES = 16   # half2 lists: the particle's compact record, fetched once as a j operand
 SURVEY_I_BYTES = 64         # the per-particle i read and write of the per-pair record model
 
 

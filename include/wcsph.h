@@ -169,8 +169,10 @@ int wcsph_filter_retrieve(int32_t tag, int32_t n_walk, const int32_t* n_i, void*
 typedef enum {
   WCSPH_PREC_FP32 = 0,  /* plain FP32 pair arithmetic, one thread per i-particle          */
   WCSPH_PREC_TILED = 1, /* FP32, shared-memory j-tiles, ballot-compacted pair queues      */
-  WCSPH_PREC_HALF2 = 2  /* tiled; pair geometry and kernel gradient in packed half2,
-                           FP32 accumulation, FP32 positions and velocities              */
+  WCSPH_PREC_HALF2 = 2  /* with neighbour lists: the list pass gathers 16-byte compact
+                           j-records (16-bit cell-relative positions and velocities, FP32
+                           density), FP32 pair arithmetic and accumulation; without
+                           lists the same as WCSPH_PREC_TILED                            */
 } wcsph_precision;
 
 typedef enum {

@@ -83,8 +83,7 @@ struct SimImpl {
   uint32_t* list = nullptr;
   int* list_cnt = nullptr;
   float4* x0 = nullptr;
-  float4* jv = nullptr;  // compact j-records of the half2 list pass
-  uint2* jq = nullptr;
+  uint4* jh = nullptr;  // compact j-records of the half2 list pass (write_h16)
   unsigned* d_lflags = nullptr;       // kLfWords words, see ListFlag
   unsigned* d_motion = nullptr;       // 3 words per instance, see StepArgs::inst_motion
   unsigned* h_lflags = nullptr;       // pinned copy, written at the end of every list-mode step
@@ -97,6 +96,12 @@ struct SimImpl {
 
 constexpr int kListMax = kListMaxEntries;  // entries per particle list (2h + 0.3 h holds ~100-115 at h = 1.3 dx)
 static float list_skin(const wcsph_sim_options& o) { return o.list_skin > 0.f ? o.list_skin : 0.3f; }
+// velocity_quantum (sim_list.cuh) on the host: 2^-15 of the smallest power of
+// two above max(vb, c0 2^-12).
+static float host_velocity_quantum(float vb, float c0) {
+  const float v = std::max(vb, c0 / 4096.0f);
+  return std::ldexp(1.0f, std::ilogb(v) + 1 - 15);
+}
 
 static int alloc(SimImpl& S, void** p, size_t bytes) {
   WCSPH_CUDA(cudaMalloc(p, bytes ? bytes : 16));
@@ -123,7 +128,7 @@ static bool h16_lists(const wcsph_sim_options& o) { return o.list_interval > 0 &
 
 static int64_t device_bytes(const wcsph_sim_options& o) {
   const int64_t list_bytes =
-      o.list_interval > 0 ? (int64_t)(kListMax * 4 + 4 + 16 + (h16_lists(o) ? 24 : 0)) * o.max_particles : 0;
+      o.list_interval > 0 ? (int64_t)(kListMax * 4 + 4 + 16 + (h16_lists(o) ? 16 : 0)) * o.max_particles : 0;
   return (int64_t)per_particle_bytes() * o.max_particles + list_bytes + 2 * sizeof(int) * o.max_cells +
          (sizeof(InstParams) + sizeof(InstDyn) + sizeof(int)) * (int64_t)o.max_instances + (int64_t)cub_sort_bytes(o.max_particles) +
          (1 << 20);
@@ -203,8 +208,7 @@ static StepArgs make_args(SimImpl& S) {
     a.list_max = kListMax;
     a.list_flags = S.d_lflags;
     a.inst_motion = S.d_motion;
-    a.jv = S.jv;
-    a.jq = S.jq;
+    a.jh = S.jh;
   }
   return a;
 }
@@ -686,6 +690,11 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
               "centre, which needs list_skin <= 1.5 h (got %g)", (double)opt->list_skin);
     return WCSPH_E_INVALID;
   }
+  if (h16_lists(*opt) && opt->max_particles >= kMaxH16ListParticles) {
+    set_error("wcsph_sim_create: half2 list entries hold the slot in %d bits: max_particles < %d (got %d)",
+              kH16SlotBits, kMaxH16ListParticles, opt->max_particles);
+    return WCSPH_E_INVALID;
+  }
   int ndev = 0;
   WCSPH_CUDA(cudaGetDeviceCount(&ndev));
   if (opt->device < 0 || opt->device >= ndev) {
@@ -743,8 +752,7 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
     rc |= alloc(S, (void**)&S.d_lflags, kLfWords * sizeof(unsigned));
     rc |= alloc(S, (void**)&S.d_motion, 3 * (size_t)opt->max_instances * sizeof(unsigned));
     if (h16_lists(*opt)) {
-      rc |= alloc(S, (void**)&S.jv, N * sizeof(float4));
-      rc |= alloc(S, (void**)&S.jq, N * sizeof(uint2));
+      rc |= alloc(S, (void**)&S.jh, N * sizeof(uint4));
     }
     if (!rc && cudaHostAlloc((void**)&S.h_lflags, kLfWords * sizeof(unsigned), cudaHostAllocDefault) != cudaSuccess)
       rc = 1;
@@ -933,6 +941,12 @@ static int append_instance(SimImpl& S, const AppendSpec& A, int32_t* slot) {
   InstDyn dyn{};
   dyn.dt_next_bits = 0x7f800000u;
   if (A.saved) dyn = *A.saved;
+  {  // velocity quantum of the compact records until the list passes bound the motion (k_list_set)
+    float vmax = 0.f;
+    for (int q = 0; q < n; ++q)
+      vmax = std::max(vmax, std::max(std::fabs(vel[q].x), std::max(std::fabs(vel[q].y), std::fabs(vel[q].z))));
+    dyn.vq = host_velocity_quantum(2.0f * vmax, (float)desc->c0);
+  }
   WCSPH_CUDA(cudaMemcpyAsync(S.d_dyn + k, &dyn, sizeof(InstDyn), cudaMemcpyHostToDevice, S.s));
   S.n_host = base + n;
   S.appended = true;

@@ -30,49 +30,57 @@ __device__ __forceinline__ JRec ld_jrec(const JRec* p) {
 }
 
 // ---------------------------------------------- compact (half2) j-records
-// The half2 list pass reads, per list entry, jv = (vx, vy, vz, P/rho^2) in
-// FP32 and jq: x, y, z as 16-bit fixed-point offsets from the centre of the
-// particle's cell at the last list build (units of 2^-15 cell edges, biased
-// by 2^15, so one cell edge either side) and (rho - rho0) as a half.  24
-// bytes instead of the 32 of the FP32 record.  A particle more than one cell
-// edge from that centre (above the grid, where the cells are clamped; or
-// removed) is marked far (the half NaN kFarMark), and its entries are read
-// from the FP32 record.
-constexpr uint32_t kFarMark = 0x7e00u;  // half NaN in the high 16 bits of jq.y
+// The half2 list pass gathers one 16-byte record per list entry (two records
+// per 32-byte sector), jh[p] = uint4:
+//   .x = x | y << 16, .y = z | vx << 16, .z = vy | vz << 16, .w = rho (FP32 bits)
+// Positions are 16-bit fixed-point offsets from the centre of the particle's
+// cell at the last list build (steps of 2^-15 cell edges, biased by 2^15, so
+// one cell edge either side).  Velocities are 16-bit fixed point in steps of
+// the instance's velocity quantum vq (a power of two, 2^-15 of a bound on its
+// fastest particle this step; InstDyn::vq), biased by 2^15.  P/rho^2 and c
+// are recomputed from rho by the pass.  A particle outside either range (far
+// from its build cell, above the grid where cells are clamped, faster than
+// the bound) or removed is marked far (rho = kFarRho, a NaN), and its entries
+// are read from the FP32 record.
+constexpr uint32_t kFarRho = 0xffffffffu;
 constexpr float kQ16Scale = 32768.0f;
 
 __device__ __forceinline__ float cell_centre(const InstParams& P, int k, int c) {
   return __fmaf_rn((float)c + 0.5f, P.cell[k], P.lo[k]);
 }
 
-__device__ __forceinline__ uint32_t rho_half_bits(const InstParams& P, float rho) {
-  return (uint32_t)__half_as_ushort(__float2half_rn(rho - P.rho0));
+// Biased 16-bit code (1 .. 65535) of q, in steps, or -1 when |q| > 32767 or q is NaN.
+__device__ __forceinline__ int q16(float q) {
+  if (!(fabsf(q) <= 32767.0f)) return -1;
+  return __float2int_rn(q) + 32768;
 }
 
-// Write the compact record of slot p: position x, velocity v, P/rho^2 po,
-// density rho, build cell (cx, cy, cz).
-__device__ __forceinline__ void write_h16(float4* jv, uint2* jq, const InstParams& P, int p, const float4& x,
-                                          const float4& v, float po, float rho, int cx, int cy, int cz) {
+// Write the compact record of slot p: position x, velocity v, density rho,
+// build cell (cx, cy, cz), velocity quantum vq.
+__device__ __forceinline__ void write_h16(uint4* jh, const InstParams& P, float vq, int p, const float4& x,
+                                          const float4& v, float rho, int cx, int cy, int cz) {
   const int c[3] = {cx, cy, cz};
   const float* xa = &x.x;
-  uint32_t u[3];
-  bool far = false;
+  int u[6];
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const float q = (xa[k] - cell_centre(P, k, c[k])) * P.inv_cell[k];
-    const int t = __float2int_rn(q * kQ16Scale) + 32768;  // NaN converts to 0: far below
-    far |= t < 0 || t > 65535;
-    u[k] = (uint32_t)min(max(t, 0), 65535);
+  for (int k = 0; k < 3; ++k) u[k] = q16((xa[k] - cell_centre(P, k, c[k])) * P.inv_cell[k] * kQ16Scale);
+  const float ivq = 1.0f / vq;  // vq is a power of two: exact
+  u[3] = q16(v.x * ivq), u[4] = q16(v.y * ivq), u[5] = q16(v.z * ivq);
+  bool far = !(rho > 0.0f);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) far |= u[k] < 0;
+  if (far) {
+    jh[p] = make_uint4(0x80008000u, 0x80008000u, 0x80008000u, kFarRho);
+    return;
   }
-  jv[p] = make_float4(v.x, v.y, v.z, po);
-  jq[p] = make_uint2(u[0] | (u[1] << 16), u[2] | ((far ? kFarMark : rho_half_bits(P, rho)) << 16));
+  jh[p] = make_uint4((uint32_t)u[0] | ((uint32_t)u[1] << 16), (uint32_t)u[2] | ((uint32_t)u[3] << 16),
+                     (uint32_t)u[4] | ((uint32_t)u[5] << 16), __float_as_uint(rho));
 }
 
 // A removed particle: far, so that its entries take the FP32 record (whose
 // position is far from everything).
-__device__ __forceinline__ void write_h16_dead(float4* jv, uint2* jq, int p) {
-  jv[p] = make_float4(0.f, 0.f, 0.f, 0.f);
-  jq[p] = make_uint2(0x80008000u, 0x8000u | (kFarMark << 16));
+__device__ __forceinline__ void write_h16_dead(uint4* jh, int p) {
+  jh[p] = make_uint4(0x80008000u, 0x80008000u, 0x80008000u, kFarRho);
 }
 
 struct SimArrays {
@@ -113,8 +121,7 @@ struct StepArgs {
   unsigned* inst_motion;  // neighbour lists: per instance, the largest |x - x0|, |v| and |a| over its moving
                           // particles at the end of the step, in units of its skin (float bits)
   // compact j-records of the half2 list pass (WCSPH_PREC_HALF2 with lists; null otherwise)
-  float4* jv;             // (vx, vy, vz, P/rho^2)
-  uint2* jq;              // 16-bit cell-relative x, y, z and (rho - rho0) as a half (h16_record)
+  uint4* jh;              // 16-bit cell-relative x, y, z, 16-bit velocity, FP32 rho (write_h16)
   int probe_density;      // density pass of a probe launch: 0 none, 1 summation, 2 Shepard
   // diagnostics (probe phase)
   float4* diag_acc;
@@ -299,7 +306,7 @@ __global__ void k_permute(StepArgs a) {
   a.jr[p].a = make_float4(x.x, x.y, x.z, po);
   a.jr[p].b = make_float4(v.x, v.y, v.z, x.w);
   a.jC[p] = snds;
-  if (a.jv) write_h16(a.jv, a.jq, P, p, x, v, po, x.w, cx, cy, cz);
+  if (a.jh) write_h16(a.jh, P, a.dyn[inst].vq, p, x, v, x.w, cx, cy, cz);
 }
 
 // Does the hydro pass run for an instance in the current launch?
@@ -389,11 +396,7 @@ __global__ void k_eos(StepArgs a) {
   a.jr[p].a.w = po;
   a.jr[p].b.w = rho;
   a.jC[p] = snds;
-  if (a.jv) {  // the compact record's P/rho^2 and density (a far mark stays)
-    a.jv[p].w = po;
-    const uint2 q = a.jq[p];
-    if ((q.y >> 16) != kFarMark) a.jq[p].y = (q.y & 0xffffu) | (rho_half_bits(P, rho) << 16);
-  }
+  if (a.jh && a.jh[p].w != kFarRho) a.jh[p].w = __float_as_uint(rho);  // the compact record's density
   if (ph != PH_PROBE) a.alt.pos[p].w = rho;
 }
 

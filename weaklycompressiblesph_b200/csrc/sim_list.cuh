@@ -67,11 +67,20 @@ __device__ __forceinline__ void motion_max(unsigned* w, int inst, const Motion& 
   }
 }
 
+// Velocity quantum of the compact records for speeds below vb: 2^-15 of the
+// smallest power of two above max(vb, c0 2^-12).
+__device__ __forceinline__ float velocity_quantum(float vb, float c0) {
+  const float v = fmaxf(vb, c0 * (1.0f / 4096.0f));
+  return __uint_as_float(((__float_as_uint(v) >> 23) + 1u - 15u) << 23);
+}
+
 // One thread, after k_step_begin: the step's build decision, the counters,
 // and (in a graph) the condition of the node that selects the build or the
 // list-step branch.  An instance needs a build when the largest displacement
 // its particles can reach in this step, d + dt s + dt^2/2 acc from the motion
-// the last list pass recorded, reaches kListRebuildAt skins.
+// the last list pass recorded, reaches kListRebuildAt skins.  With compact
+// records the same motion bounds this step's velocities, s + dt acc, which
+// sets the instance's velocity quantum (kept when there is no motion yet).
 __global__ void k_list_set(StepArgs a, int interval, cudaGraphConditionalHandle cond, int use_cond) {
   unsigned* lf = a.list_flags;
   bool moved = false;
@@ -82,6 +91,10 @@ __global__ void k_list_set(StepArgs a, int interval, cudaGraphConditionalHandle 
     if (P.active && P.inv_skin > 0.0f && a.phase[k] == PH_STEP && dt > 0.0f) {
       const float reach = __uint_as_float(w[0]) + dt * __uint_as_float(w[1]) + 0.5f * dt * dt * __uint_as_float(w[2]);
       moved |= reach >= kListRebuildAt;
+      if (a.jh && (w[1] | w[2])) {
+        const float vb = (__uint_as_float(w[1]) + dt * __uint_as_float(w[2])) / P.inv_skin;
+        a.dyn[k].vq = velocity_quantum(vb * 1.001f, P.c0);
+      }
     }
     w[0] = w[1] = w[2] = 0u;  // refilled by this step's list pass
   }
@@ -129,8 +142,8 @@ __global__ void k_kick_refresh(StepArgs a) {
     a.jr[p].b = make_float4(v.x, v.y, v.z, x.w);
     a.jC[p] = snds;
     const float4 o = a.x0[p];
-    if (a.jv)  // compact record relative to the particle's cell at the build
-      write_h16(a.jv, a.jq, P, p, x, v, po, x.w, cell_of(o.x, P.lo[0], P.inv_cell[0], P.ncell[0]),
+    if (a.jh)  // compact record relative to the particle's cell at the build
+      write_h16(a.jh, P, a.dyn[inst].vq, p, x, v, x.w, cell_of(o.x, P.lo[0], P.inv_cell[0], P.ncell[0]),
                 cell_of(o.y, P.lo[1], P.inv_cell[1], P.ncell[1]), cell_of(o.z, P.lo[2], P.inv_cell[2], P.ncell[2]));
     const float dx = x.x - o.x, dy = x.y - o.y, dz = x.z - o.z;
     const float r = sqrtf(dx * dx + dy * dy + dz * dz) * P.inv_skin;
@@ -139,7 +152,7 @@ __global__ void k_kick_refresh(StepArgs a) {
     a.jr[p].a = make_float4(1.0e30f, 1.0e30f, 1.0e30f, 0.f);
     a.jr[p].b = make_float4(0.f, 0.f, 0.f, 1.f);
     a.jC[p] = 0.f;
-    if (a.jv) write_h16_dead(a.jv, a.jq, p);
+    if (a.jh) write_h16_dead(a.jh, p);
   }
 }
 
@@ -151,21 +164,20 @@ __device__ __forceinline__ void build_cell(const StepArgs& a, const InstParams& 
   c[2] = cell_of(o.z, P.lo[2], P.inv_cell[2], P.ncell[2]);
 }
 
-// Neighbour-cell offsets + 1 of an offset code k = (ox+1) + 3 (oy+1) + 9 (oz+1).
-__device__ __forceinline__ void offset_code(uint32_t k, uint32_t& ox1, uint32_t& oy1, uint32_t& oz1) {
-  const uint32_t t = (k * 11u) >> 5;  // k / 3 for k < 32
-  ox1 = k - 3u * t;
-  oz1 = (t * 11u) >> 5;  // t / 3
-  oy1 = t - 3u * oz1;
+// Neighbour-cell offsets + 1 (0, 1, 2 per axis) of a half2 list entry.
+__device__ __forceinline__ void h16_offsets(uint32_t e, uint32_t& ox1, uint32_t& oy1, uint32_t& oz1) {
+  ox1 = (e >> kH16SlotBits) & 3u;
+  oy1 = (e >> (kH16SlotBits + 2)) & 3u;
+  oz1 = e >> (kH16SlotBits + 4);
 }
 
-// Periodic image shift of an entry with offset code k for a particle in
-// build cell c: the neighbour cell c + o wraps past an edge on an axis exactly
-// where the image code of the FP32 list build would name a shift.
-__device__ __forceinline__ void offset_shift(const InstParams& P, const int c[3], uint32_t k, float& sx, float& sy,
+// Periodic image shift of a half2 list entry for a particle in build cell c:
+// the neighbour cell c + o wraps past an edge on an axis exactly where the
+// image code of the FP32 list build would name a shift.
+__device__ __forceinline__ void offset_shift(const InstParams& P, const int c[3], uint32_t e, float& sx, float& sy,
                                              float& sz) {
   uint32_t o1[3];
-  offset_code(k, o1[0], o1[1], o1[2]);
+  h16_offsets(e, o1[0], o1[1], o1[2]);
   float sh[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -209,11 +221,11 @@ __global__ void __launch_bounds__(128) k_density_list(StepArgs a) {
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       if (k + u < n) {
-        const int q = ent[u] & kSlotMask;
+        const int q = ent[u] & (H16 ? kH16SlotMask : kSlotMask);
         const float4 J = __ldg(&a.jr[q].a);
         float sx = 0.f, sy = 0.f, sz = 0.f;
         if (P.periodic) {
-          if (H16) offset_shift(P, ci, ent[u] >> 27, sx, sy, sz);
+          if (H16) offset_shift(P, ci, ent[u], sx, sy, sz);
           else entry_shift(P, ent[u] >> 27, sx, sy, sz);
         }
         const float dx = __fsub_rn(I.x, __fadd_rn(J.x, sx));
@@ -249,82 +261,113 @@ __device__ __forceinline__ f2 snds7_2(f2 RHO, f2 RHO0, f2 IRHO0, f2 C0) {
 
 // i-side operands of the half2 list pass: i's position relative to the
 // centre of its build cell (FP32, exact: the two are within a factor of two),
-// its build cell, and the scales -cell / 2^15 that turn the 16-bit offsets
-// into lengths.
+// its build cell, the scales -cell / 2^15 that turn the 16-bit offsets into
+// lengths, and the instance's velocity quantum.
 struct H16I {
-  f2 QX, QY, QZ, SX, SY, SZ;
+  f2 QX, QY, QZ, SX, SY, SZ, VQ;
   int c[3];
   float band;
 };
 
-// Two list entries (halves a, b) of the half2 list pass.  The displacement of
-// j from i is rebuilt from the 16-bit offsets: x_i - x_j = q_i - (o + q_j)
-// cell, with o the neighbour-cell offset of the entry; the biased offset and
-// o are added as integers below the float mantissa's top (0x4B000000 is
-// 2^23), so one packed subtraction turns them into an exact (q_j + o) 2^15.
-// An entry takes the FP32 record instead (the displacement exactly as the
-// FP32 path and the oracle round it) when its squared distance lies within
-// the band where the 16-bit positions cannot decide 0 < r^2 < (2h)^2, or when
-// j is marked far: the pairs summed, and the neighbour counts, are exactly
-// those of the FP32 support test.
+// 2^23 + the 16 bits of w selected by s (0x7610 low, 0x7632 high) as a float:
+// byte-permuted under the exponent of 2^23.
+__device__ __forceinline__ float h16_magic(uint32_t w, uint32_t s) { return __uint_as_float(__byte_perm(w, 0x4B000000u, s)); }
+
+// (rho / rho0)^7 - 1 in Horner form and P / rho^2 of the two densities
+// (the Tait pressure of tait(), clamped at 0; rho^-2 by the fast quotient).
+__device__ __forceinline__ f2 po7_2(f2 RHO, f2 RHO0, f2 IRHO0, f2 B) {
+  const f2 D = mul2(sub2(RHO, RHO0), IRHO0);
+  f2 X = add2(D, dup(7.0f));
+  X = fma2(D, X, dup(21.0f));
+  X = fma2(D, X, dup(35.0f));
+  X = fma2(D, X, dup(35.0f));
+  X = fma2(D, X, dup(21.0f));
+  X = fma2(D, X, dup(7.0f));
+  X = mul2(mul2(D, X), B);
+  const f2 R2 = mul2(RHO, RHO);
+  return pk(__fdividef(fmaxf(lo(X), 0.0f), lo(R2)), __fdividef(fmaxf(hi(X), 0.0f), hi(R2)));
+}
+
+// Two list entries (halves a, b) of the half2 list pass, from their 16-byte
+// records Qa, Qb.  The displacement of j from i is rebuilt from the 16-bit
+// offsets: x_i - x_j = q_i - (o + q_j) cell, with o the entry's neighbour-cell
+// offset; the biased offset and o + 1 (shifted to 2^15) are added as integers
+// under the exponent of 2^23, so one packed subtraction turns them into an
+// exact (q_j + o) 2^15.  Velocities come the same way, times the velocity
+// quantum (exact); P/rho^2 and c are recomputed from the FP32 density.  An
+// entry takes the FP32 record instead (the displacement exactly as the FP32
+// path and the oracle round it, and j's FP32 velocity and density) when its
+// squared distance lies within the band where the 16-bit positions cannot
+// decide 0 < r^2 < (2h)^2, or when j is marked far: the pairs summed, and the
+// neighbour counts, are exactly those of the FP32 support test.
 __device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P, const PairC& C, const PairI& I,
-                                          const H16I& H, const float4& Va, const float4& Vb, uint2 Qa, uint2 Qb,
-                                          uint32_t ea, uint32_t eb, bool qva, bool qvb, bool g7, f2& AX, f2& AY,
+                                          const H16I& H, const uint4& Qa, const uint4& Qb, uint32_t ea, uint32_t eb,
+                                          bool qva, bool qvb, bool g7, f2 RHO0, f2 IRHO0, f2 C0, f2 B, f2& AX, f2& AY,
                                           f2& AZ, f2& DS, float& vsa, float& vsb, unsigned& na, unsigned& nb) {
-  const f2 MAG = dup(8388608.0f + 65536.0f);
-  uint32_t oxa, oya, oza, oxb, oyb, ozb;
-  offset_code(ea >> 27, oxa, oya, oza);
-  offset_code(eb >> 27, oxb, oyb, ozb);
-  auto fb = [](uint32_t u16, uint32_t o1) { return __uint_as_float(0x4B000000u + u16 + (o1 << 15)); };
-  const f2 TX = sub2(pk(fb(Qa.x & 0xffffu, oxa), fb(Qb.x & 0xffffu, oxb)), MAG);
-  const f2 TY = sub2(pk(fb(Qa.x >> 16, oya), fb(Qb.x >> 16, oyb)), MAG);
-  const f2 TZ = sub2(pk(fb(Qa.y & 0xffffu, oza), fb(Qb.y & 0xffffu, ozb)), MAG);
+  const f2 MAG = dup(8388608.0f + 65536.0f), MAGV = dup(8388608.0f + 32768.0f);
+  constexpr uint32_t kLo = 0x7610u, kHi = 0x7632u, kO = 0x18000u;  // o + 1 shifted to bits 15-16
+  const f2 TX = sub2(pk(__uint_as_float(__float_as_uint(h16_magic(Qa.x, kLo)) + ((ea >> (kH16SlotBits - 15)) & kO)),
+                        __uint_as_float(__float_as_uint(h16_magic(Qb.x, kLo)) + ((eb >> (kH16SlotBits - 15)) & kO))),
+                     MAG);
+  const f2 TY = sub2(pk(__uint_as_float(__float_as_uint(h16_magic(Qa.x, kHi)) + ((ea >> (kH16SlotBits - 13)) & kO)),
+                        __uint_as_float(__float_as_uint(h16_magic(Qb.x, kHi)) + ((eb >> (kH16SlotBits - 13)) & kO))),
+                     MAG);
+  const f2 TZ = sub2(pk(__uint_as_float(__float_as_uint(h16_magic(Qa.y, kLo)) + ((ea >> (kH16SlotBits - 11)) & kO)),
+                        __uint_as_float(__float_as_uint(h16_magic(Qb.y, kLo)) + ((eb >> (kH16SlotBits - 11)) & kO))),
+                     MAG);
   f2 DX = fma2(TX, H.SX, H.QX), DY = fma2(TY, H.SY, H.QY), DZ = fma2(TZ, H.SZ, H.QZ);
   f2 R2raw = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
-  const uint32_t ha = Qa.y >> 16, hb = Qb.y >> 16;
+  f2 VXJ = mul2(sub2(pk(h16_magic(Qa.y, kHi), h16_magic(Qb.y, kHi)), MAGV), H.VQ);
+  f2 VYJ = mul2(sub2(pk(h16_magic(Qa.z, kLo), h16_magic(Qb.z, kLo)), MAGV), H.VQ);
+  f2 VZJ = mul2(sub2(pk(h16_magic(Qa.z, kHi), h16_magic(Qb.z, kHi)), MAGV), H.VQ);
+  const bool fa = Qa.w == kFarRho, fb = Qb.w == kFarRho;
   float r2a = lo(R2raw), r2b = hi(R2raw);
-  const bool xa = qva && (ha == kFarMark || r2a < H.band || fabsf(r2a - C.H2) < H.band);
-  const bool xb = qvb && (hb == kFarMark || r2b < H.band || fabsf(r2b - C.H2) < H.band);
+  const bool xa = qva && (fa || r2a < H.band || fabsf(r2a - C.H2) < H.band);
+  const bool xb = qvb && (fb || r2b < H.band || fabsf(r2b - C.H2) < H.band);
   // a far record's density comes from its FP32 record (exact path); an idle
   // half naming one still needs a finite stand-in (its terms are multiplied
   // by zero, and NaN times zero is NaN)
-  float rja = ha == kFarMark ? P.rho0 : P.rho0 + __half2float(__ushort_as_half((unsigned short)ha));
-  float rjb = hb == kFarMark ? P.rho0 : P.rho0 + __half2float(__ushort_as_half((unsigned short)hb));
-  if (xa || xb) {  // rare: the exact FP32 displacement of the FP32 path
+  float rja = fa ? P.rho0 : __uint_as_float(Qa.w);
+  float rjb = fb ? P.rho0 : __uint_as_float(Qb.w);
+  if (xa || xb) {  // rare: the exact FP32 record, as the FP32 path reads it
     float dx[2] = {lo(DX), hi(DX)}, dy[2] = {lo(DY), hi(DY)}, dz[2] = {lo(DZ), hi(DZ)}, r2[2] = {r2a, r2b};
-    float rj[2] = {rja, rjb};
+    float rj[2] = {rja, rjb}, vx[2] = {lo(VXJ), hi(VXJ)}, vy[2] = {lo(VYJ), hi(VYJ)}, vz[2] = {lo(VZJ), hi(VZJ)};
     const bool ex[2] = {xa, xb};
     const uint32_t e[2] = {ea, eb};
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       if (!ex[h]) continue;
-      const JRec R = ld_jrec(&a.jr[e[h] & kSlotMask]);
+      const JRec R = ld_jrec(&a.jr[e[h] & kH16SlotMask]);
       float sx = 0.f, sy = 0.f, sz = 0.f;
-      if (P.periodic) offset_shift(P, H.c, e[h] >> 27, sx, sy, sz);
+      if (P.periodic) offset_shift(P, H.c, e[h], sx, sy, sz);
       const float ix = h ? hi(I.X) : lo(I.X), iy = h ? hi(I.Y) : lo(I.Y), iz = h ? hi(I.Z) : lo(I.Z);
       dx[h] = __fsub_rn(ix, __fadd_rn(R.a.x, sx));
       dy[h] = __fsub_rn(iy, __fadd_rn(R.a.y, sy));
       dz[h] = __fsub_rn(iz, __fadd_rn(R.a.z, sz));
       r2[h] = dist2(dx[h], dy[h], dz[h]);
       rj[h] = R.b.w;
+      vx[h] = R.b.x, vy[h] = R.b.y, vz[h] = R.b.z;
     }
     DX = pk(dx[0], dx[1]), DY = pk(dy[0], dy[1]), DZ = pk(dz[0], dz[1]);
     R2raw = pk(r2[0], r2[1]);
     r2a = r2[0], r2b = r2[1];
     rja = rj[0], rjb = rj[1];
+    VXJ = pk(vx[0], vx[1]), VYJ = pk(vy[0], vy[1]), VZJ = pk(vz[0], vz[1]);
   }
   const bool va = qva && r2a > 0.0f && r2a < C.H2;
   const bool vb = qvb && r2b > 0.0f && r2b < C.H2;
   na += va, nb += vb;
   const f2 RHOJ = pk(rja, rjb);
-  f2 CJ;
+  f2 CJ, POJ;
   if (g7) {
-    CJ = snds7_2(RHOJ, dup(P.rho0), dup(P.inv_rho0), dup(P.c0));
+    CJ = snds7_2(RHOJ, RHO0, IRHO0, C0);
+    POJ = po7_2(RHOJ, RHO0, IRHO0, B);
   } else {
-    CJ = pk(__ldg(&a.jC[ea & kSlotMask]), __ldg(&a.jC[eb & kSlotMask]));
+    const uint32_t ga = ea & kH16SlotMask, gb = eb & kH16SlotMask;
+    CJ = pk(__ldg(&a.jC[ga]), __ldg(&a.jC[gb]));
+    POJ = pk(__ldg(&a.jr[ga].a.w), __ldg(&a.jr[gb].a.w));
   }
-  pair_terms2(C, I, DX, DY, DZ, R2raw, va, vb, pk(Va.x, Vb.x), pk(Va.y, Vb.y), pk(Va.z, Vb.z), pk(Va.w, Vb.w), RHOJ,
-              CJ, AX, AY, AZ, DS, vsa, vsb);
+  pair_terms2(C, I, DX, DY, DZ, R2raw, va, vb, VXJ, VYJ, VZJ, POJ, RHOJ, CJ, AX, AY, AZ, DS, vsa, vsb);
 }
 
 // The list pass over particle slots below the build's live count (the
@@ -396,17 +439,20 @@ __global__ void __launch_bounds__(128, MINB) k_hydro_list(StepArgs a) {
         H.QY = dup(R.a.y - cell_centre(P, 1, H.c[1]));
         H.QZ = dup(R.a.z - cell_centre(P, 2, H.c[2]));
         H.SX = dup(-P.cell[0] / kQ16Scale), H.SY = dup(-P.cell[1] / kQ16Scale), H.SZ = dup(-P.cell[2] / kQ16Scale);
+        H.VQ = dup(a.dyn[inst].vq);
         H.band = P.h16_band;
+        const f2 B = dup(P.B);
+        const uint32_t hself = (uint32_t)p | (21u << kH16SlotBits);  // offset (0, 0, 0): i's own record
         for (int k = 4 * sub; k < n; k += 4 * TPI) {
           const uint4 e = __ldg(&row[k >> 2]);
-          const uint32_t e0 = e.x, e1 = k + 1 < n ? e.y : self, e2 = k + 2 < n ? e.z : self,
-                         e3 = k + 3 < n ? e.w : self;
-          const int g0 = e0 & kSlotMask, g1 = e1 & kSlotMask, g2 = e2 & kSlotMask, g3 = e3 & kSlotMask;
-          const float4 V0 = __ldg(&a.jv[g0]), V1 = __ldg(&a.jv[g1]), V2 = __ldg(&a.jv[g2]), V3 = __ldg(&a.jv[g3]);
-          const uint2 Q0 = __ldg(&a.jq[g0]), Q1 = __ldg(&a.jq[g1]), Q2 = __ldg(&a.jq[g2]), Q3 = __ldg(&a.jq[g3]);
-          h16_pair2(a, P, C, I, H, V0, V1, Q0, Q1, e0, e1, true, k + 1 < n, g7, AX, AY, AZ, DS, vsa, vsb, ca, cb);
-          h16_pair2(a, P, C, I, H, V2, V3, Q2, Q3, e2, e3, k + 2 < n, k + 3 < n, g7, AX, AY, AZ, DS, vsa, vsb, ca,
-                    cb);
+          const uint32_t e0 = e.x, e1 = k + 1 < n ? e.y : hself, e2 = k + 2 < n ? e.z : hself,
+                         e3 = k + 3 < n ? e.w : hself;
+          const uint4 Q0 = __ldg(&a.jh[e0 & kH16SlotMask]), Q1 = __ldg(&a.jh[e1 & kH16SlotMask]);
+          const uint4 Q2 = __ldg(&a.jh[e2 & kH16SlotMask]), Q3 = __ldg(&a.jh[e3 & kH16SlotMask]);
+          h16_pair2(a, P, C, I, H, Q0, Q1, e0, e1, true, k + 1 < n, g7, RHO0, IRHO0, C0, B, AX, AY, AZ, DS, vsa,
+                    vsb, ca, cb);
+          h16_pair2(a, P, C, I, H, Q2, Q3, e2, e3, k + 2 < n, k + 3 < n, g7, RHO0, IRHO0, C0, B, AX, AY, AZ, DS,
+                    vsa, vsb, ca, cb);
         }
       } else {
         for (int k = 4 * sub; k < n; k += 4 * TPI) {

@@ -39,6 +39,11 @@ namespace wcsph {
 constexpr int kStageUnroll = 4;            // staging loads in flight per lane
 constexpr uint32_t kSlotMask = (1u << 27) - 1;
 constexpr int kMaxTiledParticles = 1 << 27;  // queue entries hold the slot in 27 bits
+// Half2 list entries: the slot in the low 26 bits, the neighbour cell's offset
+// + 1 per axis (0, 1, 2) in bits 26-27 (x), 28-29 (y), 30-31 (z).
+constexpr int kH16SlotBits = 26;
+constexpr uint32_t kH16SlotMask = (1u << kH16SlotBits) - 1;
+constexpr int kMaxH16ListParticles = 1 << kH16SlotBits;
 
 // Shared memory of a block of WARPS warps with TILE-candidate tiles
 // (TILE a multiple of 64).
@@ -299,6 +304,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
         code = (uint32_t)((shx > 0.f) - (shx < 0.f) + 1) + 3u * (uint32_t)((shy > 0.f) - (shy < 0.f) + 1) +
                9u * (uint32_t)((shz > 0.f) - (shz < 0.f) + 1);
       }
+      // the half2 list build writes the neighbour-cell offset instead, two
+      // bits per axis (its compact records are relative to the build's cells)
+      if (H16 && LB) code = (uint32_t)(lane % 3) | ((uint32_t)((lane / 3) % 3) << 2) | ((uint32_t)(lane / 9) << 4);
     }
     int incl = nb_cnt;
 #pragma unroll
@@ -348,9 +356,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
             const int k = kk[r];
             const float sx = __shfl_sync(full, shx, k), sy = __shfl_sync(full, shy, k), sz = __shfl_sync(full, shz, k);
             // entries carry the image code, or for the half2 list pass the
-            // neighbour-cell offset code k (its compact records are relative
-            // to the cells of the build)
-            const uint32_t ck27 = (H16 && LB ? (uint32_t)k : __shfl_sync(full, code, k)) << 27;
+            // neighbour-cell offset (h16_entry)
+            const uint32_t ck27 = __shfl_sync(full, code, k) << (H16 && LB ? kH16SlotBits : 27);
             if (u < t0 + tn) {
               tx[u - t0] = __fadd_rn(J[r].x, sx);
               ty[u - t0] = __fadd_rn(J[r].y, sy);

@@ -110,6 +110,7 @@ struct InstDyn {
   int range_lo, range_hi;// [first, last+1) sorted slot of this instance after binning
   int n_alive;
   unsigned errors;       // kErrDrift: a slab particle drifted past the ghost-layer margin
+  float vq;              // half2 list records: velocity quantum (a power of two; write_h16)
 };
 
 constexpr unsigned kErrDrift = 1u;
