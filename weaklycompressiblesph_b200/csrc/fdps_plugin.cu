@@ -633,61 +633,94 @@ struct HydroPack {
   float *hic, *hjc;    // compact: c of record q at hic[q] / hjc[q], inside the piece's own part of the C blocks
 };
 
-// Pack walk w: positions relative to its first i-particle (or j when it has
-// no i).  Full staging: A = (x, y, z, h), B = (v, rho), C = (P/rho^2, c, nu, m).
-// Compact: A = (x, y, z, P/rho^2), B, c alone; returns false when a record's
-// h, nu or m differs from the piece's (the piece is then packed again in full).
-static bool pack_hydro_walk(const HydroPack& K, int w) {
+// Origin of walk w: its first i-particle's position (or j when it has no i).
+// Staged positions are relative to it.
+static void walk_origin(const HydroPack& K, int w, double o[3]) {
   const wcsph_fdps_layout& L = *K.L;
-  const char* pi = (const char*)K.epi[w];
-  const char* pj = (const char*)K.epj[w];
-  double o[3] = {0, 0, 0};
+  o[0] = o[1] = o[2] = 0.0;
   if (K.n_epi[w] > 0) {
-    for (int k = 0; k < 3; ++k) o[k] = rd(pi, L.epi_pos + 8 * k);
+    for (int k = 0; k < 3; ++k) o[k] = rd(K.epi[w], L.epi_pos + 8 * k);
   } else if (K.n_epj[w] > 0) {
-    for (int k = 0; k < 3; ++k) o[k] = rd(pj, L.epj_pos + 8 * k);
+    for (int k = 0; k < 3; ++k) o[k] = rd(K.epj[w], L.epj_pos + 8 * k);
   }
+}
+
+// Pack staged records [q0, q1) of one side (i or j) of walks w0.. (the walk
+// of q0 found by bisection of the displacements), positions relative to each
+// walk's origin org[w - w_first].  Full staging: A = (x, y, z, h),
+// B = (v, rho), C = (P/rho^2, c, nu, m).  Compact: A = (x, y, z, P/rho^2), B,
+// c alone.  Returns false when a record's h, nu or m differs from the piece's
+// (the piece is then packed again in full).  Record-parallel: walks of very
+// different sizes (a few carry 40-80x the median j-list) split evenly.
+template <bool J>
+static bool pack_hydro_range(const HydroPack& K, long long q0, long long q1, int w_first, int w_last,
+                             const double* org) {
+  const wcsph_fdps_layout& L = *K.L;
+  const long long* d = J ? K.nj_d : K.ni_d;
+  const void* const* base = J ? K.epj : K.epi;
+  const int size = J ? L.epj_size : L.epi_size;
+  const int o_pos = J ? L.epj_pos : L.epi_pos, o_vel = J ? L.epj_vel : L.epi_vel, o_dens = J ? L.epj_dens : L.epi_dens,
+            o_pres = J ? L.epj_pres : L.epi_pres, o_snds = J ? L.epj_snds : L.epi_snds,
+            o_smth = J ? L.epj_smth : L.epi_smth, o_visc = J ? L.epj_visc : L.epi_visc;
+  float4* A = J ? K.hjA : K.hiA;
+  float4* B = J ? K.hjB : K.hiB;
+  float4* C = J ? K.hjC : K.hiC;
+  float* c1 = J ? K.hjc : K.hic;
+  // the walk holding record q0: last w with d[w] <= q0 (empty walks skipped)
+  int lo = w_first, hi = w_last;  // invariant: d[lo] <= q0 < d[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) / 2;
+    if (d[mid] <= q0) lo = mid;
+    else hi = mid;
+  }
+  int w = lo;
   bool uniform = true;
-  float* hic = K.hic;
-  float* hjc = K.hjc;
-  for (int i = 0; i < K.n_epi[w]; ++i) {
-    const char* r = pi + (size_t)i * L.epi_size;
-    const long long q = K.ni_d[w] + i;
-    const double dens = rd(r, L.epi_dens);
-    const float po = (float)(rd(r, L.epi_pres) / (dens * dens));
-    const float x = (float)(rd(r, L.epi_pos) - o[0]), y = (float)(rd(r, L.epi_pos + 8) - o[1]),
-                z = (float)(rd(r, L.epi_pos + 16) - o[2]);
-    st_stage(&K.hiB[q], (float)rd(r, L.epi_vel), (float)rd(r, L.epi_vel + 8), (float)rd(r, L.epi_vel + 16),
-             (float)dens);
+  for (long long q = q0; q < q1; ++q) {
+    while (q >= d[w + 1]) ++w;
+    const char* r = (const char*)base[w] + (size_t)(q - d[w]) * size;
+    const double* o = org + 3 * (w - w_first);
+    const double dens = rd(r, o_dens);
+    const float po = (float)(rd(r, o_pres) / (dens * dens));
+    const float x = (float)(rd(r, o_pos) - o[0]), y = (float)(rd(r, o_pos + 8) - o[1]),
+                z = (float)(rd(r, o_pos + 16) - o[2]);
+    st_stage(&B[q], (float)rd(r, o_vel), (float)rd(r, o_vel + 8), (float)rd(r, o_vel + 16), (float)dens);
     if (K.compact) {
-      uniform &= rd(r, L.epi_smth) == K.h0 && rd(r, L.epi_visc) == K.nu0;
-      st_stage(&K.hiA[q], x, y, z, po);
-      hic[q] = (float)rd(r, L.epi_snds);
+      uniform &= rd(r, o_smth) == K.h0 && rd(r, o_visc) == K.nu0 && (!J || rd(r, L.epj_mass) == K.m0);
+      st_stage(&A[q], x, y, z, po);
+      c1[q] = (float)rd(r, o_snds);
     } else {
-      st_stage(&K.hiA[q], x, y, z, (float)rd(r, L.epi_smth));
-      st_stage(&K.hiC[q], po, (float)rd(r, L.epi_snds), (float)rd(r, L.epi_visc), 0.f);
-    }
-  }
-  for (int j = 0; j < K.n_epj[w]; ++j) {
-    const char* r = pj + (size_t)j * L.epj_size;
-    const long long q = K.nj_d[w] + j;
-    const double dens = rd(r, L.epj_dens);
-    const float po = (float)(rd(r, L.epj_pres) / (dens * dens));
-    const float x = (float)(rd(r, L.epj_pos) - o[0]), y = (float)(rd(r, L.epj_pos + 8) - o[1]),
-                z = (float)(rd(r, L.epj_pos + 16) - o[2]);
-    st_stage(&K.hjB[q], (float)rd(r, L.epj_vel), (float)rd(r, L.epj_vel + 8), (float)rd(r, L.epj_vel + 16),
-             (float)dens);
-    if (K.compact) {
-      uniform &= rd(r, L.epj_smth) == K.h0 && rd(r, L.epj_visc) == K.nu0 && rd(r, L.epj_mass) == K.m0;
-      st_stage(&K.hjA[q], x, y, z, po);
-      hjc[q] = (float)rd(r, L.epj_snds);
-    } else {
-      st_stage(&K.hjA[q], x, y, z, (float)rd(r, L.epj_smth));
-      st_stage(&K.hjC[q], po, (float)rd(r, L.epj_snds), (float)rd(r, L.epj_visc), (float)rd(r, L.epj_mass));
+      st_stage(&A[q], x, y, z, (float)rd(r, o_smth));
+      st_stage(&C[q], po, (float)rd(r, o_snds), (float)rd(r, o_visc), J ? (float)rd(r, L.epj_mass) : 0.f);
     }
   }
   stage_fence();
   return uniform;
+}
+
+// Pack the i- and j-records of walks [w0, w1) on all host threads, in blocks
+// of kPackBlock records.  Returns false when the piece's records are not
+// uniform in h, nu and m (compact staging only).
+constexpr long long kPackBlock = 2048;
+static bool pack_hydro_piece(const HydroPack& K, int w0, int w1) {
+  std::vector<double> org(3 * (size_t)(w1 - w0));
+#pragma omp parallel for schedule(static)
+  for (int w = w0; w < w1; ++w) walk_origin(K, w, &org[3 * (size_t)(w - w0)]);
+  const long long a0 = K.ni_d[w0], a1 = K.ni_d[w1], b0 = K.nj_d[w0], b1 = K.nj_d[w1];
+  const long long ni_blk = (a1 - a0 + kPackBlock - 1) / kPackBlock, nj_blk = (b1 - b0 + kPackBlock - 1) / kPackBlock;
+  int mixed = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(| : mixed)
+  for (long long t = 0; t < ni_blk + nj_blk; ++t) {
+    bool u;
+    if (t < nj_blk) {
+      const long long q0 = b0 + t * kPackBlock;
+      u = pack_hydro_range<true>(K, q0, std::min(b1, q0 + kPackBlock), w0, w1, org.data());
+    } else {
+      const long long q0 = a0 + (t - nj_blk) * kPackBlock;
+      u = pack_hydro_range<false>(K, q0, std::min(a1, q0 + kPackBlock), w0, w1, org.data());
+    }
+    mixed |= u ? 0 : 1;
+  }
+  return !mixed;
 }
 
 // Shared dispatch body.  kind selects the record shapes and the kernel.
@@ -800,13 +833,9 @@ static int dispatch_common(int kind, int32_t tag, int32_t n_walk, const void* co
           K.compact = true;
           K.h0 = rd(r, L.epj_smth), K.nu0 = rd(r, L.epj_visc), K.m0 = rd(r, L.epj_mass);
         }
-      int mixed = 0;
-#pragma omp parallel for schedule(dynamic, 16) reduction(| : mixed)
-      for (int w = w0; w < w1; ++w) mixed |= pack_hydro_walk(K, w) ? 0 : 1;
-      if (K.compact && mixed) {
+      if (!pack_hydro_piece(K, w0, w1) && K.compact) {
         K.compact = false;
-#pragma omp parallel for schedule(dynamic, 16)
-        for (int w = w0; w < w1; ++w) pack_hydro_walk(K, w);
+        pack_hydro_piece(K, w0, w1);
       }
       compact = K.compact;
       if (compact) pp.h = (float)K.h0, pp.nu = (float)K.nu0, pp.m = (float)K.m0;
