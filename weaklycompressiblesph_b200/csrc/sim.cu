@@ -308,17 +308,40 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
 
 // A step that reads the neighbour lists (sim_list.cuh): no sort, no scan.
 // The list-step branch (the step has begun in the prologue).
-static int enqueue_reuse(SimImpl& S, StepArgs a, bool density, int* launches, cudaEvent_t* ev = nullptr) {
+// The list step.  When dens_body is given (capture of the list-step branch
+// of the step graph, whose conditional handle dcond was created on that
+// branch's graph), the density pass sits under a conditional node that
+// k_kick_refresh opens only when some instance has a density pass due (most
+// steps have none, and the two kernels would only return at once); the
+// node's body is left in *dens_body for the caller to capture.
+static int enqueue_reuse(SimImpl& S, StepArgs a, bool density, int* launches, cudaEvent_t* ev = nullptr,
+                         cudaGraphConditionalHandle dcond = 0, cudaGraph_t* dens_body = nullptr) {
   const int n = S.n_host;
   a.list_reuse = 1;
   a.x0 = S.x0;    // read by k_kick_refresh (the displacement since the build)
   a.alt = a.main;  // in place: no re-sort, each particle's state is its own thread's
   int L = 0;
   if (n > 0) {
-    k_kick_refresh<<<nblk(n), kBlock, 0, S.s>>>(a);
+    const bool cond_density = density && dens_body;
+    k_kick_refresh<<<nblk(n), kBlock, 0, S.s>>>(a, dcond, cond_density ? 1 : 0);
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));
-    if (density) {  // the kernels return at once for instances with no density pass due
+    if (cond_density) {
+      cudaStreamCaptureStatus st;
+      cudaGraph_t cg = nullptr;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t ndeps = 0;
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = dcond;
+      cp.conditional.type = cudaGraphCondTypeIf;
+      cp.conditional.size = 1;
+      cudaGraphNode_t node = nullptr;
+      WCSPH_CUDA(cudaStreamGetCaptureInfo(S.s, &st, nullptr, &cg, &deps, &ndeps));
+      WCSPH_CUDA(cudaGraphAddNode(&node, cg, deps, ndeps, &cp));
+      WCSPH_CUDA(cudaStreamUpdateCaptureDependencies(S.s, &node, 1, cudaStreamSetCaptureDependencies));
+      *dens_body = cp.conditional.phGraph_out[0];
+    } else if (density) {  // the kernels return at once for instances with no density pass due
       if (int rc = launch_density_list(a, n, S.s, h16_lists(S.opt))) return rc;
       k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
       L += 2;
@@ -334,6 +357,18 @@ static int enqueue_reuse(SimImpl& S, StepArgs a, bool density, int* launches, cu
   }
   WCSPH_CUDA(cudaGetLastError());
   if (launches) *launches = L;
+  return 0;
+}
+
+// The density pass of a list step (the body of enqueue_reuse's conditional node).
+static int enqueue_list_density(SimImpl& S, StepArgs a) {
+  const int n = S.n_host;
+  a.list_reuse = 1;
+  a.x0 = S.x0;
+  a.alt = a.main;
+  if (int rc = launch_density_list(a, n, S.s, h16_lists(S.opt))) return rc;
+  k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
+  WCSPH_CUDA(cudaGetLastError());
   return 0;
 }
 
@@ -643,15 +678,30 @@ static int capture_list_graph(SimImpl& S) {
   cudaGraph_t out = nullptr;
   const cudaError_t e = cudaStreamEndCapture(S.s, &out);
   if (rc || e != cudaSuccess) return fail(rc, "prologue");
+  // the list-step branch's own conditional (its density pass), set by k_kick_refresh
+  cudaGraphConditionalHandle dcond = 0;
+  if (S.any_density &&
+      cudaGraphConditionalHandleCreate(&dcond, cp.conditional.phGraph_out[1], 0, cudaGraphCondAssignDefault) !=
+          cudaSuccess)
+    return fail(WCSPH_E_CUDA, "density conditional handle");
   for (int branch = 0; branch < 2; ++branch) {
     if (cudaStreamBeginCaptureToGraph(S.s, cp.conditional.phGraph_out[branch], nullptr, nullptr, 0, mode) !=
         cudaSuccess)
       return fail(WCSPH_E_CUDA, "begin branch capture");
+    cudaGraph_t dens_body = nullptr;
     rc = branch == 0 ? enqueue_pass(S, a, S.any_density, false, &S.kernels_per_step, nullptr, true, true)
-                     : enqueue_reuse(S, a, S.any_density, &S.kernels_reuse);
+                     : enqueue_reuse(S, a, S.any_density, &S.kernels_reuse, nullptr, dcond,
+                                     S.any_density ? &dens_body : nullptr);
     cudaGraph_t bo = nullptr;
     const cudaError_t eb = cudaStreamEndCapture(S.s, &bo);
     if (rc || eb != cudaSuccess) return fail(rc, branch == 0 ? "build branch" : "list-step branch");
+    if (dens_body) {  // the list step's density pass, under its conditional node
+      if (cudaStreamBeginCaptureToGraph(S.s, dens_body, nullptr, nullptr, 0, mode) != cudaSuccess)
+        return fail(WCSPH_E_CUDA, "begin density capture");
+      rc = enqueue_list_density(S, a);
+      const cudaError_t ed = cudaStreamEndCapture(S.s, &bo);
+      if (rc || ed != cudaSuccess) return fail(rc, "list-step density pass");
+    }
   }
   const cudaError_t ei = cudaGraphInstantiate(&S.gexec, g, 0);
   cudaGraphDestroy(g);
@@ -1396,7 +1446,7 @@ static int enqueue_probe_lists(SimImpl& S, int density_pass) {
   WCSPH_CUDA(cudaMemsetAsync(S.d_counters + 4, 0, sizeof(int), S.s));
   k_step_begin<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
   if (n > 0) {
-    k_kick_refresh<<<nblk(n), kBlock, 0, S.s>>>(a);
+    k_kick_refresh<<<nblk(n), kBlock, 0, S.s>>>(a, 0, 0);
     if (density_pass) {
       if (int rc = launch_density_list(a, n, S.s, h16_lists(S.opt))) return rc;
       k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);

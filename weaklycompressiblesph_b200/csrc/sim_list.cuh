@@ -118,8 +118,11 @@ __global__ void k_list_set(StepArgs a, int interval, cudaGraphConditionalHandle 
 // order, with the EoS j-records refreshed and |x - x0| checked.  List steps
 // run on one buffer set (alt = main): every particle's state is read and
 // written by its own thread only, so the list pass updates it in place too.
-__global__ void k_kick_refresh(StepArgs a) {
+__global__ void k_kick_refresh(StepArgs a, cudaGraphConditionalHandle dens_cond, int use_dens_cond) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  // in the step graph: open the density pass's conditional node when some
+  // instance has a density pass due (k_step_begin set dens_any)
+  if (p == 0 && use_dens_cond) cudaGraphSetConditional(dens_cond, *a.dens_any ? 1u : 0u);
   if (p >= a.n_host) return;
   uint32_t f = a.main.flags[p];
   const int inst = f & kInstMask;
