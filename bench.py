@@ -61,7 +61,9 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble and serving samples")
     ap.add_argument("--ensemble-steps", type=int, default=60)
     ap.add_argument("--ensemble-precision", default="half2", choices=["tiled", "half2"],
-                    help="precision of the batched ensemble and served requests (config: half2 pairs)")
+                    help="precision of the batched ensemble (config: half2 pairs; the FP32 list path is timed beside it)")
+    ap.add_argument("--serving-precision", default="tiled", choices=["tiled", "half2"],
+                    help="precision of the served requests (the config names none: the default FP32 list path)")
     ap.add_argument("--serving-requests", type=int, default=16)
     ap.add_argument("--serving-nmax", type=float, default=2e5, help="largest request (config: 2e6 particles)")
     ap.add_argument("--serving-tend", type=float, default=0.1, help="physical end time (config: 1.0 s)")
@@ -470,11 +472,19 @@ def measure_ensemble(device, steps=None):
     b = ensemble.run_batched(ens, steps=steps, warmup=3, device=device, list_interval=ARGS.list_interval,
                              precision=ARGS.ensemble_precision)
     s = ensemble.run_serial(ens, steps=steps, warmup=3, precision="fp32", device=device)
+    other = None
+    if ARGS.ensemble_precision != "tiled":  # the default FP32 list path on the same instances
+        o = ensemble.run_batched(ens, steps=steps, warmup=3, device=device, list_interval=ARGS.list_interval,
+                                 precision="tiled")
+        other = {"precision": "tiled", "batched_particle_steps_per_s": o["particle_steps_per_s"],
+                 "speedup_vs_serial_plain": o["particle_steps_per_s"] / s["particle_steps_per_s"],
+                 "lists": _list_summary(o.get("lists"))}
     return {"instances": len(ens), "particles": b["particles"], "steps": steps,
             "precision": ARGS.ensemble_precision,
             "batched_particle_steps_per_s": b["particle_steps_per_s"],
             "serial_plain_particle_steps_per_s": s["particle_steps_per_s"],
             "speedup_vs_serial_plain": b["particle_steps_per_s"] / s["particle_steps_per_s"],
+            "fp32_lists": other,
             "tuning": b.get("tuning"),
             "lists": _list_summary(b.get("lists")),
             "sample": f"{steps} timed steps per instance" + ("" if steps >= 2000 else " (config: 2000)"),
@@ -495,7 +505,7 @@ def measure_serving(device):
                                   n_max=ARGS.serving_nmax, t_end=ARGS.serving_tend)
     total = sum(c.n for _, c in reqs)
     with Server(budget_bytes=150e9, max_particles=total + 1024, device=device, read_results=False,
-                list_interval=ARGS.list_interval, precision=precision_code(ARGS.ensemble_precision)) as srv:
+                list_interval=ARGS.list_interval, precision=precision_code(ARGS.serving_precision)) as srv:
         out = srv.run(reqs)
     el = 0.0
     ps = 0
@@ -509,7 +519,7 @@ def measure_serving(device):
             "speedup_vs_serial_plain": out["particle_steps_per_s"] / (ps / el),
             "neighbour_search": (f"lists, rebuilt at least every {ARGS.list_interval} steps" if ARGS.list_interval
                                  else "every step") + "; serial baseline: plain FP32, search every step",
-            "precision": ARGS.ensemble_precision,
+            "precision": ARGS.serving_precision,
             "lists": _list_summary(out.get("lists")),
             "sample": f"{len(reqs)} requests, counts log-uniform [2e4, {ARGS.serving_nmax:.0e}], "
                       f"t_end {ARGS.serving_tend:g} s, Poisson 20/s, budget 150 GB"
