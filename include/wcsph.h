@@ -369,6 +369,13 @@ int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out4);
  * step builds again), out[3] largest list built so far, out[4] kernel
  * launches of a build step, out[5] kernel launches of a list step. */
 int wcsph_sim_list_stats(wcsph_sim* sim, int64_t* out6);
+/* The neighbour-list schedule (list_interval > 0): out[0] builds, out[1]
+ * partial builds among them (only the instances whose particles could reach
+ * half the skin re-sorted and rebuilt; the others kept their lists), out[2]
+ * steps that read the lists, out[3] steps since the last full build.  No
+ * counterpart in the reference (its FDPS call rebuilds every interaction
+ * list each step, main.cpp:107-121, param.h:11). */
+int wcsph_sim_list_schedule(wcsph_sim* sim, int64_t* out4);
 /* Entries of the current neighbour lists over all particles (what one list
  * pass reads: each entry a list word and a j-record), 0 without current
  * lists, -1 on error. */

@@ -319,3 +319,72 @@ def test_profile_split_follows_the_schedule(native):
         s.add(case)
         sp = s.profile_split(4)
     assert sp["build_steps"] == 4 and sp["list_steps"] == 0 and sp["scan_ms"] == 0.0
+
+
+def calm_and_fast():
+    """A dam break at rest beside a periodic lattice whose particles move at
+    metres per second: the lattice needs new lists every few steps, the dam
+    break none within the run, so most builds are partial."""
+    calm = small_dam(dx=0.04, seed=9, vel_sigma=0.0)
+    fast = cases.periodic_lattice(n_side=12, dx=0.01, seed=3,
+                                  phys=cases.Physics(g=0.0, density_mode=N.DENSITY_CONTINUITY))
+    fast.vel = np.random.default_rng(4).normal(0.0, 2.0, size=fast.vel.shape)
+    return calm, fast
+
+
+def run_pair(calm, fast, steps, list_interval, probe=False):
+    with Solver(calm.n + fast.n, precision=N.PREC_TILED, list_interval=list_interval) as s:
+        kc, kf = s.add(calm), s.add(fast)
+        s.step(steps)
+        states = [s.read(kc), s.read(kf)]
+        sched = s.list_schedule() if list_interval else None
+        probes = [s.probe(k, lists=True) for k in (kc, kf)] if probe else None
+    return states, sched, probes
+
+
+def periodic_rel(got, ref, case):
+    L = np.array(case.hi) - np.array(case.lo)
+    d = got - ref
+    d -= L * np.round(d / L)
+    return np.linalg.norm(d) / np.linalg.norm(ref)
+
+
+def test_partial_builds_keep_calm_instances(native, oracle_lib):
+    """Partial builds: only the instance whose particles could reach half the
+    skin is re-sorted and gets new lists; the other keeps its lists, cells
+    and slots.  The list passes of both match the FP64 oracle, and both
+    trajectories match the per-step search."""
+    calm, fast = calm_and_fast()
+    ref, _, _ = run_pair(calm, fast, 40, 0)
+    got, sched, probes = run_pair(calm, fast, 40, 30, probe=True)
+    assert sched["partial_builds"] >= 5 and sched["builds"] >= sched["partial_builds"] + 1
+    assert sched["builds"] + sched["list_steps"] == 40
+    for case, st, pr in zip((calm, fast), got, probes):
+        r = oracle_list_check(oracle_lib, case, st, pr, 0)
+        np.testing.assert_array_equal(pr["nbr"], r["cnt"])
+        assert r["acc"] < 1e-5 and r["div_v"] < 1e-5, r
+    assert rel_l2(got[0]["pos"], ref[0]["pos"]) < 1e-6
+    assert periodic_rel(got[1]["pos"], ref[1]["pos"], fast) < 1e-6
+    for a, b in zip(got, ref):
+        assert rel_l2(a["vel"], b["vel"]) < 1e-4
+        assert rel_l2(a["dens"], b["dens"]) < 1e-6
+
+
+def test_removal_during_partial_builds(native):
+    """Particles leaving the kill box while the other instance forces partial
+    builds stay in place, marked dead, until the next build compacts them in
+    full; the survivors' trajectories match the per-step search."""
+    calm, fast = calm_and_fast()
+    fluid = np.nonzero(calm.type == N.HYDRO)[0]
+    fluid = fluid[np.argsort(-calm.pos[fluid, 2], kind="stable")]  # top surface first
+    calm.vel[fluid[:5]] = [0.0, 0.0, 200.0]
+    calm.kill_hi = (calm.kill_hi[0], calm.kill_hi[1], 1.2)
+    ref, _, _ = run_pair(calm, fast, 40, 0)
+    got, sched, _ = run_pair(calm, fast, 40, 30)
+    assert sched["partial_builds"] >= 5
+    assert np.all(got[0]["alive"][fluid[:5]] == 0) and got[0]["alive"].sum() == calm.n - 5
+    assert np.array_equal(got[0]["alive"], ref[0]["alive"])
+    alive = got[0]["alive"] == 1
+    assert rel_l2(got[0]["pos"][alive], ref[0]["pos"][alive]) < 1e-6
+    assert rel_l2(got[0]["vel"][alive], ref[0]["vel"][alive]) < 1e-4
+    assert periodic_rel(got[1]["pos"], ref[1]["pos"], fast) < 1e-6

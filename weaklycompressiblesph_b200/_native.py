@@ -127,6 +127,7 @@ _SIGS = {
     "wcsph_sim_list_entries": (C.c_int64, [P]),
     "wcsph_sim_profile_steps": (C.c_int, [P, C.c_int32, F64P]),
     "wcsph_sim_profile_split": (C.c_int, [P, C.c_int32, F64P, C.POINTER(C.c_int32)]),
+    "wcsph_sim_list_schedule": (C.c_int, [P, C.POINTER(C.c_int64)]),
 }
 
 

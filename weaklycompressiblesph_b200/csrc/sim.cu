@@ -84,6 +84,7 @@ struct SimImpl {
   int* list_cnt = nullptr;
   float4* x0 = nullptr;
   uint4* jh = nullptr;  // compact j-records of the half2 list pass (write_h16)
+  int* d_keep = nullptr;  // per instance: keeps its lists in a partial build (k_list_set)
   unsigned* d_lflags = nullptr;       // kLfWords words, see ListFlag
   unsigned* d_motion = nullptr;       // 3 words per instance, see StepArgs::inst_motion
   unsigned* h_lflags = nullptr;       // pinned copy, written at the end of every list-mode step
@@ -208,6 +209,7 @@ static StepArgs make_args(SimImpl& S) {
     a.list_max = kListMax;
     a.list_flags = S.d_lflags;
     a.inst_motion = S.d_motion;
+    a.inst_keep = S.d_keep;
     a.jh = S.jh;
   }
   return a;
@@ -241,6 +243,7 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
   const int n = S.n_host;
   if (build_lists) a.x0 = S.x0;
   else S.lists_valid = false;  // any other pass re-sorts or changes what the lists refer to
+  if (!after_prologue) a.inst_keep = nullptr;  // partial builds happen only in a list step's build branch
   if (after_prologue) {  // a list-mode build branch: the step has begun
     k_begin_build<<<nblk(std::max<int>(1, (int)S.inst.size())), kBlock, 0, S.s>>>(a);
   } else {
@@ -266,6 +269,12 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));
     if (density) {
       k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(a);
+      if (a.inst_keep) {  // a partial build: the instances that keep their lists read them
+        StepArgs b = a;
+        b.density_keep_only = 1;
+        if (int rc = launch_density_list(b, n, S.s, h16_lists(S.opt))) return rc;
+        ++L;
+      }
       k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
       L += 2;
     }
@@ -801,6 +810,7 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
     rc |= alloc(S, (void**)&S.x0, N * sizeof(float4));
     rc |= alloc(S, (void**)&S.d_lflags, kLfWords * sizeof(unsigned));
     rc |= alloc(S, (void**)&S.d_motion, 3 * (size_t)opt->max_instances * sizeof(unsigned));
+    rc |= alloc(S, (void**)&S.d_keep, (size_t)opt->max_instances * sizeof(int));
     if (h16_lists(*opt)) {
       rc |= alloc(S, (void**)&S.jh, N * sizeof(uint4));
     }
@@ -821,7 +831,8 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
   if (S.d_lflags) {
     memset(S.h_lflags, 0, kLfWords * sizeof(unsigned));
     if (cudaMemsetAsync(S.d_lflags, 0, kLfWords * sizeof(unsigned), S.s) != cudaSuccess ||
-        cudaMemsetAsync(S.d_motion, 0, 3 * (size_t)opt->max_instances * sizeof(unsigned), S.s) != cudaSuccess)
+        cudaMemsetAsync(S.d_motion, 0, 3 * (size_t)opt->max_instances * sizeof(unsigned), S.s) != cudaSuccess ||
+        cudaMemsetAsync(S.d_keep, 0, (size_t)opt->max_instances * sizeof(int), S.s) != cudaSuccess)
       return fail(WCSPH_E_CUDA);
   }
   *out = sim;
@@ -1599,6 +1610,20 @@ int wcsph_sim_list_stats(wcsph_sim* sim, int64_t* out6) {
   out6[3] = (int64_t)lf[kLfLongest];
   out6[4] = S.kernels_per_step;
   out6[5] = S.kernels_reuse;
+  return 0;
+}
+
+int wcsph_sim_list_schedule(wcsph_sim* sim, int64_t* out4) {
+  if (!sim || !out4) return WCSPH_E_INVALID;
+  SimImpl& S = sim->impl;
+  WCSPH_CUDA(cudaSetDevice(S.opt.device));
+  WCSPH_CUDA(cudaStreamSynchronize(S.s));
+  unsigned lf[kLfWords] = {};
+  if (S.d_lflags) WCSPH_CUDA(cudaMemcpy(lf, S.d_lflags, sizeof(lf), cudaMemcpyDeviceToHost));
+  out4[0] = lf[kLfBuilds];
+  out4[1] = lf[kLfPartials];
+  out4[2] = lf[kLfListSteps];
+  out4[3] = (int64_t)lf[kLfSince];
   return 0;
 }
 

@@ -120,6 +120,8 @@ struct StepArgs {
   int* dens_any;          // set by k_step_begin when any instance has a density pass in this launch
   unsigned* inst_motion;  // neighbour lists: per instance, the largest |x - x0|, |v| and |a| over its moving
                           // particles at the end of the step, in units of its skin (float bits)
+  int* inst_keep;          // neighbour lists, partial builds: per instance, 1 = keeps its lists (k_list_set)
+  int density_keep_only;   // a partial build's list density pass: only the instances that keep their lists
   // compact j-records of the half2 list pass (WCSPH_PREC_HALF2 with lists; null otherwise)
   uint4* jh;              // 16-bit cell-relative x, y, z, 16-bit velocity, FP32 rho (write_h16)
   int probe_density;      // density pass of a probe launch: 0 none, 1 summation, 2 Shepard
@@ -200,7 +202,7 @@ __device__ __forceinline__ bool wrap_periodic(const InstParams& P, float4& x) {
 // steps), escapee removal (Dam2.h:117-122).  Returns true when the state
 // changed; dead is set when the particle left the kill box.
 __device__ __forceinline__ bool kick_particle(const StepArgs& a, const InstParams& P, int inst, int p, uint32_t f,
-                                              float4& x, float4& v, float4& vh, bool& dead) {
+                                              float4& x, float4& v, float4& vh, bool& dead, bool keep = false) {
   const int ph = a.phase[inst];
   const float dt = a.dyn[inst].dt_cur;
   if (!(ph == PH_STEP && dt > 0.0f)) return false;
@@ -215,7 +217,7 @@ __device__ __forceinline__ bool kick_particle(const StepArgs& a, const InstParam
     if (P.slab_margin2 > 0.0f && dt * dt * (vh.x * vh.x + vh.y * vh.y + vh.z * vh.z) > P.slab_margin2)
       atomicOr(&a.dyn[inst].errors, kErrDrift);  // the ghost layer no longer covers this drift
     v = make_float4(v.x + dt * acc.x, v.y + dt * acc.y, v.z + dt * acc.z, 0.f);
-    if (P.periodic && !a.list_reuse) wrap_periodic(P, x);  // between list builds positions run on continuously
+    if (P.periodic && !a.list_reuse && !keep) wrap_periodic(P, x);  // between list builds positions run on continuously
     if (P.kill_on) {
       const float* c = &x.x;
 #pragma unroll
@@ -228,30 +230,49 @@ __device__ __forceinline__ bool kick_particle(const StepArgs& a, const InstParam
 
 // The kick, the periodic wrap (every binning pass: positions run on
 // continuously between neighbour-list builds), then the Morton cell key of
-// each particle.
+// each particle.  In a partial list build, an instance that keeps its lists
+// (inst_keep) is kicked like a list step (no wrap, |x - x0| checked) and keyed
+// by its build positions x0, so the stable sort leaves its particles in
+// their slots; a particle removed during a partial build keeps the key of
+// its build position too (in place, marked dead, far records), and the next
+// step builds in full.
 __global__ void k_kick_bin(StepArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.n_host) return;
   uint32_t f = a.main.flags[p];
   const int inst = f & kInstMask;
   const InstParams& P = a.params[inst];
-  bool dead = (f & kDeadBit) || !P.active;
+  const bool was_dead = (f & kDeadBit) || !P.active;
+  bool dead = was_dead;
+  const bool partial = a.inst_keep && a.list_flags[9] != 0u;  // kLfPartial
+  const bool keep = partial && a.inst_keep[inst];
   float4 x = a.main.pos[p];
   float4 v = a.main.vel[p];
   float4 vh = v;
-  bool changed = !dead && kick_particle(a, P, inst, p, f, x, v, vh, dead);
+  bool changed = !dead && kick_particle(a, P, inst, p, f, x, v, vh, dead, keep);
   // passes without a kick (probe, initial and binning passes) wrap too, so
   // that positions left outside the box by list steps are binned correctly
-  if (!dead && !changed && P.periodic && wrap_periodic(P, x)) changed = true;
+  if (!dead && !changed && !keep && P.periodic && wrap_periodic(P, x)) changed = true;
   if (changed) {
     a.main.pos[p] = x;
     a.main.vel[p] = v;
   }
   a.main.vh[p] = vh;
   uint32_t key = kDeadKey;
-  if (dead) {
-    if (!(f & kDeadBit)) a.main.flags[p] = f | kDeadBit;
-  } else {
+  if (dead && !(f & kDeadBit)) a.main.flags[p] = f | kDeadBit;
+  // (particles removed before this step sit in the tail since the last full
+  // build, which every removal forces: they keep the dead key)
+  if (partial && !was_dead && (keep || dead)) {
+    const float4 o = a.x0[p];  // the build position: the particle keeps its cell and slot
+    key = P.key_base + morton3(cell_of(o.x, P.lo[0], P.inv_cell[0], P.ncell[0]),
+                               cell_of(o.y, P.lo[1], P.inv_cell[1], P.ncell[1]),
+                               cell_of(o.z, P.lo[2], P.inv_cell[2], P.ncell[2]));
+    if (dead) atomicOr(&a.list_flags[0], 1u);  // kLfDeaths: the next step builds in full
+    if (keep && !dead) {
+      const float dx = x.x - o.x, dy = x.y - o.y, dz = x.z - o.z;
+      if (sqrtf(dx * dx + dy * dy + dz * dz) * P.inv_skin > 0.5f) atomicOr(&a.list_flags[2], 1u);  // kLfErr
+    }
+  } else if (!dead) {
     const int cx = cell_of(x.x, P.lo[0], P.inv_cell[0], P.ncell[0]);
     const int cy = cell_of(x.y, P.lo[1], P.inv_cell[1], P.ncell[1]);
     const int cz = cell_of(x.z, P.lo[2], P.inv_cell[2], P.ncell[2]);
@@ -299,7 +320,17 @@ __global__ void k_permute(StepArgs a) {
   if (p == 0 || kprev == kDeadKey || (int)(a.main.flags[a.vals_out[p - 1]] & kInstMask) != inst)
     a.dyn[inst].range_lo = p;
   if (knext == kDeadKey || (int)(a.main.flags[a.vals_out[p + 1]] & kInstMask) != inst) a.dyn[inst].range_hi = p + 1;
-  if (a.x0) a.x0[p] = make_float4(x.x, x.y, x.z, 0.f);  // list build: positions the lists refer to
+  // list build: the positions the lists refer to (kept by an instance that
+  // keeps its lists in a partial build)
+  const bool keep = a.inst_keep && a.list_flags[9] != 0u && a.inst_keep[inst];  // kLfPartial
+  if (a.x0 && !keep) a.x0[p] = make_float4(x.x, x.y, x.z, 0.f);
+  if (f & kDeadBit) {  // removed during a partial build: in place until the next full build, far from all
+    a.jr[p].a = make_float4(1.0e30f, 1.0e30f, 1.0e30f, 0.f);
+    a.jr[p].b = make_float4(0.f, 0.f, 0.f, 1.f);
+    a.jC[p] = 0.f;
+    if (a.jh) write_h16_dead(a.jh, p);
+    return;
+  }
   float pres, snds;
   tait(P, x.w, pres, snds);
   const float po = pres / (x.w * x.w);
@@ -367,6 +398,9 @@ __global__ void k_density_plain(StepArgs a) {
   const InstParams& P = a.params[inst];
   const int kind = density_kind(a, P, a.dyn[inst], a.phase[inst]);
   if (!kind) return;
+  // an instance that keeps its lists in a partial build: its cells are those
+  // of its build positions, so its density pass reads the lists (k_density_list)
+  if (a.inst_keep && a.list_flags[9] != 0u && a.inst_keep[inst]) return;
   const float4 I = a.jr[p].a;
   const float rho_i = a.jr[p].b.w;
   float sum = 0.5f, one = 0.5f / rho_i;  // self term: w(0) = 1/2

@@ -32,16 +32,16 @@ constexpr int kListMaxEntries = 192;  // entries per list (the solver's list_max
 
 // Words of StepArgs::list_flags.
 enum ListFlag {
-  kLfReserved0 = 0,
-  kLfReserved1 = 1,
+  kLfDeaths = 0,           // a particle was removed since the last full build: the next step builds in full
+  kLfPartials = 1,         // partial builds so far (counted in kLfBuilds too)
   kLfErr = 2,              // sticky errors: bit 0 a displacement passed skin / 2 on a list step
   kLfLongest = 3,          // largest list built
   kLfOverflowPending = 4,  // the last build overflowed a list: the next step builds
   kLfBuilds = 5,           // builds so far
   kLfListSteps = 6,        // list steps so far
   kLfOverflows = 7,        // builds whose lists overflowed
-  kLfSince = 8,            // steps since the last build (the build counts 1)
-  kLfUnused9 = 9,
+  kLfSince = 8,            // steps since the last full build (the build counts 1)
+  kLfPartial = 9,          // this step's build is partial: instances with inst_keep set keep their lists
   kLfForce = 10,           // the host asks for a build (lists stale)
   kLfDecision = 11,        // this step builds (1) or reads the lists (0)
   kLfWords = 16
@@ -76,40 +76,62 @@ __device__ __forceinline__ float velocity_quantum(float vb, float c0) {
 
 // One thread, after k_step_begin: the step's build decision, the counters,
 // and (in a graph) the condition of the node that selects the build or the
-// list-step branch.  An instance needs a build when the largest displacement
-// its particles can reach in this step, d + dt s + dt^2/2 acc from the motion
-// the last list pass recorded, reaches kListRebuildAt skins.  With compact
+// list-step branch.  An instance needs new lists when the largest
+// displacement its particles can reach in this step, d + dt s + dt^2/2 acc
+// from the motion the last list pass recorded, reaches kListRebuildAt skins.
+// The build is full (every instance, removed particles compacted) when the
+// host asks for it, the last build overflowed, list_interval steps have
+// passed since the last full build, a particle was removed since, or every
+// instance needs new lists; otherwise it is partial: the instances that do
+// not need new lists keep them (inst_keep), their particles keep their cells
+// and slots, and the step re-sorts and scans the others.  With compact
 // records the same motion bounds this step's velocities, s + dt acc, which
 // sets the instance's velocity quantum (kept when there is no motion yet).
 __global__ void k_list_set(StepArgs a, int interval, cudaGraphConditionalHandle cond, int use_cond) {
   unsigned* lf = a.list_flags;
-  bool moved = false;
+  int need = 0, live = 0;
   for (int k = 0; k < a.n_inst; ++k) {
     const InstParams& P = a.params[k];
     const float dt = a.dyn[k].dt_cur;
     unsigned* w = a.inst_motion + 3 * k;
+    bool moved = false;
     if (P.active && P.inv_skin > 0.0f && a.phase[k] == PH_STEP && dt > 0.0f) {
       const float reach = __uint_as_float(w[0]) + dt * __uint_as_float(w[1]) + 0.5f * dt * dt * __uint_as_float(w[2]);
-      moved |= reach >= kListRebuildAt;
+      moved = reach >= kListRebuildAt;
       if (a.jh && (w[1] | w[2])) {
         const float vb = (__uint_as_float(w[1]) + dt * __uint_as_float(w[2])) / P.inv_skin;
         a.dyn[k].vq = velocity_quantum(vb * 1.001f, P.c0);
       }
     }
+    if (P.active) {
+      ++live;
+      need += moved;
+    }
+    a.inst_keep[k] = moved ? 0 : 1;  // read only in a partial build
     w[0] = w[1] = w[2] = 0u;  // refilled by this step's list pass
   }
   const bool overflowed = lf[kLfOverflowPending] != 0u;
-  const bool build = lf[kLfForce] != 0u || overflowed || (int)lf[kLfSince] >= interval || moved;
+  const bool full = lf[kLfForce] != 0u || overflowed || (int)lf[kLfSince] >= interval || lf[kLfDeaths] != 0u ||
+                    (need > 0 && need == live);
+  const bool build = full || need > 0;
   if (overflowed) ++lf[kLfOverflows];
   if (build) {
     ++lf[kLfBuilds];
-    lf[kLfSince] = 1u;
     lf[kLfForce] = 0u;
     lf[kLfOverflowPending] = 0u;
   } else {
     ++lf[kLfListSteps];
+  }
+  if (full) {
+    lf[kLfSince] = 1u;
+    lf[kLfDeaths] = 0u;
+  } else {
     ++lf[kLfSince];
   }
+  if (build && !full) ++lf[kLfPartials];
+  if (!build || full)
+    for (int k = 0; k < a.n_inst; ++k) a.inst_keep[k] = 0;  // only a partial build keeps lists
+  lf[kLfPartial] = (build && !full) ? 1u : 0u;
   lf[kLfDecision] = build ? 1u : 0u;
   if (use_cond) cudaGraphSetConditional(cond, build ? 1u : 0u);
 }
@@ -136,7 +158,10 @@ __global__ void k_kick_refresh(StepArgs a, cudaGraphConditionalHandle dens_cond,
     a.main.vel[p] = v;
   }
   a.main.vh[p] = vh;
-  if (dead && !(f & kDeadBit)) a.main.flags[p] = f | kDeadBit;
+  if (dead && !(f & kDeadBit)) {
+    a.main.flags[p] = f | kDeadBit;
+    atomicOr(&a.list_flags[kLfDeaths], 1u);  // the next build compacts it: in full
+  }
   if (!dead) {
     float pres, snds;
     tait(P, x.w, pres, snds);
@@ -202,6 +227,7 @@ __global__ void __launch_bounds__(128) k_density_list(StepArgs a) {
   if (p >= *a.n_alive) return;
   const uint32_t fp = a.alt.flags[p];
   const int inst = fp & kInstMask;
+  if (a.density_keep_only && !a.inst_keep[inst]) return;  // a partial build: the others searched
   const InstParams& P = a.params[inst];
   const int kind = density_kind(a, P, a.dyn[inst], a.phase[inst]);
   if (!kind) return;

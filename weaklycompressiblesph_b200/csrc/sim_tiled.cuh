@@ -278,6 +278,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
     const int s = a.cell_start[lin], e = a.cell_end[lin];
     const uint32_t f0 = a.alt.flags[s];
     const int inst = f0 & kInstMask;
+    if (LB && a.inst_keep && a.list_flags[9] != 0u && a.inst_keep[inst]) continue;  // keeps its lists
     const InstParams& P = a.params[inst];
     const int ph = a.phase[inst];
     if (!wants_force(P, a.dyn[inst], ph)) {

@@ -222,6 +222,14 @@ class Solver:
         return dict(builds=int(out[0]), list_steps=int(out[1]), overflows=int(out[2]), longest=int(out[3]),
                     kernels_build=int(out[4]), kernels_list=int(out[5]))
 
+    def list_schedule(self):
+        """Builds, partial builds among them, list steps, steps since the last
+        full build (wcsph_sim_list_schedule)."""
+        out = (C.c_int64 * 4)()
+        N.call("wcsph_sim_list_schedule", self._h, out)
+        return dict(builds=int(out[0]), partial_builds=int(out[1]), list_steps=int(out[2]),
+                    since_full=int(out[3]))
+
     def list_entries(self):
         """Entries of the current neighbour lists (0 without current lists)."""
         v = int(N.lib().wcsph_sim_list_entries(self._h))
