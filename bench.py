@@ -531,8 +531,8 @@ def _list_summary(ls):
     if not ls:
         return None
     steps = ls["builds"] + ls["list_steps"]
-    return {"builds": ls["builds"], "list_steps": ls["list_steps"], "overflows": ls["overflows"],
-            "steps_per_build": steps / max(1, ls["builds"])}
+    return {"builds": ls["builds"], "partial_builds": ls.get("partial_builds"), "list_steps": ls["list_steps"],
+            "overflows": ls["overflows"], "steps_per_build": steps / max(1, ls["builds"])}
 
 
 ARGS = None

@@ -47,6 +47,10 @@ enum ListFlag {
   kLfWords = 16
 };
 constexpr float kListRebuildAt = 0.45f;  // predicted displacement / skin that makes a step build
+// In a build that happens anyway, an instance that has used this much of its
+// skin gets new lists too: instances rebuild together instead of one build
+// (and one sort of every particle) per instance.
+constexpr float kListJoinAt = 0.225f;
 
 // Warp-aggregated maxima of a particle's motion into its instance's words.
 __device__ __forceinline__ void motion_max(unsigned* w, int inst, const Motion& m) {
@@ -94,10 +98,11 @@ __global__ void k_list_set(StepArgs a, int interval, cudaGraphConditionalHandle 
     const InstParams& P = a.params[k];
     const float dt = a.dyn[k].dt_cur;
     unsigned* w = a.inst_motion + 3 * k;
-    bool moved = false;
+    bool moved = false, near = false;
     if (P.active && P.inv_skin > 0.0f && a.phase[k] == PH_STEP && dt > 0.0f) {
       const float reach = __uint_as_float(w[0]) + dt * __uint_as_float(w[1]) + 0.5f * dt * dt * __uint_as_float(w[2]);
       moved = reach >= kListRebuildAt;
+      near = reach >= kListJoinAt;
       if (a.jh && (w[1] | w[2])) {
         const float vb = (__uint_as_float(w[1]) + dt * __uint_as_float(w[2])) / P.inv_skin;
         a.dyn[k].vq = velocity_quantum(vb * 1.001f, P.c0);
@@ -107,7 +112,7 @@ __global__ void k_list_set(StepArgs a, int interval, cudaGraphConditionalHandle 
       ++live;
       need += moved;
     }
-    a.inst_keep[k] = moved ? 0 : 1;  // read only in a partial build
+    a.inst_keep[k] = moved ? 0 : (near ? 2 : 1);  // read only in a partial build (2: joins one)
     w[0] = w[1] = w[2] = 0u;  // refilled by this step's list pass
   }
   const bool overflowed = lf[kLfOverflowPending] != 0u;
@@ -129,8 +134,8 @@ __global__ void k_list_set(StepArgs a, int interval, cudaGraphConditionalHandle 
     ++lf[kLfSince];
   }
   if (build && !full) ++lf[kLfPartials];
-  if (!build || full)
-    for (int k = 0; k < a.n_inst; ++k) a.inst_keep[k] = 0;  // only a partial build keeps lists
+  for (int k = 0; k < a.n_inst; ++k)  // only a partial build keeps lists, and the instances near the bound join it
+    a.inst_keep[k] = (!build || full || a.inst_keep[k] == 2) ? 0 : a.inst_keep[k];
   lf[kLfPartial] = (build && !full) ? 1u : 0u;
   lf[kLfDecision] = build ? 1u : 0u;
   if (use_cond) cudaGraphSetConditional(cond, build ? 1u : 0u);

@@ -35,7 +35,7 @@ def run_batched(cases, steps, precision="tiled", warmup=3, device=0, list_interv
         el = _sync_time(s, lambda: s.step(steps))
         st = [s.status(k) for k in slots]
         states = [s.read(k) for k in slots] if read else None
-        lists = s.list_stats() if list_interval else None
+        lists = dict(s.list_stats(), **s.list_schedule()) if list_interval else None
         tuning = s.tuning()
     return dict(seconds=el, steps=steps, particles=total, particle_steps_per_s=total * steps / el,
                 status=st, states=states, lists=lists, tuning=tuning)

@@ -109,7 +109,7 @@ class Server:
         return dict(records=[done[k] for k in sorted(done)], wall_s=wall, particle_steps=particle_steps,
                     particle_steps_per_s=particle_steps / wall if wall > 0 else 0.0,
                     p50_s=float(np.percentile(lat, 50)), p99_s=float(np.percentile(lat, 99)),
-                    lists=s.list_stats() if s.opt.list_interval else None)
+                    lists=dict(s.list_stats(), **s.list_schedule()) if s.opt.list_interval else None)
 
 
 def run_alone(case, precision=N.PREC_TILED, chunk_steps=25, device=0, list_interval=0):
