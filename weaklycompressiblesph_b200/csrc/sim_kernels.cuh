@@ -83,6 +83,23 @@ __device__ __forceinline__ void write_h16_dead(uint4* jh, int p) {
   jh[p] = make_uint4(0x80008000u, 0x80008000u, 0x80008000u, kFarRho);
 }
 
+// Words of StepArgs::list_flags.
+enum ListFlag {
+  kLfDeaths = 0,           // a particle was removed since the last full build: the next step builds in full
+  kLfPartials = 1,         // partial builds so far (counted in kLfBuilds too)
+  kLfErr = 2,              // sticky errors: bit 0 a displacement passed skin / 2 on a list step
+  kLfLongest = 3,          // largest list built
+  kLfOverflowPending = 4,  // the last build overflowed a list: the next step builds
+  kLfBuilds = 5,           // builds so far
+  kLfListSteps = 6,        // list steps so far
+  kLfOverflows = 7,        // builds whose lists overflowed
+  kLfSince = 8,            // steps since the last full build (the build counts 1)
+  kLfPartial = 9,          // this step's build is partial: instances with inst_keep set keep their lists
+  kLfForce = 10,           // the host asks for a build (lists stale)
+  kLfDecision = 11,        // this step builds (1) or reads the lists (0)
+  kLfWords = 16
+};
+
 struct SimArrays {
   float4 *pos, *vel, *vh, *acc;  // one buffer set
   int* pid;
@@ -114,8 +131,8 @@ struct StepArgs {
   int* list_cnt;          // entries per slot
   int list_max;
   float4* x0;             // build steps: record the positions the lists were built at
-  unsigned* list_flags;   // kLf* words (sim_list.cuh): displacement and drift maxima, sticky errors,
-                          // largest list, the device's rebuild decision and its counters
+  unsigned* list_flags;   // ListFlag words: sticky errors, largest list, the device's build
+                          // decision (full or partial) and the schedule's counters
   int list_reuse;         // this step reads the lists: periodic wrapping waits for the next build
   int* dens_any;          // set by k_step_begin when any instance has a density pass in this launch
   unsigned* inst_motion;  // neighbour lists: per instance, the largest |x - x0|, |v| and |a| over its moving
@@ -244,7 +261,7 @@ __global__ void k_kick_bin(StepArgs a) {
   const InstParams& P = a.params[inst];
   const bool was_dead = (f & kDeadBit) || !P.active;
   bool dead = was_dead;
-  const bool partial = a.inst_keep && a.list_flags[9] != 0u;  // kLfPartial
+  const bool partial = a.inst_keep && a.list_flags[kLfPartial] != 0u;
   const bool keep = partial && a.inst_keep[inst];
   float4 x = a.main.pos[p];
   float4 v = a.main.vel[p];
@@ -267,10 +284,10 @@ __global__ void k_kick_bin(StepArgs a) {
     key = P.key_base + morton3(cell_of(o.x, P.lo[0], P.inv_cell[0], P.ncell[0]),
                                cell_of(o.y, P.lo[1], P.inv_cell[1], P.ncell[1]),
                                cell_of(o.z, P.lo[2], P.inv_cell[2], P.ncell[2]));
-    if (dead) atomicOr(&a.list_flags[0], 1u);  // kLfDeaths: the next step builds in full
+    if (dead) atomicOr(&a.list_flags[kLfDeaths], 1u);  // the next step builds in full
     if (keep && !dead) {
       const float dx = x.x - o.x, dy = x.y - o.y, dz = x.z - o.z;
-      if (sqrtf(dx * dx + dy * dy + dz * dz) * P.inv_skin > 0.5f) atomicOr(&a.list_flags[2], 1u);  // kLfErr
+      if (sqrtf(dx * dx + dy * dy + dz * dz) * P.inv_skin > 0.5f) atomicOr(&a.list_flags[kLfErr], 1u);
     }
   } else if (!dead) {
     const int cx = cell_of(x.x, P.lo[0], P.inv_cell[0], P.ncell[0]);
@@ -322,7 +339,7 @@ __global__ void k_permute(StepArgs a) {
   if (knext == kDeadKey || (int)(a.main.flags[a.vals_out[p + 1]] & kInstMask) != inst) a.dyn[inst].range_hi = p + 1;
   // list build: the positions the lists refer to (kept by an instance that
   // keeps its lists in a partial build)
-  const bool keep = a.inst_keep && a.list_flags[9] != 0u && a.inst_keep[inst];  // kLfPartial
+  const bool keep = a.inst_keep && a.list_flags[kLfPartial] != 0u && a.inst_keep[inst];
   if (a.x0 && !keep) a.x0[p] = make_float4(x.x, x.y, x.z, 0.f);
   if (f & kDeadBit) {  // removed during a partial build: in place until the next full build, far from all
     a.jr[p].a = make_float4(1.0e30f, 1.0e30f, 1.0e30f, 0.f);
@@ -400,7 +417,7 @@ __global__ void k_density_plain(StepArgs a) {
   if (!kind) return;
   // an instance that keeps its lists in a partial build: its cells are those
   // of its build positions, so its density pass reads the lists (k_density_list)
-  if (a.inst_keep && a.list_flags[9] != 0u && a.inst_keep[inst]) return;
+  if (a.inst_keep && a.list_flags[kLfPartial] != 0u && a.inst_keep[inst]) return;
   const float4 I = a.jr[p].a;
   const float rho_i = a.jr[p].b.w;
   float sum = 0.5f, one = 0.5f / rho_i;  // self term: w(0) = 1/2

@@ -30,22 +30,6 @@ namespace wcsph {
 
 constexpr int kListMaxEntries = 192;  // entries per list (the solver's list_max; the dam break needs up to ~140)
 
-// Words of StepArgs::list_flags.
-enum ListFlag {
-  kLfDeaths = 0,           // a particle was removed since the last full build: the next step builds in full
-  kLfPartials = 1,         // partial builds so far (counted in kLfBuilds too)
-  kLfErr = 2,              // sticky errors: bit 0 a displacement passed skin / 2 on a list step
-  kLfLongest = 3,          // largest list built
-  kLfOverflowPending = 4,  // the last build overflowed a list: the next step builds
-  kLfBuilds = 5,           // builds so far
-  kLfListSteps = 6,        // list steps so far
-  kLfOverflows = 7,        // builds whose lists overflowed
-  kLfSince = 8,            // steps since the last full build (the build counts 1)
-  kLfPartial = 9,          // this step's build is partial: instances with inst_keep set keep their lists
-  kLfForce = 10,           // the host asks for a build (lists stale)
-  kLfDecision = 11,        // this step builds (1) or reads the lists (0)
-  kLfWords = 16
-};
 constexpr float kListRebuildAt = 0.45f;  // predicted displacement / skin that makes a step build
 // In a build that happens anyway, an instance that has used this much of its
 // skin gets new lists too: instances rebuild together instead of one build

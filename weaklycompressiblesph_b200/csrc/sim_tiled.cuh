@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
     const int s = a.cell_start[lin], e = a.cell_end[lin];
     const uint32_t f0 = a.alt.flags[s];
     const int inst = f0 & kInstMask;
-    if (LB && a.inst_keep && a.list_flags[9] != 0u && a.inst_keep[inst]) continue;  // keeps its lists
+    if (LB && a.inst_keep && a.list_flags[kLfPartial] != 0u && a.inst_keep[inst]) continue;  // keeps its lists
     const InstParams& P = a.params[inst];
     const int ph = a.phase[inst];
     if (!wants_force(P, a.dyn[inst], ph)) {
@@ -423,10 +423,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
       if (LB) {
         if (lane < nbat) {
           a.list_cnt[ib + lane] = lcount;
-          if (lcount > a.list_max) a.list_flags[4] = 1u;  // kLfOverflowPending: the next step rebuilds
+          if (lcount > a.list_max) a.list_flags[kLfOverflowPending] = 1u;  // the next step rebuilds
         }
         const int mx = __reduce_max_sync(full, lane < nbat ? lcount : 0);
-        if (lane == 0) atomicMax(&a.list_flags[3], (unsigned)mx);  // kLfLongest
+        if (lane == 0) atomicMax(&a.list_flags[kLfLongest], (unsigned)mx);
       }
       if (!LB && lane < nbat) {
         const int p = ib + lane;
