@@ -413,7 +413,7 @@ def cpu_reference(case, walks, epi, epj, seconds, pairs_total, whole_budget_s=No
     workload on all host threads.  Whole passes over every walk when one fits
     in whole_budget_s (default: seconds), else repeated passes over a bounded
     sample of the walks (every k-th walk).  Returns (pairs/s, description,
-    cores, seconds of one whole pass or None)."""
+    cores, seconds of one whole pass: measured, or from the sample's rate)."""
     import oracle
     if not oracle.ref_available():
         raise RuntimeError("oracle/_ref/libwcsph_ref.so missing")
@@ -459,7 +459,7 @@ def cpu_reference(case, walks, epi, epj, seconds, pairs_total, whole_budget_s=No
     el = (time.perf_counter() - t0) / reps
     desc = (f"{len(sel)} of {n_walk} FDPS-style walks (every {stride}th, <=128 i each), {pairs} true pairs, "
             f"{reps} repetitions, STD::CalcHydroForce -O3 -ffast-math OpenMP {consts}")
-    return pairs / el, desc, cores, None
+    return pairs / el, desc, cores, tot * el / max(pairs, 1)
 
 
 def measure_ensemble(device, steps=None):
@@ -803,14 +803,17 @@ def main_reference(args):
     # each step one whole pass over every walk when the whole run stays within
     # about four minutes, else a bounded sample of the walks
     per_step = max(1.0, min(10.0, 240.0 / max(1, args.steps + args.warmup)))
-    vals = []
+    vals, secs = [], []
     for k in range(args.warmup + args.steps):
-        v, desc, cores, _ = cpu_reference(case, w, epi, epj, per_step, None, whole_budget_s=per_step)
+        v, desc, cores, whole_s = cpu_reference(case, w, epi, epj, per_step, None, whole_budget_s=per_step)
         if k >= args.warmup:
             vals.append(v)
+            secs.append(whole_s)
     value = statistics.median(vals)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": 1e3 * statistics.median(secs),
+            "ms_per_step_note": "one hydro pass of the functor over every walk of the workload (no tree, EoS or KDK)",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice IC, no dataset)",
             "config": bench_config(args, case, args.precision if args.precision != "best" else best_precision(),
                                    int(os.environ.get("WORLD_SIZE", "1"))),
