@@ -388,3 +388,35 @@ def test_removal_during_partial_builds(native):
     assert rel_l2(got[0]["pos"][alive], ref[0]["pos"][alive]) < 1e-6
     assert rel_l2(got[0]["vel"][alive], ref[0]["vel"][alive]) < 1e-4
     assert periodic_rel(got[1]["pos"], ref[1]["pos"], fast) < 1e-6
+
+
+def test_list_build_reaches_the_list_radius(native, oracle_lib):
+    """A pair whose separation along one axis lies between 2h and the list
+    radius 2h + skin must be in the lists: two particles 2.2h apart along x,
+    placed so that they fall in cells two apart when cells are only 2h wide,
+    close in head-on without a rebuild and must be summed once within 2h."""
+    phys = cases.Physics(g=0.0, density_mode=N.DENSITY_CONTINUITY)
+    dx = 0.01
+    h = phys.h_over_dx * dx
+    lo, hi = (0.0, 0.0, 0.0), (0.2605, 0.1, 0.1)  # 10 cells of 2.0038 h along x when cells are 2h
+    x1 = 0.95 * 0.02605
+    pos = np.array([[x1, 0.05, 0.05], [x1 + 2.2 * h, 0.05, 0.05]])
+    vel = np.array([[0.5, 0.0, 0.0], [-0.5, 0.0, 0.0]])
+    case = cases.Case(name="pair", pos=pos, vel=vel, dens=np.full(2, phys.rho0), type=np.zeros(2, np.int32),
+                      dx=dx, h=h, mass=phys.rho0 * dx ** 3, phys=phys, lo=lo, hi=hi)
+    cfg = oracle_lib.config_from_case(case)
+    with Solver(64, precision=N.PREC_TILED, list_interval=1000) as s:
+        k = s.add(case)
+        met = False
+        for _ in range(40):
+            s.step(1)
+            st = s.read(k)
+            cnt, _ = oracle_lib.neighbors(oracle_lib.pos4(st["pos"].astype(np.float32)), cfg)
+            if cnt.sum() == 2:
+                met = True
+                break
+        sched = s.list_schedule()
+        pr = s.probe(k, lists=True)
+    assert met, "the particles never came within 2h"
+    assert sched["builds"] == 1, sched  # the lists of the first step were read throughout
+    np.testing.assert_array_equal(pr["nbr"], cnt)

@@ -491,7 +491,10 @@ static int set_all_phases(SimImpl& S, int active_phase) {
   return 0;
 }
 
-static int fill_params(const wcsph_instance_desc& d, HostInst& I, InstParams& P) {
+// H_cell: the smallest cell edge, the largest radius any neighbour scan of
+// the instance uses (2h; the list radius 2h + skin with neighbour lists), so
+// that the 27 cells around a particle's cell hold every particle within it.
+static int fill_params(const wcsph_instance_desc& d, float H_cell, HostInst& I, InstParams& P) {
   if (d.n <= 0 || !(d.h > 0) || !(d.mass > 0) || !(d.rho0 > 0) || !(d.gamma > 0) || !(d.c0 > 0) || d.nu < 0) {
     set_error("instance: n, h, mass, rho0, gamma, c0 must be positive and nu >= 0");
     return WCSPH_E_INVALID;
@@ -505,17 +508,19 @@ static int fill_params(const wcsph_instance_desc& d, HostInst& I, InstParams& P)
     return WCSPH_E_INVALID;
   }
   P = InstParams{};
-  const float H = 2.0f * (float)d.h;
+  const float H = 2.0f * (float)d.h;             // the support radius
+  const float Hc = std::max(H_cell, H);          // the smallest cell edge
   for (int k = 0; k < 3; ++k) {
     const float ext = d.hi[k] - d.lo[k];
     if (!(ext > 0)) {
       set_error("instance: grid bounds must satisfy lo < hi on every axis");
       return WCSPH_E_INVALID;
     }
-    int nc = (int)std::floor(ext / (H * 1.0001f));
+    int nc = (int)std::floor(ext / (Hc * 1.0001f));
     if (nc < 1) nc = 1;
     if (d.periodic && nc < 3) {
-      set_error("instance: periodic box needs at least 3 cells of edge >= 2h per axis (got %d on axis %d)", nc, k);
+      set_error("instance: periodic box needs at least 3 cells of edge >= 2h (2h + skin with neighbour lists) per "
+                "axis (got %d on axis %d)", nc, k);
       return WCSPH_E_INVALID;
     }
     if (nc > 1024) {
@@ -523,8 +528,8 @@ static int fill_params(const wcsph_instance_desc& d, HostInst& I, InstParams& P)
       return WCSPH_E_CAPACITY;
     }
     I.ncell[k] = nc;
-    I.cell[k] = d.periodic ? ext / (float)nc : std::max(ext / (float)nc, H * 1.0001f);
-    if (I.cell[k] < H) I.cell[k] = H * 1.0001f;
+    I.cell[k] = d.periodic ? ext / (float)nc : std::max(ext / (float)nc, Hc * 1.0001f);
+    if (I.cell[k] < Hc) I.cell[k] = Hc * 1.0001f;
     P.lo[k] = d.lo[k];
     P.cell[k] = I.cell[k];
     P.inv_cell[k] = 1.0f / I.cell[k];
@@ -942,7 +947,8 @@ static int append_instance(SimImpl& S, const AppendSpec& A, int32_t* slot) {
     if (sl.has_left) d.lo[0] = std::max(d.lo[0], sl.x_lo - W - sl.margin);
     if (sl.has_right) d.hi[0] = std::min(d.hi[0], sl.x_hi + W + sl.margin);
   }
-  if (int rc = fill_params(d, I, P)) return rc;
+  const float H_cell = 2.0f * (float)d.h + (S.opt.list_interval > 0 ? list_skin(S.opt) * (float)d.h : 0.0f);
+  if (int rc = fill_params(d, H_cell, I, P)) return rc;
   if (A.slab) {
     const wcsph_slab& sl = *A.slab;
     I.slab = true;
