@@ -221,7 +221,9 @@ typedef struct wcsph_sim_options {
                                   so the pairs summed are the same as with a fresh search (the
                                   summation order differs) */
   float list_skin;             /* skin in units of h (0: 0.3) */
-  int32_t reserved_;
+  int32_t list_shape;          /* launch shape of the neighbour-list pass: 0 the autotuner's choice
+                                  (shape 0 without autotune); s + 1 fixes shape s (the shapes of
+                                  wcsph_sim_tuning's out[1]) */
 } wcsph_sim_options;
 
 typedef struct wcsph_sim wcsph_sim;

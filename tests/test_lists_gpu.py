@@ -213,6 +213,28 @@ def test_list_pass_vs_fp64(prec, density_pass, native, oracle_lib):
         assert r["dens"] < 1e-5, r
 
 
+@pytest.mark.parametrize("shape", range(N.LIST_SHAPES))
+@pytest.mark.parametrize("prec", [N.PREC_TILED, N.PREC_HALF2], ids=["tiled", "half2"])
+def test_list_pass_every_shape_vs_fp64(prec, shape, native, oracle_lib):
+    """Every launch shape of the list pass (threads per particle, blocks per
+    SM, lanes on consecutive or alternate entries), fixed instead of chosen
+    by the autotuner: after a build and list steps, the list pass on the
+    state read back against the FP64 oracle, with the oracle's neighbour
+    counts; and the shape is the one the solver reports."""
+    case = small_dam(dx=0.04, seed=31, vel_sigma=0.4)
+    with Solver(case.n, precision=prec, list_interval=50, list_skin=0.6, list_shape=shape) as s:
+        k = s.add(case)
+        s.step(6)
+        st = s.read(k)
+        pr = s.probe(k, density_pass=2, lists=True)
+        assert s.tuning()["list_shape"] == shape
+        assert s.list_stats()["list_steps"] >= 3
+    r = oracle_list_check(oracle_lib, case, st, pr, 2)
+    tol = LIST_TOL[prec]
+    np.testing.assert_array_equal(pr["nbr"], r["cnt"])
+    assert r["acc"] < tol and r["div_v"] < tol and r["dt"] < tol and r["dens"] < 1e-5, r
+
+
 @pytest.mark.parametrize("prec", [N.PREC_TILED, N.PREC_HALF2], ids=["tiled", "half2"])
 def test_list_pass_periodic_vs_fp64(prec, native, oracle_lib):
     """Config-3 mode (periodic box, summation density every step) through the

@@ -21,6 +21,7 @@ PREC_FP32, PREC_TILED, PREC_HALF2 = 0, 1, 2
 DENSITY_CONTINUITY, DENSITY_SUMMATION, DENSITY_SHEPARD = 0, 1, 2
 HYDRO, FREEZE = 0, 1
 FDPS_MAX_TAGS = 4
+LIST_SHAPES = 4  # launch shapes of the neighbour-list pass (wcsph_sim_tuning out[1])
 
 
 class FdpsLayout(C.Structure):
@@ -54,7 +55,7 @@ class SimOptions(C.Structure):
     _fields_ = [("device", C.c_int32), ("precision", C.c_int32), ("max_particles", C.c_int64),
                 ("max_cells", C.c_int64), ("max_instances", C.c_int32), ("use_graph", C.c_int32),
                 ("autotune", C.c_int32), ("list_interval", C.c_int32), ("list_skin", C.c_float),
-                ("reserved_", C.c_int32)]
+                ("list_shape", C.c_int32)]
 
 
 class Slab(C.Structure):

@@ -84,6 +84,7 @@ struct SimImpl {
   int* list_cnt = nullptr;
   float4* x0 = nullptr;
   uint4* jh = nullptr;  // compact j-records of the half2 list pass (write_h16)
+  float* jpo = nullptr;  // P/rho^2 beside them
   int* d_keep = nullptr;  // per instance: keeps its lists in a partial build (k_list_set)
   unsigned* d_lflags = nullptr;       // kLfWords words, see ListFlag
   unsigned* d_motion = nullptr;       // 3 words per instance, see StepArgs::inst_motion
@@ -129,7 +130,7 @@ static bool h16_lists(const wcsph_sim_options& o) { return o.list_interval > 0 &
 
 static int64_t device_bytes(const wcsph_sim_options& o) {
   const int64_t list_bytes =
-      o.list_interval > 0 ? (int64_t)(kListMax * 4 + 4 + 16 + (h16_lists(o) ? 16 : 0)) * o.max_particles : 0;
+      o.list_interval > 0 ? (int64_t)(kListMax * 4 + 4 + 16 + (h16_lists(o) ? 20 : 0)) * o.max_particles : 0;
   return (int64_t)per_particle_bytes() * o.max_particles + list_bytes + 2 * sizeof(int) * o.max_cells +
          (sizeof(InstParams) + sizeof(InstDyn) + sizeof(int)) * (int64_t)o.max_instances + (int64_t)cub_sort_bytes(o.max_particles) +
          (1 << 20);
@@ -211,6 +212,7 @@ static StepArgs make_args(SimImpl& S) {
     a.inst_motion = S.d_motion;
     a.inst_keep = S.d_keep;
     a.jh = S.jh;
+    a.jpo = S.jpo;
   }
   return a;
 }
@@ -455,8 +457,8 @@ static int autotune(SimImpl& S) {
     b.x0 = S.x0;
     b.alt = b.main;
     float best_list = 1e30f;
-    int best_list_shape = 0;
-    for (int v = 0; v < kListShapes; ++v) {
+    int best_list_shape = S.opt.list_shape > 0 ? S.opt.list_shape - 1 : 0;
+    for (int v = 0; v < kListShapes && S.opt.list_shape == 0; ++v) {
       int rc = time_launches(S, 3, [&]() {
         return h16 ? launch_hydro_list<true>(b, n, S.s, v) : launch_hydro_list<false>(b, n, S.s, v);
       }, &ms);
@@ -741,7 +743,8 @@ int64_t wcsph_sim_device_bytes(const wcsph_sim_options* opt) { return opt ? devi
 int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
   if (!opt || !out || opt->max_particles <= 0 || opt->max_particles > INT32_MAX - 1 || opt->max_cells <= 0 ||
       opt->max_cells > INT32_MAX || opt->max_instances <= 0 || opt->max_instances > (int)kInstMask ||
-      opt->precision < 0 || opt->precision > 2 || opt->list_interval < 0 || !(opt->list_skin >= 0.f)) {
+      opt->precision < 0 || opt->precision > 2 || opt->list_interval < 0 || !(opt->list_skin >= 0.f) ||
+      opt->list_shape < 0 || opt->list_shape > kListShapes) {
     set_error("wcsph_sim_create: invalid options");
     return WCSPH_E_INVALID;
   }
@@ -769,6 +772,7 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
   auto* sim = new wcsph_sim();
   SimImpl& S = sim->impl;
   S.opt = *opt;
+  S.list_shape = opt->list_shape > 0 ? opt->list_shape - 1 : 0;
   auto fail = [&](int rc) {
     for (void* p : S.allocs) cudaFree(p);
     if (S.s) cudaStreamDestroy(S.s);
@@ -818,6 +822,7 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
     rc |= alloc(S, (void**)&S.d_keep, (size_t)opt->max_instances * sizeof(int));
     if (h16_lists(*opt)) {
       rc |= alloc(S, (void**)&S.jh, N * sizeof(uint4));
+      rc |= alloc(S, (void**)&S.jpo, N * sizeof(float));
     }
     if (!rc && cudaHostAlloc((void**)&S.h_lflags, kLfWords * sizeof(unsigned), cudaHostAllocDefault) != cudaSuccess)
       rc = 1;

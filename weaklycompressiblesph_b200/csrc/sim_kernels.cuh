@@ -141,6 +141,7 @@ struct StepArgs {
   int density_keep_only;   // a partial build's list density pass: only the instances that keep their lists
   // compact j-records of the half2 list pass (WCSPH_PREC_HALF2 with lists; null otherwise)
   uint4* jh;              // 16-bit cell-relative x, y, z, 16-bit velocity, FP32 rho (write_h16)
+  float* jpo;             // P/rho^2 of every slot beside jh (jr[p].a.w, gathered in 4 bytes)
   int probe_density;      // density pass of a probe launch: 0 none, 1 summation, 2 Shepard
   // diagnostics (probe phase)
   float4* diag_acc;
@@ -346,6 +347,7 @@ __global__ void k_permute(StepArgs a) {
     a.jr[p].b = make_float4(0.f, 0.f, 0.f, 1.f);
     a.jC[p] = 0.f;
     if (a.jh) write_h16_dead(a.jh, p);
+    if (a.jpo) a.jpo[p] = 0.f;
     return;
   }
   float pres, snds;
@@ -355,6 +357,7 @@ __global__ void k_permute(StepArgs a) {
   a.jr[p].b = make_float4(v.x, v.y, v.z, x.w);
   a.jC[p] = snds;
   if (a.jh) write_h16(a.jh, P, a.dyn[inst].vq, p, x, v, x.w, cx, cy, cz);
+  if (a.jpo) a.jpo[p] = po;
 }
 
 // Does the hydro pass run for an instance in the current launch?
@@ -445,6 +448,7 @@ __global__ void k_eos(StepArgs a) {
   tait(P, rho, pres, snds);
   const float po = pres / (rho * rho);
   a.jr[p].a.w = po;
+  if (a.jpo) a.jpo[p] = po;
   a.jr[p].b.w = rho;
   a.jC[p] = snds;
   if (a.jh && a.jh[p].w != kFarRho) a.jh[p].w = __float_as_uint(rho);  // the compact record's density

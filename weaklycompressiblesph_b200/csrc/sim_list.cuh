@@ -158,6 +158,7 @@ __global__ void k_kick_refresh(StepArgs a, cudaGraphConditionalHandle dens_cond,
     a.jr[p].a = make_float4(x.x, x.y, x.z, po);
     a.jr[p].b = make_float4(v.x, v.y, v.z, x.w);
     a.jC[p] = snds;
+    if (a.jpo) a.jpo[p] = po;
     const float4 o = a.x0[p];
     if (a.jh)  // compact record relative to the particle's cell at the build
       write_h16(a.jh, P, a.dyn[inst].vq, p, x, v, x.w, cell_of(o.x, P.lo[0], P.inv_cell[0], P.ncell[0]),
@@ -170,6 +171,7 @@ __global__ void k_kick_refresh(StepArgs a, cudaGraphConditionalHandle dens_cond,
     a.jr[p].b = make_float4(0.f, 0.f, 0.f, 1.f);
     a.jC[p] = 0.f;
     if (a.jh) write_h16_dead(a.jh, p);
+    if (a.jpo) a.jpo[p] = 0.f;
   }
 }
 
@@ -279,32 +281,19 @@ __device__ __forceinline__ f2 snds7_2(f2 RHO, f2 RHO0, f2 IRHO0, f2 C0) {
 
 // i-side operands of the half2 list pass: i's position relative to the
 // centre of its build cell (FP32, exact: the two are within a factor of two),
-// its build cell, the scales -cell / 2^15 that turn the 16-bit offsets into
-// lengths, and the instance's velocity quantum.
+// the scales -cell / 2^15 that turn the 16-bit offsets into lengths, the
+// instance's velocity quantum, the band of squared distances that take the
+// FP32 record, half of (2h)^2, and i's slot (the rare FP32-record entries
+// read i's FP32 position and build cell again instead of holding them).
 struct H16I {
   f2 QX, QY, QZ, SX, SY, SZ, VQ;
-  int c[3];
-  float band;
+  float band, hm;
+  int slot;
 };
 
 // 2^23 + the 16 bits of w selected by s (0x7610 low, 0x7632 high) as a float:
 // byte-permuted under the exponent of 2^23.
 __device__ __forceinline__ float h16_magic(uint32_t w, uint32_t s) { return __uint_as_float(__byte_perm(w, 0x4B000000u, s)); }
-
-// (rho / rho0)^7 - 1 in Horner form and P / rho^2 of the two densities
-// (the Tait pressure of tait(), clamped at 0; rho^-2 by the fast quotient).
-__device__ __forceinline__ f2 po7_2(f2 RHO, f2 RHO0, f2 IRHO0, f2 B) {
-  const f2 D = mul2(sub2(RHO, RHO0), IRHO0);
-  f2 X = add2(D, dup(7.0f));
-  X = fma2(D, X, dup(21.0f));
-  X = fma2(D, X, dup(35.0f));
-  X = fma2(D, X, dup(35.0f));
-  X = fma2(D, X, dup(21.0f));
-  X = fma2(D, X, dup(7.0f));
-  X = mul2(mul2(D, X), B);
-  const f2 R2 = mul2(RHO, RHO);
-  return pk(__fdividef(fmaxf(lo(X), 0.0f), lo(R2)), __fdividef(fmaxf(hi(X), 0.0f), hi(R2)));
-}
 
 // Two list entries (halves a, b) of the half2 list pass, from their 16-byte
 // records Qa, Qb.  The displacement of j from i is rebuilt from the 16-bit
@@ -312,7 +301,8 @@ __device__ __forceinline__ f2 po7_2(f2 RHO, f2 RHO0, f2 IRHO0, f2 B) {
 // offset; the biased offset and o + 1 (shifted to 2^15) are added as integers
 // under the exponent of 2^23, so one packed subtraction turns them into an
 // exact (q_j + o) 2^15.  Velocities come the same way, times the velocity
-// quantum (exact); P/rho^2 and c are recomputed from the FP32 density.  An
+// quantum (exact); P/rho^2 is gathered from its 4-byte array (jpo: the
+// FP32 record's value) and c recomputed from the FP32 density.  An
 // entry takes the FP32 record instead (the displacement exactly as the FP32
 // path and the oracle round it, and j's FP32 velocity and density) when its
 // squared distance lies within the band where the 16-bit positions cannot
@@ -320,7 +310,7 @@ __device__ __forceinline__ f2 po7_2(f2 RHO, f2 RHO0, f2 IRHO0, f2 B) {
 // neighbour counts, are exactly those of the FP32 support test.
 __device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P, const PairC& C, const PairI& I,
                                           const H16I& H, const uint4& Qa, const uint4& Qb, uint32_t ea, uint32_t eb,
-                                          bool qva, bool qvb, bool g7, f2 RHO0, f2 IRHO0, f2 C0, f2 B, f2& AX, f2& AY,
+                                          bool qva, bool qvb, bool g7, f2 RHO0, f2 IRHO0, f2 C0, f2& AX, f2& AY,
                                           f2& AZ, f2& DS, float& vsa, float& vsb, unsigned& na, unsigned& nb) {
   const f2 MAG = dup(8388608.0f + 65536.0f), MAGV = dup(8388608.0f + 32768.0f);
   constexpr uint32_t kLo = 0x7610u, kHi = 0x7632u, kO = 0x18000u;  // o + 1 shifted to bits 15-16
@@ -340,8 +330,10 @@ __device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P
   f2 VZJ = mul2(sub2(pk(h16_magic(Qa.z, kHi), h16_magic(Qb.z, kHi)), MAGV), H.VQ);
   const bool fa = Qa.w == kFarRho, fb = Qb.w == kFarRho;
   float r2a = lo(R2raw), r2b = hi(R2raw);
-  const bool xa = qva && (fa || r2a < H.band || fabsf(r2a - C.H2) < H.band);
-  const bool xb = qvb && (fb || r2b < H.band || fabsf(r2b - C.H2) < H.band);
+  // |(|r^2 - (2h)^2/2|) - (2h)^2/2| < band: r^2 within the band of 0 or of
+  // (2h)^2 (two roundings of at most ulp((2h)^2) / 4, inside the band's margin)
+  const bool xa = qva && (fa || fabsf(fabsf(r2a - H.hm) - H.hm) < H.band);
+  const bool xb = qvb && (fb || fabsf(fabsf(r2b - H.hm) - H.hm) < H.band);
   // a far record's density comes from its FP32 record (exact path); an idle
   // half naming one still needs a finite stand-in (its terms are multiplied
   // by zero, and NaN times zero is NaN)
@@ -352,16 +344,18 @@ __device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P
     float rj[2] = {rja, rjb}, vx[2] = {lo(VXJ), hi(VXJ)}, vy[2] = {lo(VYJ), hi(VYJ)}, vz[2] = {lo(VZJ), hi(VZJ)};
     const bool ex[2] = {xa, xb};
     const uint32_t e[2] = {ea, eb};
+    const float4 Xi = __ldg(&a.jr[H.slot].a);
+    int c[3] = {0, 0, 0};
+    if (P.periodic) build_cell(a, P, H.slot, c);
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       if (!ex[h]) continue;
       const JRec R = ld_jrec(&a.jr[e[h] & kH16SlotMask]);
       float sx = 0.f, sy = 0.f, sz = 0.f;
-      if (P.periodic) offset_shift(P, H.c, e[h], sx, sy, sz);
-      const float ix = h ? hi(I.X) : lo(I.X), iy = h ? hi(I.Y) : lo(I.Y), iz = h ? hi(I.Z) : lo(I.Z);
-      dx[h] = __fsub_rn(ix, __fadd_rn(R.a.x, sx));
-      dy[h] = __fsub_rn(iy, __fadd_rn(R.a.y, sy));
-      dz[h] = __fsub_rn(iz, __fadd_rn(R.a.z, sz));
+      if (P.periodic) offset_shift(P, c, e[h], sx, sy, sz);
+      dx[h] = __fsub_rn(Xi.x, __fadd_rn(R.a.x, sx));
+      dy[h] = __fsub_rn(Xi.y, __fadd_rn(R.a.y, sy));
+      dz[h] = __fsub_rn(Xi.z, __fadd_rn(R.a.z, sz));
       r2[h] = dist2(dx[h], dy[h], dz[h]);
       rj[h] = R.b.w;
       vx[h] = R.b.x, vy[h] = R.b.y, vz[h] = R.b.z;
@@ -376,15 +370,9 @@ __device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P
   const bool vb = qvb && r2b > 0.0f && r2b < C.H2;
   na += va, nb += vb;
   const f2 RHOJ = pk(rja, rjb);
-  f2 CJ, POJ;
-  if (g7) {
-    CJ = snds7_2(RHOJ, RHO0, IRHO0, C0);
-    POJ = po7_2(RHOJ, RHO0, IRHO0, B);
-  } else {
-    const uint32_t ga = ea & kH16SlotMask, gb = eb & kH16SlotMask;
-    CJ = pk(__ldg(&a.jC[ga]), __ldg(&a.jC[gb]));
-    POJ = pk(__ldg(&a.jr[ga].a.w), __ldg(&a.jr[gb].a.w));
-  }
+  const uint32_t ga = ea & kH16SlotMask, gb = eb & kH16SlotMask;
+  const f2 POJ = pk(__ldg(&a.jpo[ga]), __ldg(&a.jpo[gb]));  // P/rho^2 as the FP32 records hold it
+  const f2 CJ = g7 ? snds7_2(RHOJ, RHO0, IRHO0, C0) : pk(__ldg(&a.jC[ga]), __ldg(&a.jC[gb]));
   pair_terms2(C, I, DX, DY, DZ, R2raw, va, vb, VXJ, VYJ, VZJ, POJ, RHOJ, CJ, AX, AY, AZ, DS, vsa, vsb);
 }
 
@@ -400,8 +388,8 @@ __device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P
 // bound's blocks per SM (it sets the register budget).  With TPI = 1 every
 // sum runs in list order; TPI = 2 changes the summation order (the results
 // agree to FP32 rounding).
-template <bool H16, int TPI, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_hydro_list(StepArgs a) {
+template <bool H16, int TPI>
+__device__ __forceinline__ void hydro_list_body(const StepArgs& a) {
   const unsigned full = 0xffffffffu;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int p = t / TPI, sub = t % TPI;
@@ -452,14 +440,16 @@ __global__ void __launch_bounds__(128, MINB) k_hydro_list(StepArgs a) {
       }
       if (H16) {  // compact records
         H16I H;
-        build_cell(a, P, p, H.c);
-        H.QX = dup(R.a.x - cell_centre(P, 0, H.c[0]));
-        H.QY = dup(R.a.y - cell_centre(P, 1, H.c[1]));
-        H.QZ = dup(R.a.z - cell_centre(P, 2, H.c[2]));
+        int bc[3];
+        build_cell(a, P, p, bc);
+        H.QX = dup(R.a.x - cell_centre(P, 0, bc[0]));
+        H.QY = dup(R.a.y - cell_centre(P, 1, bc[1]));
+        H.QZ = dup(R.a.z - cell_centre(P, 2, bc[2]));
         H.SX = dup(-P.cell[0] / kQ16Scale), H.SY = dup(-P.cell[1] / kQ16Scale), H.SZ = dup(-P.cell[2] / kQ16Scale);
         H.VQ = dup(a.dyn[inst].vq);
         H.band = P.h16_band;
-        const f2 B = dup(P.B);
+        H.hm = 0.5f * C.H2;
+        H.slot = p;
         const uint32_t hself = (uint32_t)p | (21u << kH16SlotBits);  // offset (0, 0, 0): i's own record
         for (int k = 4 * sub; k < n; k += 4 * TPI) {
           const uint4 e = __ldg(&row[k >> 2]);
@@ -467,10 +457,10 @@ __global__ void __launch_bounds__(128, MINB) k_hydro_list(StepArgs a) {
                          e3 = k + 3 < n ? e.w : hself;
           const uint4 Q0 = __ldg(&a.jh[e0 & kH16SlotMask]), Q1 = __ldg(&a.jh[e1 & kH16SlotMask]);
           const uint4 Q2 = __ldg(&a.jh[e2 & kH16SlotMask]), Q3 = __ldg(&a.jh[e3 & kH16SlotMask]);
-          h16_pair2(a, P, C, I, H, Q0, Q1, e0, e1, true, k + 1 < n, g7, RHO0, IRHO0, C0, B, AX, AY, AZ, DS, vsa,
+          h16_pair2(a, P, C, I, H, Q0, Q1, e0, e1, true, k + 1 < n, g7, RHO0, IRHO0, C0, AX, AY, AZ, DS, vsa, vsb,
+                    ca, cb);
+          h16_pair2(a, P, C, I, H, Q2, Q3, e2, e3, k + 2 < n, k + 3 < n, g7, RHO0, IRHO0, C0, AX, AY, AZ, DS, vsa,
                     vsb, ca, cb);
-          h16_pair2(a, P, C, I, H, Q2, Q3, e2, e3, k + 2 < n, k + 3 < n, g7, RHO0, IRHO0, C0, B, AX, AY, AZ, DS,
-                    vsa, vsb, ca, cb);
         }
       } else {
         for (int k = 4 * sub; k < n; k += 4 * TPI) {
@@ -492,7 +482,7 @@ __global__ void __launch_bounds__(128, MINB) k_hydro_list(StepArgs a) {
                       cb);
         }
       }
-      sx = lo(AX) + hi(AX), sy = lo(AY) + hi(AY), sz = lo(AZ) + hi(AZ), sd = lo(DS) + hi(DS);
+      sx = lo(AX) + hi(AX), sy = lo(AY) + hi(AY), sz = lo(AZ) + hi(AZ), sd = -(lo(DS) + hi(DS));  // DS: -sum g dr.dv
       sv = fmaxf(vsa, vsb);
       scnt = ca + cb;
     }
@@ -518,19 +508,27 @@ __global__ void __launch_bounds__(128, MINB) k_hydro_list(StepArgs a) {
   if ((threadIdx.x & 31) == 0 && tot) atomicAdd(a.pair_count, (unsigned long long)tot);
 }
 
+template <bool H16, int TPI, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_hydro_list(StepArgs a) {
+  hydro_list_body<H16, TPI>(a);
+}
+
 // Launch shapes of the list pass the autotuner chooses among: (threads per
-// particle, blocks per SM of the launch bound).  Shapes 0 and 2 sum in one
-// order (bit-identical results), shapes 1 and 3 in another.
+// particle, blocks of 128 per SM of the launch bound, which sets the register
+// budget: 96 or 128).  Shapes 0 and 2 sum in one order (bit-identical
+// results), shapes 1 and 3 in another.
 constexpr int kListShapes = 4;
 constexpr int kListShapeTPI[kListShapes] = {1, 2, 1, 2};
-constexpr int kListShapeMINB[kListShapes] = {5, 4, 4, 5};
+constexpr int kListShapeBlock[kListShapes] = {128, 128, 128, 128};
 
 template <bool H16>
 inline int launch_hydro_list(const StepArgs& a, int n, cudaStream_t s, int shape = 0) {
   if (n <= 0) return 0;
-  const long long threads = (long long)n * kListShapeTPI[shape < 0 || shape >= kListShapes ? 0 : shape];
-  const int grid = (int)((threads + 127) / 128);
-  switch (shape) {
+  const int sh = shape < 0 || shape >= kListShapes ? 0 : shape;
+  const long long threads = (long long)n * kListShapeTPI[sh];
+  const int B = kListShapeBlock[sh];
+  const int grid = (int)((threads + B - 1) / B);
+  switch (sh) {
     case 1: k_hydro_list<H16, 2, 4><<<grid, 128, 0, s>>>(a); break;
     case 2: k_hydro_list<H16, 1, 4><<<grid, 128, 0, s>>>(a); break;
     case 3: k_hydro_list<H16, 2, 5><<<grid, 128, 0, s>>>(a); break;

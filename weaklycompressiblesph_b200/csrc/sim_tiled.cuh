@@ -105,17 +105,19 @@ __device__ __forceinline__ void entry_shift(const InstParams& P, uint32_t code, 
 struct PairI {
   f2 X, Y, Z, VX, VY, VZ, RHO, PO, CI;
 };
+// The constants carry factors of pair_terms2: 3 Kg (the spline gradient,
+// negated), -4 nu, 2 beta and -alpha (the factor 2 of Pi_ij moved in: exact).
 struct PairC {
   float H2, iH, KgiH;
-  f2 IH, KG, EH2, HH, NU4, BETA, MHALPHA;
+  f2 IH, KG3, EH2, HH, NNU4, BETA2, MALPHA;
   int vs;
   bool per;
 };
 __device__ __forceinline__ PairC pair_consts(const InstParams& P) {
   PairC c;
   c.H2 = P.H2, c.iH = P.inv_H, c.KgiH = P.Kg * P.inv_H;
-  c.IH = dup(P.inv_H), c.KG = dup(P.Kg), c.EH2 = dup(P.eh2), c.HH = dup(P.h), c.NU4 = dup(P.nu4);
-  c.BETA = dup(P.beta), c.MHALPHA = dup(-0.5f * P.alpha);
+  c.IH = dup(P.inv_H), c.KG3 = dup(3.0f * P.Kg), c.EH2 = dup(P.eh2), c.HH = dup(P.h);
+  c.NNU4 = dup(-P.nu4), c.BETA2 = dup(2.0f * P.beta), c.MALPHA = dup(-P.alpha);
   c.vs = P.vsig_mode, c.per = P.periodic;
   return c;
 }
@@ -125,27 +127,31 @@ __device__ __forceinline__ PairC pair_consts(const InstParams& P) {
 // DZ = x_i - x_j with R2raw their squared length, j's velocity VJX..VJZ,
 // P_j/rho_j^2 POJ, density RHOJ and sound speed CJ; va, vb say whether a half
 // holds an in-support pair (idle halves add exactly zero).  Accumulates a_x,
-// a_y, a_z, sum g dr.dv and the v_sig maximum per half.
+// a_y, a_z, MINUS sum g dr.dv (the gradient factor is carried negated) and the
+// v_sig maximum per half.
 __device__ __forceinline__ void pair_terms2(const PairC& C, const PairI& I, f2 DX, f2 DY, f2 DZ, f2 R2raw, bool va,
                                             bool vb, f2 VJX, f2 VJY, f2 VJZ, f2 POJ, f2 RHOJ, f2 CJ, f2& AX, f2& AY,
                                             f2& AZ, f2& DS, float& vsa, float& vsb) {
-  const f2 ONE = dup(1.0f), HALF = dup(0.5f), TWELVE = dup(12.0f), MTHREE = dup(-3.0f), TWO = dup(2.0f);
-  const f2 MONE = dup(-1.0f);
+  const f2 ONE = dup(1.0f), HALF = dup(0.5f);
   const f2 R2 = pk(va ? lo(R2raw) : C.H2, vb ? hi(R2raw) : C.H2);  // finite stand-in for idle halves
   const f2 W = pk(va ? 1.0f : 0.0f, vb ? 1.0f : 0.0f);
-  // gradW = G * dr
+  // gradW = g dr with g = (12 (1/2-s)+^2 - 3 (1-s)^2) Kg / r; NG = -g = 3 Kg ((1-s)^2 - 4 (1/2-s)+^2) / r
   const f2 RINV = rsqrt2(R2);
   const f2 S = mul2(mul2(R2, RINV), C.IH);
-  const f2 A = max0_2(sub2(ONE, S)), B = max0_2(sub2(HALF, S));
-  const f2 F = fma2(TWELVE, mul2(B, B), mul2(MTHREE, mul2(A, A)));  // 12 (1/2-s)+^2 - 3 (1-s)+^2
-  const f2 G = mul2(mul2(F, C.KG), mul2(RINV, W));
+  // 1 - s needs no clamp: s <= 1 in support and for the stand-in up to
+  // rounding, and a rounding residue squared is far below FP32 resolution
+  const f2 A = sub2(ONE, S), B = max0_2(sub2(HALF, S));
+  const f2 NG = mul2(mul2(fma2(dup(-4.0f), mul2(B, B), mul2(A, A)), C.KG3), mul2(RINV, W));
   const f2 DVX = sub2(I.VX, VJX), DVY = sub2(I.VY, VJY), DVZ = sub2(I.VZ, VJZ);
   const f2 DRDV = fma2(DZ, DVZ, fma2(DY, DVY, mul2(DX, DVX)));
   const f2 RDEN = rcp2(add2(R2, C.EH2));
   const f2 MUr = mul2(mul2(DRDV, RDEN), C.HH);
-  const f2 MU = pk(va && lo(DRDV) < 0.0f ? lo(MUr) : 0.0f, vb && hi(DRDV) < 0.0f ? hi(MUr) : 0.0f);
+  // mu = h dr.dv / (r^2 + eps h^2) where dr.dv < 0 (the sign of MUr), 0
+  // otherwise and for idle halves (W = 0; MUr is finite there)
+  const f2 MU = pk(va ? fminf(lo(MUr), 0.0f) : 0.0f, vb ? fminf(hi(MUr), 0.0f) : 0.0f);
   const f2 RS = rcp2(add2(I.RHO, RHOJ));
-  const f2 AV = mul2(mul2(fma2(C.BETA, MU, mul2(C.MHALPHA, add2(I.CI, CJ))), MU), mul2(RS, TWO));
+  // Pi_ij = (beta mu - alpha/2 (c_i + c_j)) mu 2 / (rho_i + rho_j)
+  const f2 AV = mul2(mul2(fma2(C.BETA2, MU, mul2(C.MALPHA, add2(I.CI, CJ))), MU), RS);
   if (C.vs) {
     vsa = fmaxf(vsa, -lo(MU));
     vsb = fmaxf(vsb, -hi(MU));
@@ -153,12 +159,12 @@ __device__ __forceinline__ void pair_terms2(const PairC& C, const PairI& I, f2 D
     vsa = fmaxf(vsa, lo(MU));
     vsb = fmaxf(vsb, hi(MU));
   }
-  const f2 NPG = mul2(mul2(add2(add2(I.PO, POJ), AV), G), MONE);
-  const f2 VISC = mul2(mul2(mul2(C.NU4, G), R2), mul2(RS, RDEN));
+  const f2 NPG = mul2(add2(add2(I.PO, POJ), AV), NG);                  // -(P_i/rho_i^2 + P_j/rho_j^2 + Pi_ij) g
+  const f2 VISC = mul2(mul2(mul2(C.NNU4, NG), R2), mul2(RS, RDEN));  // 4 nu g r^2 / ((rho_i+rho_j)(r^2+eps h^2))
   AX = fma2(NPG, DX, fma2(VISC, DVX, AX));
   AY = fma2(NPG, DY, fma2(VISC, DVY, AY));
   AZ = fma2(NPG, DZ, fma2(VISC, DVZ, AZ));
-  DS = fma2(G, DRDV, DS);
+  DS = fma2(NG, DRDV, DS);
 }
 
 // Pair terms of two (i, j) pairs at once from FP32 j-records Ra, Rb with
@@ -216,7 +222,7 @@ __device__ __forceinline__ void hydro_queues2(const StepArgs& a, const InstParam
     const f2 CJ = pk(__ldg(&a.jC[ga]), __ldg(&a.jC[gb]));
     pair2<false>(P, C, I, Ra, Rb, ea >> 27, eb >> 27, CJ, qva, qvb, AX, AY, AZ, DS, vsa, vsb, ca, cb);
   }
-  const float v8[8] = {lo(AX), lo(AY), lo(AZ), lo(DS), hi(AX), hi(AY), hi(AZ), hi(DS)};
+  const float v8[8] = {lo(AX), lo(AY), lo(AZ), -lo(DS), hi(AX), hi(AY), hi(AZ), -hi(DS)};  // DS holds -sum g dr.dv
   const float y = butterfly8(v8, lane);
   vsa = warp_max(vsa);
   vsb = warp_max(vsb);
