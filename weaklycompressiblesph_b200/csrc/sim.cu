@@ -213,6 +213,7 @@ static StepArgs make_args(SimImpl& S) {
     a.inst_keep = S.d_keep;
     a.jh = S.jh;
     a.jpo = S.jpo;
+    a.list_pad = list_pad_entry((int)S.opt.max_particles, h16_lists(S.opt));
   }
   return a;
 }
@@ -839,6 +840,8 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
       cudaEventCreateWithFlags(&S.step_ev[1], cudaEventDisableTiming) != cudaSuccess)
     return fail(WCSPH_E_CUDA);
   if (S.d_lflags) {
+    k_list_pad_slot<<<1, 1, 0, S.s>>>(S.jr, S.jC, S.jpo, S.jh, (int)opt->max_particles);
+    if (cudaGetLastError() != cudaSuccess) return fail(WCSPH_E_CUDA);
     memset(S.h_lflags, 0, kLfWords * sizeof(unsigned));
     if (cudaMemsetAsync(S.d_lflags, 0, kLfWords * sizeof(unsigned), S.s) != cudaSuccess ||
         cudaMemsetAsync(S.d_motion, 0, 3 * (size_t)opt->max_instances * sizeof(unsigned), S.s) != cudaSuccess ||

@@ -40,9 +40,10 @@ __device__ __forceinline__ JRec ld_jrec(const JRec* p) {
 // fastest particle this step; InstDyn::vq), biased by 2^15.  P/rho^2 and c
 // are recomputed from rho by the pass.  A particle outside either range (far
 // from its build cell, above the grid where cells are clamped, faster than
-// the bound) or removed is marked far (rho = kFarRho, a NaN), and its entries
-// are read from the FP32 record.
-constexpr uint32_t kFarRho = 0xffffffffu;
+// the bound) or removed is marked far (rho = kFarRho, 0: finite in every term
+// it meets before the entry switches to the FP32 record), and its entries are
+// read from the FP32 record.
+constexpr uint32_t kFarRho = 0u;
 constexpr float kQ16Scale = 32768.0f;
 
 __device__ __forceinline__ float cell_centre(const InstParams& P, int k, int c) {
@@ -142,6 +143,8 @@ struct StepArgs {
   // compact j-records of the half2 list pass (WCSPH_PREC_HALF2 with lists; null otherwise)
   uint4* jh;              // 16-bit cell-relative x, y, z, 16-bit velocity, FP32 rho (write_h16)
   float* jpo;             // P/rho^2 of every slot beside jh (jr[p].a.w, gathered in 4 bytes)
+  uint32_t list_pad;      // list entry naming the padding slot (k_list_pad_slot): rows are padded with it
+                          // to whole groups of four entries
   int probe_density;      // density pass of a probe launch: 0 none, 1 summation, 2 Shepard
   // diagnostics (probe phase)
   float4* diag_acc;

@@ -29,6 +29,27 @@
 namespace wcsph {
 
 constexpr int kListMaxEntries = 192;  // entries per list (the solver's list_max; the dam break needs up to ~140)
+static_assert(kListMaxEntries % 4 == 0, "list rows are padded to whole groups of four entries");
+
+// The padding slot (index max_particles, past every particle's slot) that
+// list rows are padded with: records that no support test accepts and that
+// no band or far test sends to the FP32 record.  FP32 position 1e30 (r^2
+// overflows to inf, as for a removed particle), compact position one cell
+// edge into the (+1, +1, +1) neighbour cell of the padding entry's offset
+// (more than 1.4 cell edges from any i on every axis), zero velocity,
+// density 1, P/rho^2 and c 0.
+__global__ void k_list_pad_slot(JRec* jr, float* jC, float* jpo, uint4* jh, int d) {
+  jr[d].a = make_float4(1.0e30f, 1.0e30f, 1.0e30f, 0.f);
+  jr[d].b = make_float4(0.f, 0.f, 0.f, 1.f);
+  jC[d] = 0.f;
+  if (jpo) jpo[d] = 0.f;
+  if (jh) jh[d] = make_uint4(0xffffffffu, 0x8000ffffu, 0x80008000u, __float_as_uint(1.0f));
+}
+// List entries naming the padding slot d: the FP32 list's image code 13 (no
+// shift), or the half2 list's neighbour-cell offset (+1, +1, +1).
+inline uint32_t list_pad_entry(int d, bool h16) {
+  return h16 ? (uint32_t)d | (42u << kH16SlotBits) : (uint32_t)d | (13u << 27);
+}
 
 constexpr float kListRebuildAt = 0.45f;  // predicted displacement / skin that makes a step build
 // In a build that happens anyway, an instance that has used this much of its
@@ -291,6 +312,11 @@ struct H16I {
   int slot;
 };
 
+// Neighbour-cell offsets + 1 of a half2 list entry's 6-bit code (entry >> 26),
+// each shifted to bits 15-16 as h16_pair2 adds them: (x, y, z, 0).  Filled by
+// each block of the half2 list pass.
+__shared__ uint4 s_h16_off[64];
+
 // 2^23 + the 16 bits of w selected by s (0x7610 low, 0x7632 high) as a float:
 // byte-permuted under the exponent of 2^23.
 __device__ __forceinline__ float h16_magic(uint32_t w, uint32_t s) { return __uint_as_float(__byte_perm(w, 0x4B000000u, s)); }
@@ -298,7 +324,7 @@ __device__ __forceinline__ float h16_magic(uint32_t w, uint32_t s) { return __ui
 // Two list entries (halves a, b) of the half2 list pass, from their 16-byte
 // records Qa, Qb.  The displacement of j from i is rebuilt from the 16-bit
 // offsets: x_i - x_j = q_i - (o + q_j) cell, with o the entry's neighbour-cell
-// offset; the biased offset and o + 1 (shifted to 2^15) are added as integers
+// offset; the biased offset and o + 1 (shifted to 2^15, from s_h16_off) are added as integers
 // under the exponent of 2^23, so one packed subtraction turns them into an
 // exact (q_j + o) 2^15.  Velocities come the same way, times the velocity
 // quantum (exact); P/rho^2 is gathered from its 4-byte array (jpo: the
@@ -313,15 +339,16 @@ __device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P
                                           bool qva, bool qvb, bool g7, f2 RHO0, f2 IRHO0, f2 C0, f2& AX, f2& AY,
                                           f2& AZ, f2& DS, float& vsa, float& vsb, unsigned& na, unsigned& nb) {
   const f2 MAG = dup(8388608.0f + 65536.0f), MAGV = dup(8388608.0f + 32768.0f);
-  constexpr uint32_t kLo = 0x7610u, kHi = 0x7632u, kO = 0x18000u;  // o + 1 shifted to bits 15-16
-  const f2 TX = sub2(pk(__uint_as_float(__float_as_uint(h16_magic(Qa.x, kLo)) + ((ea >> (kH16SlotBits - 15)) & kO)),
-                        __uint_as_float(__float_as_uint(h16_magic(Qb.x, kLo)) + ((eb >> (kH16SlotBits - 15)) & kO))),
+  constexpr uint32_t kLo = 0x7610u, kHi = 0x7632u;
+  const uint4 Oa = s_h16_off[ea >> kH16SlotBits], Ob = s_h16_off[eb >> kH16SlotBits];
+  const f2 TX = sub2(pk(__uint_as_float(__float_as_uint(h16_magic(Qa.x, kLo)) + Oa.x),
+                        __uint_as_float(__float_as_uint(h16_magic(Qb.x, kLo)) + Ob.x)),
                      MAG);
-  const f2 TY = sub2(pk(__uint_as_float(__float_as_uint(h16_magic(Qa.x, kHi)) + ((ea >> (kH16SlotBits - 13)) & kO)),
-                        __uint_as_float(__float_as_uint(h16_magic(Qb.x, kHi)) + ((eb >> (kH16SlotBits - 13)) & kO))),
+  const f2 TY = sub2(pk(__uint_as_float(__float_as_uint(h16_magic(Qa.x, kHi)) + Oa.y),
+                        __uint_as_float(__float_as_uint(h16_magic(Qb.x, kHi)) + Ob.y)),
                      MAG);
-  const f2 TZ = sub2(pk(__uint_as_float(__float_as_uint(h16_magic(Qa.y, kLo)) + ((ea >> (kH16SlotBits - 11)) & kO)),
-                        __uint_as_float(__float_as_uint(h16_magic(Qb.y, kLo)) + ((eb >> (kH16SlotBits - 11)) & kO))),
+  const f2 TZ = sub2(pk(__uint_as_float(__float_as_uint(h16_magic(Qa.y, kLo)) + Oa.z),
+                        __uint_as_float(__float_as_uint(h16_magic(Qb.y, kLo)) + Ob.z)),
                      MAG);
   f2 DX = fma2(TX, H.SX, H.QX), DY = fma2(TY, H.SY, H.QY), DZ = fma2(TZ, H.SZ, H.QZ);
   f2 R2raw = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
@@ -334,11 +361,8 @@ __device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P
   // (2h)^2 (two roundings of at most ulp((2h)^2) / 4, inside the band's margin)
   const bool xa = qva && (fa || fabsf(fabsf(r2a - H.hm) - H.hm) < H.band);
   const bool xb = qvb && (fb || fabsf(fabsf(r2b - H.hm) - H.hm) < H.band);
-  // a far record's density comes from its FP32 record (exact path); an idle
-  // half naming one still needs a finite stand-in (its terms are multiplied
-  // by zero, and NaN times zero is NaN)
-  float rja = fa ? P.rho0 : __uint_as_float(Qa.w);
-  float rjb = fb ? P.rho0 : __uint_as_float(Qb.w);
+  // a far record's density (0) is replaced by its FP32 record's (exact path)
+  float rja = __uint_as_float(Qa.w), rjb = __uint_as_float(Qb.w);
   if (xa || xb) {  // rare: the exact FP32 record, as the FP32 path reads it
     float dx[2] = {lo(DX), hi(DX)}, dy[2] = {lo(DY), hi(DY)}, dz[2] = {lo(DZ), hi(DZ)}, r2[2] = {r2a, r2b};
     float rj[2] = {rja, rjb}, vx[2] = {lo(VXJ), hi(VXJ)}, vy[2] = {lo(VYJ), hi(VYJ)}, vz[2] = {lo(VZJ), hi(VZJ)};
@@ -391,6 +415,13 @@ __device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P
 template <bool H16, int TPI>
 __device__ __forceinline__ void hydro_list_body(const StepArgs& a) {
   const unsigned full = 0xffffffffu;
+  if (H16) {  // before any thread leaves: the offset table of the half2 entries
+    if (threadIdx.x < 64) {
+      const uint32_t c = threadIdx.x;
+      s_h16_off[c] = make_uint4((c & 3u) << 15, ((c >> 2) & 3u) << 15, (c >> 4) << 15, 0u);
+    }
+    __syncthreads();
+  }
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int p = t / TPI, sub = t % TPI;
   float dt_cand = 0.f;
@@ -421,7 +452,6 @@ __device__ __forceinline__ void hydro_list_body(const StepArgs& a) {
       const int cnt_build = a.list_cnt[p];
       const int n = cnt_build <= a.list_max ? cnt_build : 0;
       const uint4* row = reinterpret_cast<const uint4*>(a.list + (size_t)p * a.list_max);
-      const uint32_t self = (uint32_t)p | (13u << 27);  // idle halves: i's own record, weight 0
       f2 AX = 0ull, AY = 0ull, AZ = 0ull, DS = 0ull;
       float vsa = 0.f, vsb = 0.f;
       unsigned ca = 0, cb = 0;
@@ -450,19 +480,21 @@ __device__ __forceinline__ void hydro_list_body(const StepArgs& a) {
         H.band = P.h16_band;
         H.hm = 0.5f * C.H2;
         H.slot = p;
-        const uint32_t hself = (uint32_t)p | (21u << kH16SlotBits);  // offset (0, 0, 0): i's own record
+        // entries past n up to the end of the group of four name the padding
+        // slot, which no support, band or far test accepts
         for (int k = 4 * sub; k < n; k += 4 * TPI) {
           const uint4 e = __ldg(&row[k >> 2]);
-          const uint32_t e0 = e.x, e1 = k + 1 < n ? e.y : hself, e2 = k + 2 < n ? e.z : hself,
-                         e3 = k + 3 < n ? e.w : hself;
-          const uint4 Q0 = __ldg(&a.jh[e0 & kH16SlotMask]), Q1 = __ldg(&a.jh[e1 & kH16SlotMask]);
-          const uint4 Q2 = __ldg(&a.jh[e2 & kH16SlotMask]), Q3 = __ldg(&a.jh[e3 & kH16SlotMask]);
-          h16_pair2(a, P, C, I, H, Q0, Q1, e0, e1, true, k + 1 < n, g7, RHO0, IRHO0, C0, AX, AY, AZ, DS, vsa, vsb,
-                    ca, cb);
-          h16_pair2(a, P, C, I, H, Q2, Q3, e2, e3, k + 2 < n, k + 3 < n, g7, RHO0, IRHO0, C0, AX, AY, AZ, DS, vsa,
-                    vsb, ca, cb);
+          const uint4 Q0 = __ldg(&a.jh[e.x & kH16SlotMask]), Q1 = __ldg(&a.jh[e.y & kH16SlotMask]);
+          const uint4 Q2 = __ldg(&a.jh[e.z & kH16SlotMask]), Q3 = __ldg(&a.jh[e.w & kH16SlotMask]);
+          h16_pair2(a, P, C, I, H, Q0, Q1, e.x, e.y, true, true, g7, RHO0, IRHO0, C0, AX, AY, AZ, DS, vsa, vsb, ca,
+                    cb);
+          h16_pair2(a, P, C, I, H, Q2, Q3, e.z, e.w, true, true, g7, RHO0, IRHO0, C0, AX, AY, AZ, DS, vsa, vsb, ca,
+                    cb);
         }
       } else {
+        // idle halves past n read i's own record (weight 0): this loop keeps
+        // its selects, which leave the FP32 pass within 96 registers
+        const uint32_t self = (uint32_t)p | (13u << 27);
         for (int k = 4 * sub; k < n; k += 4 * TPI) {
           const uint4 e = __ldg(&row[k >> 2]);
           const uint32_t e0 = e.x, e1 = k + 1 < n ? e.y : self, e2 = k + 2 < n ? e.z : self,

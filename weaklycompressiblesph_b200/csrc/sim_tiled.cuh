@@ -429,7 +429,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
       if (LB) {
         if (lane < nbat) {
           a.list_cnt[ib + lane] = lcount;
-          if (lcount > a.list_max) a.list_flags[kLfOverflowPending] = 1u;  // the next step rebuilds
+          if (lcount > a.list_max) {
+            a.list_flags[kLfOverflowPending] = 1u;  // the next step rebuilds
+          } else {  // pad the row to a whole group of four (list_max is a multiple of four)
+            uint32_t* row = a.list + (size_t)(ib + lane) * a.list_max;
+            for (int k = lcount; k < ((lcount + 3) & ~3); ++k) row[k] = a.list_pad;
+          }
         }
         const int mx = __reduce_max_sync(full, lane < nbat ? lcount : 0);
         if (lane == 0) atomicMax(&a.list_flags[kLfLongest], (unsigned)mx);
