@@ -361,8 +361,13 @@ int32_t wcsph_sim_kernels_per_step(wcsph_sim* sim);
  * thread per particle, 5 blocks of 128 per SM; 1: two threads per particle,
  * each taking alternate groups of four list entries, 4 blocks per SM; 2: one
  * thread per particle, 4 blocks per SM; 3: two threads per particle, 5 blocks
- * per SM.  Shapes 0 and 2 sum in one order, 1 and 3 in another: results
- * agree to FP32 rounding), out[2] log2 particle bucket it was tuned for (-1:
+ * per SM; 4-6: shape 0 with the half2 pass's neighbour-cell offsets read from
+ * a shared table instead of shifted out of the entry (4), P/rho^2 recomputed
+ * from the density instead of gathered (5), or both (6); in the FP32 pass
+ * shape 0.  Shapes 0,
+ * 2 and 4 sum in one order, 1 and 3 in another; 5 and 6 round P/rho^2
+ * differently: results agree to FP32 rounding), out[2] log2 particle bucket
+ * it was tuned for (-1:
  * defaults, not tuned), out[3] shape of the list build's scan (0-2 as out[0];
  * 3, 4: 4 or 8 warps per block with 256-candidate tiles). */
 int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out4);

@@ -21,7 +21,7 @@ PREC_FP32, PREC_TILED, PREC_HALF2 = 0, 1, 2
 DENSITY_CONTINUITY, DENSITY_SUMMATION, DENSITY_SHEPARD = 0, 1, 2
 HYDRO, FREEZE = 0, 1
 FDPS_MAX_TAGS = 4
-LIST_SHAPES = 4  # launch shapes of the neighbour-list pass (wcsph_sim_tuning out[1])
+LIST_SHAPES = 7  # launch shapes of the neighbour-list pass (wcsph_sim_tuning out[1])
 
 
 class FdpsLayout(C.Structure):

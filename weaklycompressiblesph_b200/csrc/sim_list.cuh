@@ -307,14 +307,30 @@ __device__ __forceinline__ f2 snds7_2(f2 RHO, f2 RHO0, f2 IRHO0, f2 C0) {
 // FP32 record, half of (2h)^2, and i's slot (the rare FP32-record entries
 // read i's FP32 position and build cell again instead of holding them).
 struct H16I {
-  f2 QX, QY, QZ, SX, SY, SZ, VQ;
+  f2 QX, QY, QZ, SX, SY, SZ, VQ, B;
   float band, hm;
   int slot;
 };
 
+// (rho / rho0)^7 - 1 in Horner form and P / rho^2 of the two densities
+// (the Tait pressure of tait(), clamped at 0; rho^-2 by the fast quotient, so
+// within FP32 rounding of the stored value).
+__device__ __forceinline__ f2 po7_2(f2 RHO, f2 RHO0, f2 IRHO0, f2 B) {
+  const f2 D = mul2(sub2(RHO, RHO0), IRHO0);
+  f2 X = add2(D, dup(7.0f));
+  X = fma2(D, X, dup(21.0f));
+  X = fma2(D, X, dup(35.0f));
+  X = fma2(D, X, dup(35.0f));
+  X = fma2(D, X, dup(21.0f));
+  X = fma2(D, X, dup(7.0f));
+  X = mul2(mul2(D, X), B);
+  const f2 R2 = mul2(RHO, RHO);
+  return pk(__fdividef(fmaxf(lo(X), 0.0f), lo(R2)), __fdividef(fmaxf(hi(X), 0.0f), hi(R2)));
+}
+
 // Neighbour-cell offsets + 1 of a half2 list entry's 6-bit code (entry >> 26),
 // each shifted to bits 15-16 as h16_pair2 adds them: (x, y, z, 0).  Filled by
-// each block of the half2 list pass.
+// each block of the half2 list pass's table shapes (OFT).
 __shared__ uint4 s_h16_off[64];
 
 // 2^23 + the 16 bits of w selected by s (0x7610 low, 0x7632 high) as a float:
@@ -324,7 +340,7 @@ __device__ __forceinline__ float h16_magic(uint32_t w, uint32_t s) { return __ui
 // Two list entries (halves a, b) of the half2 list pass, from their 16-byte
 // records Qa, Qb.  The displacement of j from i is rebuilt from the 16-bit
 // offsets: x_i - x_j = q_i - (o + q_j) cell, with o the entry's neighbour-cell
-// offset; the biased offset and o + 1 (shifted to 2^15, from s_h16_off) are added as integers
+// offset; the biased offset and o + 1 (shifted to 2^15) are added as integers
 // under the exponent of 2^23, so one packed subtraction turns them into an
 // exact (q_j + o) 2^15.  Velocities come the same way, times the velocity
 // quantum (exact); P/rho^2 is gathered from its 4-byte array (jpo: the
@@ -333,14 +349,27 @@ __device__ __forceinline__ float h16_magic(uint32_t w, uint32_t s) { return __ui
 // path and the oracle round it, and j's FP32 velocity and density) when its
 // squared distance lies within the band where the 16-bit positions cannot
 // decide 0 < r^2 < (2h)^2, or when j is marked far: the pairs summed, and the
-// neighbour counts, are exactly those of the FP32 support test.
+// neighbour counts, are exactly those of the FP32 support test.  OFT: the
+// offsets from s_h16_off (one shared load) instead of shifts and masks of the
+// entry; POR: P/rho^2 recomputed from the density for gamma = 7 instead of
+// gathered.  Which costs less depends on whether the L1 data pipe (shared and
+// global loads) or instruction issue binds, so both are launch shapes.
+template <bool OFT, bool POR>
 __device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P, const PairC& C, const PairI& I,
                                           const H16I& H, const uint4& Qa, const uint4& Qb, uint32_t ea, uint32_t eb,
                                           bool qva, bool qvb, bool g7, f2 RHO0, f2 IRHO0, f2 C0, f2& AX, f2& AY,
                                           f2& AZ, f2& DS, float& vsa, float& vsb, unsigned& na, unsigned& nb) {
   const f2 MAG = dup(8388608.0f + 65536.0f), MAGV = dup(8388608.0f + 32768.0f);
-  constexpr uint32_t kLo = 0x7610u, kHi = 0x7632u;
-  const uint4 Oa = s_h16_off[ea >> kH16SlotBits], Ob = s_h16_off[eb >> kH16SlotBits];
+  constexpr uint32_t kLo = 0x7610u, kHi = 0x7632u, kO = 0x18000u;  // o + 1 at bits 15-16
+  uint4 Oa, Ob;
+  if (OFT) {
+    Oa = s_h16_off[ea >> kH16SlotBits], Ob = s_h16_off[eb >> kH16SlotBits];
+  } else {
+    Oa = make_uint4((ea >> (kH16SlotBits - 15)) & kO, (ea >> (kH16SlotBits - 13)) & kO,
+                    (ea >> (kH16SlotBits - 11)) & kO, 0u);
+    Ob = make_uint4((eb >> (kH16SlotBits - 15)) & kO, (eb >> (kH16SlotBits - 13)) & kO,
+                    (eb >> (kH16SlotBits - 11)) & kO, 0u);
+  }
   const f2 TX = sub2(pk(__uint_as_float(__float_as_uint(h16_magic(Qa.x, kLo)) + Oa.x),
                         __uint_as_float(__float_as_uint(h16_magic(Qb.x, kLo)) + Ob.x)),
                      MAG);
@@ -395,7 +424,8 @@ __device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P
   na += va, nb += vb;
   const f2 RHOJ = pk(rja, rjb);
   const uint32_t ga = ea & kH16SlotMask, gb = eb & kH16SlotMask;
-  const f2 POJ = pk(__ldg(&a.jpo[ga]), __ldg(&a.jpo[gb]));  // P/rho^2 as the FP32 records hold it
+  const f2 POJ = POR && g7 ? po7_2(RHOJ, RHO0, IRHO0, H.B)
+                           : pk(__ldg(&a.jpo[ga]), __ldg(&a.jpo[gb]));  // P/rho^2 as the FP32 records hold it
   const f2 CJ = g7 ? snds7_2(RHOJ, RHO0, IRHO0, C0) : pk(__ldg(&a.jC[ga]), __ldg(&a.jC[gb]));
   pair_terms2(C, I, DX, DY, DZ, R2raw, va, vb, VXJ, VYJ, VZJ, POJ, RHOJ, CJ, AX, AY, AZ, DS, vsa, vsb);
 }
@@ -412,10 +442,10 @@ __device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P
 // bound's blocks per SM (it sets the register budget).  With TPI = 1 every
 // sum runs in list order; TPI = 2 changes the summation order (the results
 // agree to FP32 rounding).
-template <bool H16, int TPI>
+template <bool H16, int TPI, bool OFT = false, bool POR = false>
 __device__ __forceinline__ void hydro_list_body(const StepArgs& a) {
   const unsigned full = 0xffffffffu;
-  if (H16) {  // before any thread leaves: the offset table of the half2 entries
+  if (H16 && OFT) {  // before any thread leaves: the offset table of the half2 entries
     if (threadIdx.x < 64) {
       const uint32_t c = threadIdx.x;
       s_h16_off[c] = make_uint4((c & 3u) << 15, ((c >> 2) & 3u) << 15, (c >> 4) << 15, 0u);
@@ -480,16 +510,17 @@ __device__ __forceinline__ void hydro_list_body(const StepArgs& a) {
         H.band = P.h16_band;
         H.hm = 0.5f * C.H2;
         H.slot = p;
+        H.B = dup(P.B);
         // entries past n up to the end of the group of four name the padding
         // slot, which no support, band or far test accepts
         for (int k = 4 * sub; k < n; k += 4 * TPI) {
           const uint4 e = __ldg(&row[k >> 2]);
           const uint4 Q0 = __ldg(&a.jh[e.x & kH16SlotMask]), Q1 = __ldg(&a.jh[e.y & kH16SlotMask]);
           const uint4 Q2 = __ldg(&a.jh[e.z & kH16SlotMask]), Q3 = __ldg(&a.jh[e.w & kH16SlotMask]);
-          h16_pair2(a, P, C, I, H, Q0, Q1, e.x, e.y, true, true, g7, RHO0, IRHO0, C0, AX, AY, AZ, DS, vsa, vsb, ca,
-                    cb);
-          h16_pair2(a, P, C, I, H, Q2, Q3, e.z, e.w, true, true, g7, RHO0, IRHO0, C0, AX, AY, AZ, DS, vsa, vsb, ca,
-                    cb);
+          h16_pair2<OFT, POR>(a, P, C, I, H, Q0, Q1, e.x, e.y, true, true, g7, RHO0, IRHO0, C0, AX, AY, AZ, DS, vsa,
+                              vsb, ca, cb);
+          h16_pair2<OFT, POR>(a, P, C, I, H, Q2, Q3, e.z, e.w, true, true, g7, RHO0, IRHO0, C0, AX, AY, AZ, DS, vsa,
+                              vsb, ca, cb);
         }
       } else {
         // idle halves past n read i's own record (weight 0): this loop keeps
@@ -540,18 +571,23 @@ __device__ __forceinline__ void hydro_list_body(const StepArgs& a) {
   if ((threadIdx.x & 31) == 0 && tot) atomicAdd(a.pair_count, (unsigned long long)tot);
 }
 
-template <bool H16, int TPI, int MINB>
+template <bool H16, int TPI, int MINB, bool OFT = false, bool POR = false>
 __global__ void __launch_bounds__(128, MINB) k_hydro_list(StepArgs a) {
-  hydro_list_body<H16, TPI>(a);
+  hydro_list_body<H16, TPI, OFT, POR>(a);
 }
 
 // Launch shapes of the list pass the autotuner chooses among: (threads per
 // particle, blocks of 128 per SM of the launch bound, which sets the register
 // budget: 96 or 128).  Shapes 0 and 2 sum in one order (bit-identical
-// results), shapes 1 and 3 in another.
-constexpr int kListShapes = 4;
-constexpr int kListShapeTPI[kListShapes] = {1, 2, 1, 2};
-constexpr int kListShapeBlock[kListShapes] = {128, 128, 128, 128};
+// results), shapes 1 and 3 in another.  Shapes 4-6 are shape 0 with the half2
+// pass's other ways to the offsets and P/rho^2 (h16_pair2 OFT, POR): 4 the
+// shared offset table, bit-identical to 0; 5 and 6 recompute P/rho^2 (FP32
+// rounding of 0), with shifts or with the table.  In the FP32 pass they are
+// shape 0.  (On the 1.6M dam break the half2 pass takes 0.566 ms in shape 0,
+// 0.615 with the table, 0.578 and 0.589 recomputing P/rho^2.)
+constexpr int kListShapes = 7;
+constexpr int kListShapeTPI[kListShapes] = {1, 2, 1, 2, 1, 1, 1};
+constexpr int kListShapeBlock[kListShapes] = {128, 128, 128, 128, 128, 128, 128};
 
 template <bool H16>
 inline int launch_hydro_list(const StepArgs& a, int n, cudaStream_t s, int shape = 0) {
@@ -564,6 +600,18 @@ inline int launch_hydro_list(const StepArgs& a, int n, cudaStream_t s, int shape
     case 1: k_hydro_list<H16, 2, 4><<<grid, 128, 0, s>>>(a); break;
     case 2: k_hydro_list<H16, 1, 4><<<grid, 128, 0, s>>>(a); break;
     case 3: k_hydro_list<H16, 2, 5><<<grid, 128, 0, s>>>(a); break;
+    case 4:
+      if (H16) k_hydro_list<true, 1, 5, true, false><<<grid, 128, 0, s>>>(a);
+      else k_hydro_list<false, 1, 5><<<grid, 128, 0, s>>>(a);
+      break;
+    case 5:
+      if (H16) k_hydro_list<true, 1, 5, false, true><<<grid, 128, 0, s>>>(a);
+      else k_hydro_list<false, 1, 5><<<grid, 128, 0, s>>>(a);
+      break;
+    case 6:
+      if (H16) k_hydro_list<true, 1, 5, true, true><<<grid, 128, 0, s>>>(a);
+      else k_hydro_list<false, 1, 5><<<grid, 128, 0, s>>>(a);
+      break;
     default: k_hydro_list<H16, 1, 5><<<grid, 128, 0, s>>>(a); break;
   }
   WCSPH_CUDA(cudaGetLastError());
