@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=16)
     ap.add_argument("--serving-nmax", type=float, default=2e5, help="largest request (config: 2e6 particles)")
     ap.add_argument("--serving-tend", type=float, default=0.1, help="physical end time (config: 1.0 s)")
+    ap.add_argument("--ncu-pass", action="store_true",
+                    help="only run 12 eager steps in list mode (launch shape 0, no autotuner, no graph) and exit: "
+                         "the 7th list-pass launch is a list step, for an ncu capture of one launch")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
@@ -553,6 +556,17 @@ def main():
     B.build()
     prec = args.precision if args.precision != "best" else best_precision()
     case = make_case(args.workload)
+    if args.ncu_pass:
+        if rank == 0:
+            from weaklycompressiblesph_b200.sim import Solver
+            with Solver(case.n + 1024, precision=precision_code(prec), max_instances=4,
+                        list_interval=args.list_interval, list_skin=args.list_skin, list_shape=0, autotune=False,
+                        use_graph=False) as s:
+                s.add(case)
+                s.step(12)
+                s.synchronize()
+                print(json.dumps({"ncu_pass": True, "precision": prec, "lists": s.list_stats()}))
+        return finish(pg)
     if args.e2e_only:
         if rank == 0:
             e = run_e2e(case, args.steps, args.warmup, local)
@@ -691,7 +705,7 @@ def validation_errors(workload, prec):
 # FP32 j-record and c (36 B); with lists its entry count (4 B).
 PASS_STATE_BYTES = 112
 OWN_RECORD_BYTES = 36
-COMPACT_RECORD_BYTES = 16   # half2 lists: the particle's compact record, fetched once as a j operand
+COMPACT_RECORD_BYTES = 20   # half2 lists: the particle's compact record and P/rho^2, fetched once as j operands
 SURVEY_I_BYTES = 64         # the per-particle i read and write of the per-pair record model
 
 
@@ -716,7 +730,7 @@ def hbm_roofline(workload, prec, n, dev, peak, peak_kind):
         per_particle = PASS_STATE_BYTES + OWN_RECORD_BYTES + 4 + (COMPACT_RECORD_BYTES if prec == "half2" else 0)
         alg = n * per_particle + 4.0 * lists["entries"]
         units = (f"{per_particle} B per particle (state {PASS_STATE_BYTES}, own record {OWN_RECORD_BYTES}, "
-                 f"list count 4" + (f", compact record {COMPACT_RECORD_BYTES}" if prec == "half2" else "")
+                 f"list count 4" + (f", compact record and P/rho^2 {COMPACT_RECORD_BYTES}" if prec == "half2" else "")
                  + ") + 4 B per list entry")
         key = f"{workload}/{prec}/lists"
     else:
@@ -730,6 +744,10 @@ def hbm_roofline(workload, prec, n, dev, peak, peak_kind):
         key = f"{workload}/{prec}"
     achieved = alg / (launch_ms * 1e-3) / 1e9
     traffic = None
+    limiter = "instruction issue"
+    if lists:
+        l1 = (_profile_json("hydro_list_l1.json") or {}).get(f"{workload}/{prec}", {})
+        limiter = l1.get("limiter", "L1 data pipe") + " (roofline_l1)"
     tp = _profile_json("hydro_traffic.json")
     if tp:
         traffic = tp.get(key, {}).get("bytes_per_launch")
@@ -737,16 +755,17 @@ def hbm_roofline(workload, prec, n, dev, peak, peak_kind):
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "kernel": kernel, "launch_ms": launch_ms, "algorithmic_bytes": alg,
             "model": units, "peak_kind": peak_kind,
-            "limiter": "L1 data pipe (roofline_l1)" if lists else "instruction issue",
+            "limiter": limiter,
             "pair_record_model": {"bytes_per_pair": bpp, "bytes_per_particle": SURVEY_I_BYTES,
                                   "operand_rate_gbs": pair_rate,
                                   "note": "j-records delivered to the pair terms, mostly from L1; not DRAM"}}
 
 
 def l1_roofline(workload, prec, dev):
-    """The list pass is bound by the L1 data pipe that delivers its gathers.
-    Per list entry it needs one list word and one j-record: at 128 B per L1
-    wavefront that is (4 + record bytes) / 128 wavefronts at least.  The
+    """The FP32 list pass is bound by the L1 data pipe that delivers its
+    gathers (the half2 pass about as much by issue).  Per list entry it needs
+    one list word and one j-record (half2: the compact record and P/rho^2): at
+    128 B per L1 wavefront that is (4 + record bytes) / 128 wavefronts at least.  The
     measured L1 load wavefronts of one launch come from the ncu capture
     summarised in profiles/hydro_list_l1.json; entries and true pairs are this
     run's."""
