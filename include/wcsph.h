@@ -221,9 +221,10 @@ typedef struct wcsph_sim_options {
                                   so the pairs summed are the same as with a fresh search (the
                                   summation order differs) */
   float list_skin;             /* skin in units of h (0: 0.3) */
-  int32_t list_shape;          /* launch shape of the neighbour-list pass: 0 the autotuner's choice
-                                  (shape 0 without autotune); s + 1 fixes shape s (the shapes of
-                                  wcsph_sim_tuning's out[1]) */
+  int32_t list_shape;          /* launch shapes of the neighbour-list passes, 0 in a field for the
+                                  autotuner's choice (shape 0 without autotune): bits 0-7 s + 1 fix
+                                  the list pass's shape s (wcsph_sim_tuning's out[1]), bits 8-15
+                                  b + 1 the list build scan's shape b (out[3]) */
 } wcsph_sim_options;
 
 typedef struct wcsph_sim wcsph_sim;
@@ -369,7 +370,9 @@ int32_t wcsph_sim_kernels_per_step(wcsph_sim* sim);
  * differently: results agree to FP32 rounding), out[2] log2 particle bucket
  * it was tuned for (-1:
  * defaults, not tuned), out[3] shape of the list build's scan (0-2 as out[0];
- * 3, 4: 4 or 8 warps per block with 256-candidate tiles). */
+ * 3, 4: 4 or 8 warps per block with 256-candidate tiles; 5, 6: one lane per
+ * particle walking a 512- or 256-candidate tile, 4 or 8 warps per block; all
+ * build the same lists). */
 int wcsph_sim_tuning(wcsph_sim* sim, int32_t* out4);
 /* Neighbour-list counters (list_interval > 0): out[0] list builds, out[1]
  * steps that read the lists, out[2] builds whose lists overflowed (the next

@@ -236,6 +236,34 @@ def test_list_pass_every_shape_vs_fp64(prec, shape, native, oracle_lib):
 
 
 @pytest.mark.parametrize("prec", [N.PREC_TILED, N.PREC_HALF2], ids=["tiled", "half2"])
+def test_every_build_shape_builds_the_same_lists(prec, native, oracle_lib):
+    """Every shape of the list build's scan (the tiled scan's block and tile
+    shapes, and the lane-per-particle scan) writes the same entries in the
+    same order: after builds and list steps the states are bit-identical,
+    and the list pass on them matches the FP64 oracle."""
+    case = small_dam(dx=0.04, seed=33, vel_sigma=0.4)
+    states, probes, entries = [], [], []
+    for b in range(N.BUILD_SHAPES):
+        with Solver(case.n, precision=prec, list_interval=4, list_shape=0, build_shape=b) as s:
+            k = s.add(case)
+            s.step(9)  # builds at steps 1, 5, 9 at least
+            assert s.tuning()["build_shape"] == b
+            assert s.list_stats()["builds"] >= 3
+            states.append(s.read(k))
+            probes.append(s.probe(k, lists=True))
+            entries.append(s.list_entries())
+    for st, pr, ne in zip(states[1:], probes[1:], entries[1:]):
+        assert ne == entries[0]
+        for key in ("pos", "vel", "dens", "acc"):
+            np.testing.assert_array_equal(st[key], states[0][key])
+        for key in ("acc", "div_v", "nbr"):
+            np.testing.assert_array_equal(pr[key], probes[0][key])
+    r = oracle_list_check(oracle_lib, case, states[0], probes[0], 0)
+    np.testing.assert_array_equal(probes[0]["nbr"], r["cnt"])
+    assert r["acc"] < LIST_TOL[prec] and r["div_v"] < LIST_TOL[prec], r
+
+
+@pytest.mark.parametrize("prec", [N.PREC_TILED, N.PREC_HALF2], ids=["tiled", "half2"])
 def test_list_pass_periodic_vs_fp64(prec, native, oracle_lib):
     """Config-3 mode (periodic box, summation density every step) through the
     lists: particles run past the faces between builds (wrapping waits for the

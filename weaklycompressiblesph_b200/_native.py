@@ -22,6 +22,7 @@ DENSITY_CONTINUITY, DENSITY_SUMMATION, DENSITY_SHEPARD = 0, 1, 2
 HYDRO, FREEZE = 0, 1
 FDPS_MAX_TAGS = 4
 LIST_SHAPES = 7  # launch shapes of the neighbour-list pass (wcsph_sim_tuning out[1])
+BUILD_SHAPES = 7  # launch shapes of the list build's scan (wcsph_sim_tuning out[3])
 
 
 class FdpsLayout(C.Structure):

@@ -458,8 +458,9 @@ static int autotune(SimImpl& S) {
     b.x0 = S.x0;
     b.alt = b.main;
     float best_list = 1e30f;
-    int best_list_shape = S.opt.list_shape > 0 ? S.opt.list_shape - 1 : 0;
-    for (int v = 0; v < kListShapes && S.opt.list_shape == 0; ++v) {
+    const int fixed_list = S.opt.list_shape & 0xff, fixed_build = (S.opt.list_shape >> 8) & 0xff;
+    int best_list_shape = fixed_list > 0 ? fixed_list - 1 : 0;
+    for (int v = 0; v < kListShapes && fixed_list == 0; ++v) {
       int rc = time_launches(S, 3, [&]() {
         return h16 ? launch_hydro_list<true>(b, n, S.s, v) : launch_hydro_list<false>(b, n, S.s, v);
       }, &ms);
@@ -471,8 +472,8 @@ static int autotune(SimImpl& S) {
     StepArgs c = a;
     c.x0 = S.x0;
     float best_build = 1e30f;
-    int best_build_shape = 0;
-    for (int v = 0; v < kBuildShapes; ++v) {
+    int best_build_shape = fixed_build > 0 ? fixed_build - 1 : 0;
+    for (int v = 0; v < kBuildShapes && fixed_build == 0; ++v) {
       int rc = time_launches(S, 3, [&]() {
         return h16 ? launch_hydro_tiled<true, true>(c, n, S.s, v) : launch_hydro_tiled<false, true>(c, n, S.s, v);
       }, &ms);
@@ -745,7 +746,8 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
   if (!opt || !out || opt->max_particles <= 0 || opt->max_particles > INT32_MAX - 1 || opt->max_cells <= 0 ||
       opt->max_cells > INT32_MAX || opt->max_instances <= 0 || opt->max_instances > (int)kInstMask ||
       opt->precision < 0 || opt->precision > 2 || opt->list_interval < 0 || !(opt->list_skin >= 0.f) ||
-      opt->list_shape < 0 || opt->list_shape > kListShapes) {
+      opt->list_shape < 0 || (opt->list_shape & 0xff) > kListShapes || ((opt->list_shape >> 8) & 0xff) > kBuildShapes ||
+      (opt->list_shape >> 16) != 0) {
     set_error("wcsph_sim_create: invalid options");
     return WCSPH_E_INVALID;
   }
@@ -773,7 +775,8 @@ int wcsph_sim_create(const wcsph_sim_options* opt, wcsph_sim** out) {
   auto* sim = new wcsph_sim();
   SimImpl& S = sim->impl;
   S.opt = *opt;
-  S.list_shape = opt->list_shape > 0 ? opt->list_shape - 1 : 0;
+  S.list_shape = (opt->list_shape & 0xff) > 0 ? (opt->list_shape & 0xff) - 1 : 0;
+  S.build_shape = ((opt->list_shape >> 8) & 0xff) > 0 ? ((opt->list_shape >> 8) & 0xff) - 1 : 0;
   auto fail = [&](int rc) {
     for (void* p : S.allocs) cudaFree(p);
     if (S.s) cudaStreamDestroy(S.s);

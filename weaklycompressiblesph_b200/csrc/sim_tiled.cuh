@@ -250,6 +250,103 @@ __device__ __forceinline__ void append2(uint32_t* q, int& n, bool he, bool ho, u
   n += __popc(me) + __popc(mo);
 }
 
+// The 27 neighbour-cell ranges of cell (cx, cy, cz) of instance P, one per
+// lane k < 27 (offset (k%3-1, k/3%3-1, k/9-1)): first slot, count, periodic
+// image shift and entry code (the image code k, or with HL, the half2 list
+// build, the neighbour-cell offset + 1 in two bits per axis: its compact
+// records are relative to the build's cells), the exclusive prefix of the
+// counts over the lanes and, in every lane, their total.
+struct NbRanges {
+  int start, excl, total;
+  float shx, shy, shz;
+  uint32_t code;
+};
+template <bool HL>
+__device__ __forceinline__ NbRanges nb_ranges(const StepArgs& a, const InstParams& P, int cx, int cy, int cz,
+                                              int lane) {
+  const unsigned full = 0xffffffffu;
+  const int nx = P.ncell[0], ny = P.ncell[1];
+  NbRanges R;
+  int cnt = 0;
+  R.start = 0, R.shx = 0.f, R.shy = 0.f, R.shz = 0.f, R.code = 13;
+  if (lane < 27) {
+    int x, y, z;
+    if (neighbor_cell(P, 0, cx + lane % 3 - 1, x, R.shx) && neighbor_cell(P, 1, cy + (lane / 3) % 3 - 1, y, R.shy) &&
+        neighbor_cell(P, 2, cz + lane / 9 - 1, z, R.shz)) {
+      const int l2 = P.cell_base + (z * ny + y) * nx + x;
+      R.start = a.cell_start[l2];
+      cnt = a.cell_end[l2] - R.start;
+      R.code = (uint32_t)((R.shx > 0.f) - (R.shx < 0.f) + 1) + 3u * (uint32_t)((R.shy > 0.f) - (R.shy < 0.f) + 1) +
+               9u * (uint32_t)((R.shz > 0.f) - (R.shz < 0.f) + 1);
+    }
+    if (HL) R.code = (uint32_t)(lane % 3) | ((uint32_t)((lane / 3) % 3) << 2) | ((uint32_t)(lane / 9) << 4);
+  }
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(full, incl, o);
+    if (lane >= o) incl += t;
+  }
+  R.total = __shfl_sync(full, incl, 31);
+  R.excl = incl - cnt;
+  return R;
+}
+
+// Stage candidates [t0, t0 + tn) of a cell's flattened neighbour ranges into
+// a warp's tile: positions pre-shifted by the periodic image, entries slot |
+// code (at bit 27, or with HL at bit 26), padded to a multiple of 64 with
+// positions that no support test accepts.  Candidate u comes from the last
+// neighbour cell k with excl_k <= u (binary search over lanes 0..26);
+// kStageUnroll independent loads per lane are in flight before any store.
+template <bool HL>
+__device__ __forceinline__ void stage_tile(const StepArgs& a, const NbRanges& R, int t0, int tn, float* tx,
+                                           float* ty, float* tz, uint32_t* te, int lane) {
+  const unsigned full = 0xffffffffu;
+  const int tn64 = (tn + 63) & ~63;
+  for (int ub = t0; ub < t0 + tn; ub += 32 * kStageUnroll) {
+    float4 J[kStageUnroll];
+    int gk[kStageUnroll], kk[kStageUnroll];
+#pragma unroll
+    for (int r = 0; r < kStageUnroll; ++r) {
+      const int u = ub + 32 * r + lane;
+      int k = 0;
+#pragma unroll
+      for (int step = 16; step; step >>= 1) {
+        const int cand = k + step;
+        const int ec = __shfl_sync(full, R.excl, cand < 27 ? cand : 26);
+        if (cand < 27 && ec <= u) k = cand;
+      }
+      const int sk = __shfl_sync(full, R.start, k), ek = __shfl_sync(full, R.excl, k);
+      kk[r] = k;
+      gk[r] = sk + (u - ek);
+      if (u < t0 + tn) J[r] = __ldg(&a.jr[gk[r]].a);
+    }
+#pragma unroll
+    for (int r = 0; r < kStageUnroll; ++r) {
+      const int u = ub + 32 * r + lane;
+      const int k = kk[r];
+      const float sx = __shfl_sync(full, R.shx, k), sy = __shfl_sync(full, R.shy, k), sz = __shfl_sync(full, R.shz, k);
+      const uint32_t ck = __shfl_sync(full, R.code, k) << (HL ? kH16SlotBits : 27);
+      if (u < t0 + tn) {
+        tx[u - t0] = __fadd_rn(J[r].x, sx);
+        ty[u - t0] = __fadd_rn(J[r].y, sy);
+        tz[u - t0] = __fadd_rn(J[r].z, sz);
+        te[u - t0] = (uint32_t)gk[r] | ck;
+      }
+    }
+  }
+  for (int u = tn + lane; u < tn64; u += 32) {  // pad to a multiple of 64: never in support
+    tx[u] = 1.0e30f;
+    ty[u] = 1.0e30f;
+    tz[u] = 1.0e30f;
+    te[u] = 0u;
+  }
+}
+
+// k_hydro_tiled keeps its own copy of the neighbour-range and staging code:
+// written through these helpers it allocated registers differently and
+// spilled in its 4- and 8-warp list-build shapes.
+
 // LB (neighbour-list build): scan only.  The scan keeps the candidates
 // within the list radius 2h + skin and each i's queue is written to its list
 // (list_cnt holds the full count, also past the list's capacity); the pair
@@ -454,6 +551,97 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
   if (lane == 0 && pairs) atomicAdd(a.pair_count, pairs);
 }
 
+// List build, lane per particle: a warp per non-empty cell stages the
+// cell's candidates as k_hydro_tiled does (stage_tile); then each lane takes
+// one particle i of the cell and walks the tile four candidates per step
+// (shared-memory broadcasts, two f32x2 distances), appending each candidate
+// within the list radius (0 < r^2 < (2h + skin)^2) to its own list row.  No
+// ballots and no queues: the entries are those of k_hydro_tiled's scan in the
+// same (candidate) order, so the lists are bit-identical.
+template <int WARPS, int TILE>
+struct ScanSmem {
+  float x[WARPS][TILE], y[WARPS][TILE], z[WARPS][TILE];
+  uint32_t e[WARPS][TILE];
+};
+
+template <bool H16, int WARPS, int TILE>
+__global__ void __launch_bounds__(WARPS * 32) k_list_scan(StepArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ScanSmem<WARPS, TILE>& S = *reinterpret_cast<ScanSmem<WARPS, TILE>*>(smem_raw);
+  const unsigned full = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* tx = S.x[warp];
+  float* ty = S.y[warp];
+  float* tz = S.z[warp];
+  uint32_t* te = S.e[warp];
+  const int nrun = *a.run_count;
+  const int L = a.list_max;
+  const int stride = gridDim.x * WARPS;
+  int c = blockIdx.x * WARPS + warp;
+  int lin_next = c < nrun ? a.run_list[c] : 0;
+  for (; c < nrun; c += stride) {
+    const int lin = lin_next;
+    if (c + stride < nrun) lin_next = a.run_list[c + stride];
+    const int s = a.cell_start[lin], e = a.cell_end[lin];
+    const int inst = a.alt.flags[s] & kInstMask;
+    if (a.inst_keep && a.list_flags[kLfPartial] != 0u && a.inst_keep[inst]) continue;  // keeps its lists
+    const InstParams& P = a.params[inst];
+    if (!wants_force(P, a.dyn[inst], a.phase[inst])) {
+      for (int p = s + lane; p < e; p += 32) a.list_cnt[p] = 0;
+      continue;
+    }
+    const int nx = P.ncell[0], ny = P.ncell[1];
+    const int local = lin - P.cell_base;
+    const NbRanges R = nb_ranges<H16>(a, P, local % nx, (local / nx) % ny, local / (nx * ny), lane);
+    const float HS = P.HL2;
+    for (int ib = s; ib < e; ib += 32) {
+      const int p = ib + lane;
+      const bool mine = p < e;
+      const float4 I = __ldg(&a.jr[mine ? p : s].a);
+      const f2 IX = dup(I.x), IY = dup(I.y), IZ = dup(I.z);
+      uint32_t* row = a.list + (size_t)(mine ? p : s) * L;
+      int cnt = 0;
+      for (int t0 = 0; t0 < R.total; t0 += TILE) {
+        const int tn = min(TILE, R.total - t0);
+        __syncwarp();
+        stage_tile<H16>(a, R, t0, tn, tx, ty, tz, te, lane);
+        __syncwarp();
+        if (mine) {
+          for (int u = 0; u < tn; u += 4) {  // the tile is padded to a multiple of 64
+            const f2* x2 = reinterpret_cast<const f2*>(&tx[u]);
+            const f2* y2 = reinterpret_cast<const f2*>(&ty[u]);
+            const f2* z2 = reinterpret_cast<const f2*>(&tz[u]);
+            const uint4 E = *reinterpret_cast<const uint4*>(&te[u]);
+            f2 DX = sub2(IX, x2[0]), DY = sub2(IY, y2[0]), DZ = sub2(IZ, z2[0]);
+            const f2 RA = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));  // == dist2 per half
+            DX = sub2(IX, x2[1]), DY = sub2(IY, y2[1]), DZ = sub2(IZ, z2[1]);
+            const f2 RB = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
+            const float r2[4] = {lo(RA), hi(RA), lo(RB), hi(RB)};
+            const uint32_t ev[4] = {E.x, E.y, E.z, E.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              if (r2[k] > 0.0f && r2[k] < HS) {
+                if (cnt < L) row[cnt] = ev[k];
+                ++cnt;
+              }
+            }
+          }
+        }
+      }
+      if (mine) {
+        a.list_cnt[p] = cnt;
+        if (cnt > L) {
+          a.list_flags[kLfOverflowPending] = 1u;  // the next step rebuilds
+        } else {  // pad the row to a whole group of four (list_max is a multiple of four)
+          for (int k = cnt; k < ((cnt + 3) & ~3); ++k) row[k] = a.list_pad;
+        }
+      }
+      const int mx = __reduce_max_sync(full, mine ? cnt : 0);
+      if (lane == 0) atomicMax(&a.list_flags[kLfLongest], (unsigned)mx);
+    }
+  }
+}
+
 struct TiledLaunch {
   int device = -1;
   int blocks = 0;
@@ -467,6 +655,27 @@ inline int launch_pair_tiled_v(const StepArgs& a, cudaStream_t s) {
   TiledLaunch& T = L[dev & 15];
   auto kern = k_hydro_tiled<H16, WARPS, TILE, LB>;
   const int bytes = (int)sizeof(TiledSmem<WARPS, TILE>);
+  if (T.device != dev) {
+    WCSPH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    int per_sm = 0, sms = 0;
+    WCSPH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, bytes));
+    WCSPH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    T.blocks = std::max(1, per_sm) * sms;
+    T.device = dev;
+  }
+  kern<<<T.blocks, WARPS * 32, bytes, s>>>(a);
+  WCSPH_CUDA(cudaGetLastError());
+  return 0;
+}
+
+template <bool H16, int WARPS, int TILE>
+inline int launch_list_scan_v(const StepArgs& a, cudaStream_t s) {
+  static TiledLaunch L[16];
+  int dev = 0;
+  WCSPH_CUDA(cudaGetDevice(&dev));
+  TiledLaunch& T = L[dev & 15];
+  auto kern = k_list_scan<H16, WARPS, TILE>;
+  const int bytes = (int)sizeof(ScanSmem<WARPS, TILE>);
   if (T.device != dev) {
     WCSPH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     int per_sm = 0, sms = 0;
@@ -494,6 +703,8 @@ inline int launch_hydro_tiled(const StepArgs& a, int n, cudaStream_t s, int shap
   if constexpr (LB) {  // list builds only: smaller tiles, more warps per SM (the scan writes no sums)
     if (shape == 3) return launch_pair_tiled_v<H16, 4, 256, LB>(a, s);
     if (shape == 4) return launch_pair_tiled_v<H16, 8, 256, LB>(a, s);
+    if (shape == 5) return launch_list_scan_v<H16, 4, 512>(a, s);
+    if (shape == 6) return launch_list_scan_v<H16, 8, 256>(a, s);
   }
   switch (shape) {
     case 1: return launch_pair_tiled_v<H16, 2, 512, LB>(a, s);
@@ -505,7 +716,9 @@ inline int launch_hydro_tiled(const StepArgs& a, int n, cudaStream_t s, int shap
 // Shapes of the list build's scan-only pass: the three above and two with
 // 256-candidate tiles (half the shared memory a warp, so up to twice the
 // warps per SM; a cell's candidates then take two tile passes, which changes
-// only the order in which its list entries are found within each pass).
-constexpr int kBuildShapes = 5;
+// only the order in which its list entries are found within each pass), and
+// the lane-per-particle scan k_list_scan with 4 warps x 512 or 8 warps x 256
+// candidates (the same entries in the same order).
+constexpr int kBuildShapes = 7;
 
 }  // namespace wcsph

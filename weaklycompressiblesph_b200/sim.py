@@ -26,10 +26,12 @@ def _f32(a, shape):
 
 class Solver:
     def __init__(self, max_particles, precision=N.PREC_FP32, max_cells=None, max_instances=64, device=0,
-                 use_graph=True, autotune=True, list_interval=0, list_skin=0.0, list_shape=None):
+                 use_graph=True, autotune=True, list_interval=0, list_skin=0.0, list_shape=None,
+                 build_shape=None):
         """list_interval > 0 turns on neighbour lists (radius 2h + list_skin h,
         rebuilt at least every list_interval steps; see wcsph_sim_options).
-        list_shape fixes the list pass's launch shape (None: the autotuner's)."""
+        list_shape / build_shape fix the list pass's and the list build scan's
+        launch shapes (None: the autotuner's)."""
         o = N.SimOptions()
         o.device = device
         o.precision = precision
@@ -40,7 +42,8 @@ class Solver:
         o.autotune = 1 if autotune else 0
         o.list_interval = int(list_interval)
         o.list_skin = float(list_skin)
-        o.list_shape = 0 if list_shape is None else int(list_shape) + 1
+        o.list_shape = (0 if list_shape is None else int(list_shape) + 1) | \
+            ((0 if build_shape is None else int(build_shape) + 1) << 8)
         self.opt = o
         h = C.c_void_p()
         N.call("wcsph_sim_create", C.byref(o), C.byref(h))
