@@ -553,8 +553,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_hydro_tiled(StepArgs a) {
 
 // List build, lane per particle: a warp per non-empty cell stages the
 // cell's candidates as k_hydro_tiled does (stage_tile); then each lane takes
-// one particle i of the cell and walks the tile four candidates per step
-// (shared-memory broadcasts, two f32x2 distances), appending each candidate
+// one particle i of the cell and walks the tile eight candidates per step
+// (shared-memory broadcasts, four f32x2 distances), appending each candidate
 // within the list radius (0 < r^2 < (2h + skin)^2) to its own list row.  No
 // ballots and no queues: the entries are those of k_hydro_tiled's scan in the
 // same (candidate) order, so the lists are bit-identical.
@@ -593,7 +593,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_list_scan(StepArgs a) {
     const int nx = P.ncell[0], ny = P.ncell[1];
     const int local = lin - P.cell_base;
     const NbRanges R = nb_ranges<H16>(a, P, local % nx, (local / nx) % ny, local / (nx * ny), lane);
-    const float HS = P.HL2;
+    // 0 < r^2 < (2h + skin)^2 as one unsigned compare of the bit patterns
+    // (r^2 is a sum of squares, never negative or NaN)
+    const uint32_t hb = __float_as_uint(P.HL2) - 1u;
     for (int ib = s; ib < e; ib += 32) {
       const int p = ib + lane;
       const bool mine = p < e;
@@ -607,20 +609,23 @@ __global__ void __launch_bounds__(WARPS * 32) k_list_scan(StepArgs a) {
         stage_tile<H16>(a, R, t0, tn, tx, ty, tz, te, lane);
         __syncwarp();
         if (mine) {
-          for (int u = 0; u < tn; u += 4) {  // the tile is padded to a multiple of 64
+          for (int u = 0; u < tn; u += 8) {  // the tile is padded to a multiple of 64
             const f2* x2 = reinterpret_cast<const f2*>(&tx[u]);
             const f2* y2 = reinterpret_cast<const f2*>(&ty[u]);
             const f2* z2 = reinterpret_cast<const f2*>(&tz[u]);
-            const uint4 E = *reinterpret_cast<const uint4*>(&te[u]);
-            f2 DX = sub2(IX, x2[0]), DY = sub2(IY, y2[0]), DZ = sub2(IZ, z2[0]);
-            const f2 RA = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));  // == dist2 per half
-            DX = sub2(IX, x2[1]), DY = sub2(IY, y2[1]), DZ = sub2(IZ, z2[1]);
-            const f2 RB = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
-            const float r2[4] = {lo(RA), hi(RA), lo(RB), hi(RB)};
-            const uint32_t ev[4] = {E.x, E.y, E.z, E.w};
+            const uint4 E0 = *reinterpret_cast<const uint4*>(&te[u]);
+            const uint4 E1 = *reinterpret_cast<const uint4*>(&te[u + 4]);
+            float r2[8];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-              if (r2[k] > 0.0f && r2[k] < HS) {
+            for (int h = 0; h < 4; ++h) {
+              const f2 DX = sub2(IX, x2[h]), DY = sub2(IY, y2[h]), DZ = sub2(IZ, z2[h]);
+              const f2 R2 = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));  // == dist2 per half
+              r2[2 * h] = lo(R2), r2[2 * h + 1] = hi(R2);
+            }
+            const uint32_t ev[8] = {E0.x, E0.y, E0.z, E0.w, E1.x, E1.y, E1.z, E1.w};
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+              if (__float_as_uint(r2[k]) - 1u < hb) {
                 if (cnt < L) row[cnt] = ev[k];
                 ++cnt;
               }
