@@ -270,14 +270,12 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
     k_permute<<<nblk(n), kBlock, 0, S.s>>>(a);
     ++L;
     if (ev) WCSPH_CUDA(cudaEventRecord(ev[1], S.s));
-    if (density) {
+    // A list build scans first and takes its density pass from the lists
+    // (every instance's are current after the scan: rebuilt or kept); the
+    // scan reads positions only, and the EoS records it gathers do not enter
+    // the lists.  Other passes search the cells for the density.
+    if (density && !build_lists) {
       k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(a);
-      if (a.inst_keep) {  // a partial build: the instances that keep their lists read them
-        StepArgs b = a;
-        b.density_keep_only = 1;
-        if (int rc = launch_density_list(b, n, S.s, h16_lists(S.opt))) return rc;
-        ++L;
-      }
       k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
       L += 2;
     }
@@ -290,6 +288,14 @@ static int enqueue_pass(SimImpl& S, StepArgs a, bool density, bool init_filter, 
                        : launch_hydro_tiled<false, true>(a, n, S.s, S.build_shape))
         return rc;
       if (ev && S.scan_ev) WCSPH_CUDA(cudaEventRecord(S.scan_ev, S.s));
+      if (density) {
+        if (int rc = launch_density_list(a, n, S.s, h16)) return rc;
+        StepArgs b = a;  // the particles whose list overflowed: the cell search
+        b.density_overflow_only = 1;
+        k_density_plain<<<nblk(n), kBlock, 0, S.s>>>(b);
+        k_eos<<<nblk(n), kBlock, 0, S.s>>>(a);
+        L += 3;
+      }
       if (int rc = h16 ? launch_hydro_list<true>(a, n, S.s, S.list_shape)
                        : launch_hydro_list<false>(a, n, S.s, S.list_shape))
         return rc;

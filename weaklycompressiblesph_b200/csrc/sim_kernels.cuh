@@ -37,8 +37,9 @@ __device__ __forceinline__ JRec ld_jrec(const JRec* p) {
 // cell at the last list build (steps of 2^-15 cell edges, biased by 2^15, so
 // one cell edge either side).  Velocities are 16-bit fixed point in steps of
 // the instance's velocity quantum vq (a power of two, 2^-15 of a bound on its
-// fastest particle this step; InstDyn::vq), biased by 2^15.  P/rho^2 and c
-// are recomputed from rho by the pass.  A particle outside either range (far
+// fastest particle this step; InstDyn::vq), biased by 2^15.  P/rho^2 is
+// gathered from jpo beside the records and c recomputed from rho by the
+// pass.  A particle outside either range (far
 // from its build cell, above the grid where cells are clamped, faster than
 // the bound) or removed is marked far (rho = kFarRho, 0: finite in every term
 // it meets before the entry switches to the FP32 record), and its entries are
@@ -139,12 +140,12 @@ struct StepArgs {
   unsigned* inst_motion;  // neighbour lists: per instance, the largest |x - x0|, |v| and |a| over its moving
                           // particles at the end of the step, in units of its skin (float bits)
   int* inst_keep;          // neighbour lists, partial builds: per instance, 1 = keeps its lists (k_list_set)
-  int density_keep_only;   // a partial build's list density pass: only the instances that keep their lists
   // compact j-records of the half2 list pass (WCSPH_PREC_HALF2 with lists; null otherwise)
   uint4* jh;              // 16-bit cell-relative x, y, z, 16-bit velocity, FP32 rho (write_h16)
   float* jpo;             // P/rho^2 of every slot beside jh (jr[p].a.w, gathered in 4 bytes)
   uint32_t list_pad;      // list entry naming the padding slot (k_list_pad_slot): rows are padded with it
                           // to whole groups of four entries
+  int density_overflow_only;  // k_density_plain of a list build: only the particles whose list overflowed
   int probe_density;      // density pass of a probe launch: 0 none, 1 summation, 2 Shepard
   // diagnostics (probe phase)
   float4* diag_acc;
@@ -417,6 +418,7 @@ __global__ void k_density_plain(StepArgs a) {
   if (a.dens_any && !*a.dens_any) return;  // no density pass in this launch
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= *a.n_alive) return;
+  if (a.density_overflow_only && a.list_cnt[p] <= a.list_max) return;  // k_density_list has it
   const int inst = a.alt.flags[p] & kInstMask;
   const InstParams& P = a.params[inst];
   const int kind = density_kind(a, P, a.dyn[inst], a.phase[inst]);

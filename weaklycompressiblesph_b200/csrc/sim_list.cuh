@@ -239,7 +239,6 @@ __global__ void __launch_bounds__(128) k_density_list(StepArgs a) {
   if (p >= *a.n_alive) return;
   const uint32_t fp = a.alt.flags[p];
   const int inst = fp & kInstMask;
-  if (a.density_keep_only && !a.inst_keep[inst]) return;  // a partial build: the others searched
   const InstParams& P = a.params[inst];
   const int kind = density_kind(a, P, a.dyn[inst], a.phase[inst]);
   if (!kind) return;
@@ -251,6 +250,9 @@ __global__ void __launch_bounds__(128) k_density_list(StepArgs a) {
   const float iH = P.inv_H, H2 = P.H2;
   const float4 I = a.jr[p].a;
   const float rho_i = a.jr[p].b.w;
+  // a list that overflowed at this step's build: k_density_plain sums it over
+  // the cell search (density_overflow_only), and the next step builds again
+  if (a.list_cnt[p] > a.list_max) return;
   const int n = min(a.list_cnt[p], a.list_max);
   const uint4* row = reinterpret_cast<const uint4*>(a.list + (size_t)p * a.list_max);
   int ci[3] = {0, 0, 0};
