@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=16)
     ap.add_argument("--serving-nmax", type=float, default=2e5, help="largest request (config: 2e6 particles)")
     ap.add_argument("--serving-tend", type=float, default=0.1, help="physical end time (config: 1.0 s)")
+    ap.add_argument("--serving-no-serial", action="store_true",
+                    help="time only the served mix (skip the one-at-a-time plain FP32 baseline)")
     ap.add_argument("--ncu-pass", action="store_true",
                     help="only run 12 eager steps in list mode (launch shape 0, no autotuner, no graph) and exit: "
                          "the 7th list-pass launch is a list step, for an ncu capture of one launch")
@@ -512,14 +514,15 @@ def measure_serving(device):
         out = srv.run(reqs)
     el = 0.0
     ps = 0
-    for _, c in reqs:
+    for _, c in ([] if ARGS.serving_no_serial else reqs):
         t, steps, _ = run_alone(c, precision=N.PREC_FP32, device=device)
         el += t
         ps += c.n * steps
+    serial = ps / el if el > 0 else None
     return {"requests": len(reqs), "particles": total, "p50_s": out["p50_s"], "p99_s": out["p99_s"],
             "wall_s": out["wall_s"], "particle_steps_per_s": out["particle_steps_per_s"],
-            "serial_plain_particle_steps_per_s": ps / el,
-            "speedup_vs_serial_plain": out["particle_steps_per_s"] / (ps / el),
+            "serial_plain_particle_steps_per_s": serial,
+            "speedup_vs_serial_plain": out["particle_steps_per_s"] / serial if serial else None,
             "neighbour_search": (f"lists, rebuilt at least every {ARGS.list_interval} steps" if ARGS.list_interval
                                  else "every step") + "; serial baseline: plain FP32, search every step",
             "precision": ARGS.serving_precision,
