@@ -443,7 +443,11 @@ __device__ __forceinline__ void h16_pair2(const StepArgs& a, const InstParams& P
 // instead of gathered: one gather per entry fewer.  MINB is the launch
 // bound's blocks per SM (it sets the register budget).  With TPI = 1 every
 // sum runs in list order; TPI = 2 changes the summation order (the results
-// agree to FP32 rounding).
+// agree to FP32 rounding).  The half2 pass (H16) reads every group of four
+// whole: rows are padded with the padding slot's entry (k_list_pad_slot);
+// OFT and POR choose how it gets the neighbour-cell offsets and P/rho^2
+// (h16_pair2).  The FP32 pass keeps its per-entry selects of i's own record
+// for the entries past n, which fit its 96 registers without spilling.
 template <bool H16, int TPI, bool OFT = false, bool POR = false>
 __device__ __forceinline__ void hydro_list_body(const StepArgs& a) {
   const unsigned full = 0xffffffffu;
